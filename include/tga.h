@@ -1,0 +1,218 @@
+/*
+ * tga.h -- C ABI of the B200 acquisition engine (libtga.so).
+ *
+ * Drop-in replacement for the parallel code-phase / Doppler acquisition
+ * search of tart-gnss-acquire v0.4.0 (tmolteno/tart-gnss).  The reference is
+ * a Rust crate with no FFI; every entry point below names the Rust function
+ * it replaces (file:line in the reference crate) so that a thin Rust
+ * `extern "C"` shim can bind it.
+ *
+ * Conventions
+ *  - Every function returns an int status (TGA_OK == 0).  Nothing aborts the
+ *    process; on failure tga_last_error() describes the problem.
+ *  - All buffers are caller-allocated.  Pointers named h_* are host memory,
+ *    d_* are device memory on the context's GPU.
+ *  - A context owns one CUDA stream, device scratch buffers and captured
+ *    graphs.  A context is not thread-safe: use one context per host thread
+ *    (contexts on the same device may coexist).
+ *  - Results follow the reference semantics exactly: dual hypothesis
+ *    ([c,c] and [c,-c]) over two code periods, 300 Hz Doppler bins over
+ *    +-search_band, last-maximum tie rule over bins, strict ">" between
+ *    hypotheses, second peak > 1 chip away from the main peak.
+ */
+#ifndef TGA_H
+#define TGA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define TGA_OK 0
+#define TGA_ERR_INVALID_ARG 1   /* bad size, PRN out of range, empty grid ... */
+#define TGA_ERR_CUDA 2          /* a CUDA runtime call failed                  */
+#define TGA_ERR_NO_DEVICE 3     /* no usable sm_100 device                      */
+#define TGA_ERR_OUT_OF_MEMORY 4
+#define TGA_ERR_UNSUPPORTED 5
+#define TGA_ERR_TIMEOUT 6       /* host watchdog expired waiting for the GPU    */
+#define TGA_ERR_CAPACITY 7      /* caller's output buffer is too small          */
+
+/* ---- constellations (order and names of CombinedOutput, lib.rs:32-45) ---- */
+#define TGA_GPS 0      /* GPS L1 C/A, PRN 1-38     (acquisition.rs)  */
+#define TGA_GALILEO 1  /* Galileo E1-C, PRN 1-50   (galileo.rs)      */
+#define TGA_BEIDOU 2   /* BeiDou B1C pilot, 1-63   (beidou.rs)       */
+#define TGA_SBAS 3     /* SBAS L1 C/A, PRN 120-158 (sbas.rs)         */
+#define TGA_L1C 4      /* GPS L1C pilot, PRN 1-63  (l1c.rs)          */
+#define TGA_QZSS 5     /* QZSS L1 C/A, PRN 184-206 (qzss.rs)         */
+#define TGA_N_CONSTELLATIONS 6
+#define TGA_ALL_CONSTELLATIONS 0x3Fu
+
+/* ---- ACR tables (acr_tables.rs) ------------------------------------------ */
+#define TGA_ACR_GPS_L1_CA 0  /* GPS / SBAS / QZSS C/A, 2 ms */
+#define TGA_ACR_GALILEO_E1C 1
+#define TGA_ACR_BEIDOU_B1C 2
+#define TGA_ACR_GPS_L1C 3
+
+typedef struct tga_ctx tga_ctx;
+
+/* Single-antenna, single-PRN result.  Mirrors AcquisitionResult
+ * (acquisition.rs:18-30) and its per-constellation twins, plus the raw
+ * CorrelationPeak fields (correlate.rs:28-38). */
+typedef struct {
+  int32_t prn;
+  int32_t best_freq_idx;      /* CorrelationPeak.best_freq_idx                */
+  int64_t best_codephase;     /* sample index of the peak, in [0, period)     */
+  double signal_strength;     /* CorrelationPeak.best_peak as f64             */
+  double second_peak;         /* CorrelationPeak.second_peak as f64           */
+  double codephase_frac;      /* (best_codephase % period) / period           */
+  double frequency;           /* fc[best_freq_idx] - center_freq (Hz)         */
+  int32_t hypothesis;         /* 0: [c,c] won, 1: [c,-c] won                  */
+  int32_t path;               /* 0: fused polyphase kernels, 1: generic path  */
+} tga_result;
+
+/* One (constellation, antenna, PRN) cell of an all-PRN search.  The per-PRN
+ * vectors of *PrnResult (acquisition.rs:32-59) are these cells grouped by
+ * (constellation, prn) in antenna order. */
+typedef struct {
+  int32_t constellation;
+  int32_t prn;
+  int32_t antenna;
+  int32_t best_freq_idx;
+  int64_t best_codephase;
+  double signal_strength;
+  double second_peak;
+  double codephase_frac;
+  double frequency;
+  double cn0_acr;             /* valid only when cn0_valid != 0                */
+  int32_t cn0_valid;          /* 0 mirrors the `null` entries of cn0_acr      */
+  int32_t hypothesis;
+} tga_cell;
+
+/* Options of an all-PRN search: the arguments of acquire_all_* (for example
+ * acquisition.rs:261-269) shared by all selected constellations. */
+typedef struct {
+  uint32_t constellation_mask;  /* bit TGA_x selects constellation x          */
+  const int32_t* ant_filter;    /* NULL: every antenna (ant_filter == None)   */
+  size_t n_ant_filter;
+  const int32_t* prn_filter;    /* NULL: every PRN of each constellation      */
+  size_t n_prn_filter;
+  double center_freq;           /* reference CLI passes 4.092e6 for all six   */
+  double search_band;           /* reference CLI passes 6000.0 for all six    */
+  int32_t cn0;                  /* estimate ACR C/N0 per antenna (--cn0)      */
+  int32_t debug;                /* per-PRN stderr lines (--debug)             */
+} tga_all_options;
+
+/* ---- context ------------------------------------------------------------- */
+/* Replaces nothing in the reference (its state is a thread-local FftPlanner,
+ * acquisition.rs:201-212, and LazyLock code caches, beidou_codes.rs:89-98). */
+int tga_create(int device, tga_ctx** out);
+int tga_destroy(tga_ctx* ctx);
+const char* tga_last_error(const tga_ctx* ctx);
+const char* tga_version(void);
+
+/* ---- single-PRN search ----------------------------------------------------
+ * Replaces acquire_full (acquisition.rs:176), acquire_sbas (sbas.rs:132),
+ * acquire_qzss (qzss.rs:135), acquire_galileo_single (galileo.rs:133),
+ * acquire_beidou_single (beidou.rs:85) and acquire_l1c_single (l1c.rs:94):
+ * same arguments (host slices of de-meaned f32 samples and f64 phase
+ * points), same AcquisitionResult.  When num_samples == 2 * samples_per_chunk
+ * and the resampled code is a whole number of samples per chip the fused
+ * polyphase kernels run; any other length runs the generic GPU path
+ * (Bluestein FFTs of length num_samples). */
+int tga_acquire_single(tga_ctx* ctx, int constellation, const float* h_signal_f32,
+                       const double* h_phasepoints, size_t num_samples, double sampling_freq,
+                       double center_freq, double search_band, int prn,
+                       size_t samples_per_chunk, tga_result* out);
+int tga_acquire_full(tga_ctx* ctx, const float* h_signal_f32, const double* h_phasepoints,
+                     size_t num_samples, double sampling_freq, double center_freq,
+                     double search_band, int prn, size_t samples_per_chunk, tga_result* out);
+int tga_acquire_sbas(tga_ctx* ctx, const float* h_signal_f32, const double* h_phasepoints,
+                     size_t num_samples, double sampling_freq, double center_freq,
+                     double search_band, int prn, size_t samples_per_chunk, tga_result* out);
+int tga_acquire_qzss(tga_ctx* ctx, const float* h_signal_f32, const double* h_phasepoints,
+                     size_t num_samples, double sampling_freq, double center_freq,
+                     double search_band, int prn, size_t samples_per_chunk, tga_result* out);
+int tga_acquire_galileo_single(tga_ctx* ctx, const float* h_signal_f32,
+                               const double* h_phasepoints, size_t num_samples,
+                               double sampling_freq, double center_freq, double search_band,
+                               int prn, size_t samples_per_chunk, tga_result* out);
+int tga_acquire_beidou_single(tga_ctx* ctx, const float* h_signal_f32,
+                              const double* h_phasepoints, size_t num_samples,
+                              double sampling_freq, double center_freq, double search_band,
+                              int prn, size_t samples_per_chunk, tga_result* out);
+int tga_acquire_l1c_single(tga_ctx* ctx, const float* h_signal_f32, const double* h_phasepoints,
+                           size_t num_samples, double sampling_freq, double center_freq,
+                           double search_band, int prn, size_t samples_per_chunk,
+                           tga_result* out);
+
+/* ---- all-PRN, all-antenna search ------------------------------------------
+ * Replaces acquire_all_gps (acquisition.rs:261), acquire_all_sbas
+ * (sbas.rs:216), acquire_all_qzss (qzss.rs:219), acquire_all_galileo
+ * (galileo.rs:219), acquire_all_beidou (beidou.rs:171), acquire_all_l1c
+ * (l1c.rs:180), and the per-constellation loop of main.rs:719-819.
+ *
+ * Input is the observation's packed 1-bit data exactly as stored in the
+ * HDF5 `data` dataset (observation.rs:62-75): n_ant rows of row_bytes bytes,
+ * MSB-first (numpy.packbits).  The antenna mean is taken over the whole row
+ * (acquisition.rs:285); the search uses the first 2 code periods.
+ *
+ * out receives one tga_cell per (constellation, PRN, antenna), ordered by
+ * constellation (TGA_x order), then PRN in the order searched (prn_filter
+ * order, or ascending), then antenna (ant_filter order).  *n_out is set to
+ * the count; TGA_ERR_CAPACITY if out_capacity is too small (then *n_out is
+ * the required count).
+ *
+ * tga_acquire_all takes host bits and copies them to the device;
+ * tga_acquire_all_device takes bits already resident on the context's GPU. */
+int tga_acquire_all(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, size_t row_bytes,
+                    double sampling_freq, const tga_all_options* opt, tga_cell* out,
+                    size_t out_capacity, size_t* n_out);
+int tga_acquire_all_device(tga_ctx* ctx, const uint8_t* d_packed_bits, size_t n_ant,
+                           size_t row_bytes, double sampling_freq, const tga_all_options* opt,
+                           tga_cell* out, size_t out_capacity, size_t* n_out);
+
+/* Number of cells tga_acquire_all would produce for these options. */
+int tga_all_cell_count(size_t n_ant, const tga_all_options* opt, size_t* n_cells);
+
+/* Search work of the last tga_acquire_all* call on this context:
+ * cells = sum over (constellation, antenna, PRN) of n_bins * period, and the
+ * kernels launched.  Used by benchmarks to report cells/s. */
+int tga_last_search_stats(const tga_ctx* ctx, double* cells, int32_t* kernel_launches,
+                          double* device_ms);
+
+/* ---- ACR C/N0 --------------------------------------------------------------
+ * Replaces estimate_cn0 (acr.rs:49-84) over a batch, on the GPU:
+ * cn0[i] = estimate_cn0(r_a[i], table), valid[i] = 0 where it returns None. */
+int tga_acr_cn0(tga_ctx* ctx, const double* h_r_a, size_t n, int table, double* h_cn0,
+                uint8_t* h_valid);
+
+/* ---- antenna cross-correlation ---------------------------------------------
+ * Replaces Observation::correlate (observation.rs:175-195): zero-lag mean of
+ * the +-1 products of antennas i and j over the whole record, on the GPU. */
+int tga_antenna_xcorr(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant,
+                      size_t row_bytes, int i, int j, double* out);
+/* All n_ant x n_ant pairs at once (row-major out[i*n_ant + j]). */
+int tga_antenna_xcorr_matrix(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant,
+                             size_t row_bytes, double* out);
+
+/* ---- code tables (host) -----------------------------------------------------
+ * +-1 primary chips of one PRN: generate_ca_code (acquisition.rs:130),
+ * generate_sbas_ca_code (sbas.rs:111), generate_qzss_ca_code (qzss.rs:111),
+ * generate_e1c_code (galileo.rs:99), generate_b1c_pilot_code
+ * (beidou_codes.rs:145, BOC(1,1) half-chips) and generate_l1c_pilot_code
+ * (l1c_codes.rs:175, BOC(1,1) half-chips).  Returns the length in *n. */
+int tga_code_chips(int constellation, int prn, int8_t* out, size_t capacity, size_t* n);
+/* The code resampled to num_samples samples: gold_code (acquisition.rs:162),
+ * sbas_gold_code, qzss_gold_code, e1c_code_resampled (galileo.rs:112),
+ * b1c_code_resampled (beidou_codes.rs:166), l1c_code_resampled
+ * (l1c_codes.rs:197). */
+int tga_code_resampled(int constellation, int prn, double samples_per_code,
+                       size_t num_samples, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TGA_H */
