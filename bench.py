@@ -1,0 +1,315 @@
+#!/usr/bin/env python3
+"""Benchmark: acquisition cells/s of the --all search over 24 antennas.
+
+Workload (one "step"): tart-gnss-acquire's `--all` search (GPS, Galileo,
+BeiDou, SBAS, L1C, QZSS: 276 PRNs) with `--cn0`, over 24 antennas of
+synthetic 1-bit data at 16.368 MHz, 100 ms per antenna, reference semantics
+(two code periods coherent, dual [c,c]/[c,-c] hypothesis, 41 x 300 Hz Doppler
+bins around 4.092 MHz).  cells = sum over (antenna, PRN) of n_bins * period.
+
+Synthetic data: 10 satellites per constellation (random PRNs, code phase
+uniform, Doppler uniform +-4 kHz, random +-1 sign per code epoch, C/N0 uniform
+38-50 dB-Hz), unit Gaussian noise, sign-quantised, packed MSB-first; seeded
+(0x5EED2026 + 1 + rank).
+
+Output: one JSON line (rank 0).  `value` is device time with the packed bits
+already in HBM; `e2e` goes through the C ABI (tga_acquire_all) from pinned
+host memory with the H2D copy and the result D2H inside the timed region.
+`--impl reference` times the CPU restatement of the reference algorithm (the
+reference itself is Rust and cannot be built here) on a bounded sample.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tart-gnss_b200"))
+
+FS = 16.368e6
+N_ANT = 24
+SAMPLES = 1636800  # 100 ms
+SEED = 0x5EED2026 + 1
+METRIC = "acq cells/s, --all x 24 ant"
+WORKLOAD = ("--all x 24 ant, 16.368 MHz 1-bit, 100 ms synthetic, 276 PRNs x 41 bins x 300 Hz, "
+            "2-period coherent dual-hypothesis, --cn0")
+
+
+def synth_observation(seed, n_ant=N_ANT, n_samples=SAMPLES, chunk=163680):
+    """Seeded synthetic 1-bit recording (see module docstring)."""
+    import tga
+    rng = np.random.default_rng(seed)
+    sats = []
+    for c in range(6):
+        lo, hi = {0: (1, 38), 1: (1, 50), 2: (1, 63), 3: (120, 158), 4: (1, 63), 5: (184, 206)}[c]
+        P = int(FS / 1000.0) if c in (0, 3, 5) else int(FS * (0.004 if c == 1 else 0.010))
+        for prn in rng.choice(np.arange(lo, hi + 1), size=10, replace=False):
+            code = tga.code_resampled(c, int(prn), float(P), P).astype(np.float32)
+            n_ep = n_samples // P + 2
+            sats.append(dict(c=c, prn=int(prn), P=P, code=code, delay=int(rng.integers(0, P)),
+                             dop=float(rng.uniform(-4000, 4000)), cn0=float(rng.uniform(38, 50)),
+                             flips=rng.choice([-1.0, 1.0], size=n_ep).astype(np.float32)))
+    phase = np.exp(1j * rng.uniform(0, 2 * np.pi, size=(n_ant, len(sats)))).astype(np.complex64)
+    bits = np.empty((n_ant, n_samples // 8), np.uint8)
+    for t0 in range(0, n_samples, chunk):
+        n = min(chunk, n_samples - t0)
+        t = np.arange(t0, t0 + n)
+        U = np.empty((len(sats), n), np.complex64)
+        for k, s in enumerate(sats):
+            amp = 2.0 * math.sqrt(10.0 ** (s["cn0"] / 10.0) / FS)
+            idx = t + s["delay"]
+            chip = s["code"][idx % s["P"]] * s["flips"][idx // s["P"]]
+            ph = (2 * np.pi * ((4.092e6 + s["dop"]) / FS) * t) % (2 * np.pi)
+            U[k] = (amp * chip) * np.exp(1j * ph).astype(np.complex64)
+        v = (phase @ U).real + rng.standard_normal((n_ant, n), dtype=np.float32)
+        bits[:, t0 // 8:(t0 + n) // 8] = np.packbits(v >= 0.0, axis=1)
+    return bits, sats
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        self.path = os.path.join("/tmp", "tga_clocks_%d_%d.csv" % (os.getpid(), index))
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i] and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_sample_baseline(threads, repeats=1):
+    """CPU restatement of the reference algorithm (oracle) on a bounded sample
+    of the same workload: antenna 0, a PRN subset of every constellation, all
+    41 bins.  Returns (cells/s, seconds, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import acq_oracle as O
+    bits, _ = synth_observation(SEED, n_ant=1)
+    ub = np.unpackbits(bits, axis=1)
+    sample = {O.GPS: [1, 2, 3, 4], O.SBAS: [120, 121], O.QZSS: [184], O.GALILEO: [1, 2], O.BEIDOU: [1, 2],
+              O.L1C: [1, 2]}
+    cells = 0.0
+    t0 = time.perf_counter()
+    for _ in range(repeats):
+        for c, prns in sample.items():
+            P = O.period_samples(c, FS)
+            O.acquire_all(ub, FS, c, prn_filter=prns, cn0=True, threads=threads)
+            cells += len(prns) * 41 * P
+    dt = time.perf_counter() - t0
+    desc = ("antenna 0 of the workload, PRNs GPS 1-4, SBAS 120-121, QZSS 184, Galileo 1-2, BeiDou 1-2, "
+            "L1C 1-2, all 41 bins, x%d; numpy/scipy (pocketfft complex64) restatement of correlate_code, "
+            "3 FFTs of 2P per bin as the reference" % repeats)
+    return cells / dt, dt, desc
+
+
+def fp32_peak_tflops(sm_mhz, n_sm=148):
+    return n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    times, vals = [], []
+    for i in range(args.warmup + args.steps):
+        v, dt, desc = cpu_sample_baseline(threads)
+        if i >= args.warmup:
+            times.append(dt)
+            vals.append(v)
+    value = statistics.mean(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "sample": "bounded CPU sample"},
+            "cpu_baseline": {"value": value, "unit": "cells/s", "cores": threads, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import tga
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    bits_np, _ = synth_observation(SEED + rank)
+    n_ant, row_bytes = bits_np.shape
+    pinned = torch.empty((n_ant, row_bytes), dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = bits_np
+    d_bits = pinned.to("cuda", non_blocking=False)
+    ctx = tga.Context(local)
+    stream = torch.cuda.ExternalStream(tga.lib().tga_stream(ctx._h))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    lib = tga.lib()
+    import ctypes
+
+    def step_device():
+        return ctx.acquire_cells(None, FS, mask=tga.ALL, cn0=True, device_bits=d_bits.data_ptr(), n_ant=n_ant,
+                                 row_bytes=row_bytes)
+
+    def kernel_times():
+        cap = 64
+        names = (ctypes.c_char_p * cap)()
+        ms = (ctypes.c_double * cap)()
+        la = (ctypes.c_int32 * cap)()
+        fl = (ctypes.c_double * cap)()
+        n = ctypes.c_int()
+        lib.tga_kernel_times.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        lib.tga_kernel_times(ctx._h, cap, names, ms, la, fl, ctypes.byref(n))
+        return {names[i].decode(): (ms[i], la[i], fl[i]) for i in range(min(n.value, cap))}
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+
+    lib.tga_set_profiling(ctx._h, 1)
+    clk = Clocks(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    total_ms, launches, agg = 0.0, 0, {}
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)  # evict L2 between steps (outside the timed events)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        cells_out = step_device()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        st = ctx.last_stats()
+        launches += st["kernel_launches"]
+        for k, (ms, la, fl) in kernel_times().items():
+            a = agg.setdefault(k, [0.0, 0, 0.0])
+            a[0] += ms
+            a[1] += la
+            a[2] += fl
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    lib.tga_set_profiling(ctx._h, 0)
+    cells = ctx.last_stats()["cells"]
+    ms_step = total_ms / args.steps
+    if world > 1:
+        t = torch.tensor([ms_step], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+        dist.barrier()
+    value = cells * world / (ms_step / 1e3)
+
+    # end to end through the C ABI from pinned host memory
+    host = pinned.numpy()
+    e2e_times = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.acquire_cells(host, FS, mask=tga.ALL, cn0=True)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_times.append(dt)
+    h2d, d2h = ctypes.c_uint64(), ctypes.c_uint64()
+    lib.tga_last_transfer_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
+                                            ctypes.POINTER(ctypes.c_uint64)]
+    lib.tga_last_transfer_bytes(ctx._h, ctypes.byref(h2d), ctypes.byref(d2h))
+    e2e_s = statistics.mean(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    # roofline of the dominant kernel (FP32 SIMT pipe)
+    dom = max(agg.items(), key=lambda kv: kv[1][0])
+    dname, (dms, dl, dfl) = dom
+    avg_launch_s = dms / dl / 1e3
+    achieved = dfl / dl / avg_launch_s / 1e12
+    sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    peak = fp32_peak_tflops(sm_mhz)
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(dname.split("[")[0], {}).get("bytes_per_launch")
+
+    line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_ant": n_ant, "cells_per_step_per_gpu": cells,
+                       "l2": "256 MB buffer written between timed steps; 3.9 GB intermediate per step",
+                       "parallelism": "replicas (weak scaling: one 24-antenna observation per GPU)"},
+            "e2e": {"value": cells * world / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": h2d.value,
+                    "d2h_bytes_per_step": d2h.value, "ms_per_step": e2e_s * 1e3},
+            "gpu_launches": launches,
+            "roofline": {"bound": "fp32", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": "148 SM x 128 FP32 lanes x 2 flop x median SM clock under load "
+                                        "(%.0f MHz); MEASURED_PEAKS.json has no FP32 SIMT figure" % sm_mhz,
+                         "flops_per_launch": dfl / dl, "avg_launch_ms": dms / dl},
+            "kernels": {k: {"ms_per_step": v[0] / args.steps, "share": v[0] / sum(x[0] for x in agg.values()),
+                            "launches_per_step": v[1] / args.steps} for k, v in agg.items()},
+            "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, dt, desc = cpu_sample_baseline(os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": v, "unit": "cells/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": desc, "seconds": dt}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -182,6 +182,17 @@ int tga_all_cell_count(size_t n_ant, const tga_all_options* opt, size_t* n_cells
  * kernels launched.  Used by benchmarks to report cells/s. */
 int tga_last_search_stats(const tga_ctx* ctx, double* cells, int32_t* kernel_launches,
                           double* device_ms);
+/* Host<->device bytes moved by the last call (inputs in, results out). */
+int tga_last_transfer_bytes(const tga_ctx* ctx, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
+/* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a
+ * caller can time calls with CUDA events on it. */
+void* tga_stream(tga_ctx* ctx);
+/* Per-kernel device timing of later calls (CUDA events around each launch,
+ * on the context stream).  tga_kernel_times returns, for the last call, up
+ * to cap entries of (kernel name, total ms, launches, algorithmic FLOPs). */
+int tga_set_profiling(tga_ctx* ctx, int enable);
+int tga_kernel_times(const tga_ctx* ctx, int cap, const char** names, double* ms,
+                     int32_t* launches, double* flops, int* n);
 
 /* ---- ACR C/N0 --------------------------------------------------------------
  * Replaces estimate_cn0 (acr.rs:49-84) over a batch, on the GPU:

@@ -203,19 +203,37 @@ def _bin_work(sig, pp, freq, cc, cc_alt, ft, ct):
     n = len(sig)
     scale = ft(1.0) / np.sqrt(ft(n))
     best = None
+    corrs = []
     for hyp, rep in enumerate((cc, cc_alt)):
         prod = spec * rep
         corr = (np.abs(sfft.ifft(prod, norm="forward")) * scale).astype(ft)
+        corrs.append(corr)
         idx = _last_argmax(corr)
         val = corr[idx]
         if best is None or val > best[1]:
             best = (idx, val, corr, hyp)
-    return best
+    return best + (corrs[1 - best[3]],)
 
 
-def correlate_code(sig, pp, cc, cc_alt, fc, num_samples, period, fs, precision="f32", threads=1):
+def _fold_grid(res, period):
+    """Per bin, the larger of the two hypotheses' |corr| at each code phase
+    (index mod period).  Used by the parity tests to recognise exact ties,
+    where the reference's own choice depends on FP rounding order."""
+    rows = []
+    for r in res:
+        c = np.asarray(r[2], dtype=np.float64)
+        other = np.asarray(r[4], dtype=np.float64)
+        m = np.maximum(c, other)
+        g = np.full(period, -np.inf)
+        idx = np.arange(len(m)) % period
+        np.maximum.at(g, idx, m)
+        rows.append(g)
+    return np.array(rows)
+
+
+def correlate_code(sig, pp, cc, cc_alt, fc, num_samples, period, fs, precision="f32", threads=1, grid=False):
     """correlate.rs:91-183.  Returns dict(best_peak, second_peak, best_freq_idx,
-    best_codephase, hypothesis)."""
+    best_codephase, hypothesis[, grid])."""
     if len(fc) == 0:
         raise ValueError("frequency bin list must be non-empty")
     ft, ct = _types(precision)
@@ -226,7 +244,7 @@ def correlate_code(sig, pp, cc, cc_alt, fc, num_samples, period, fs, precision="
         res = [_bin_work(sig, pp, f, cc, cc_alt, ft, ct) for f in fc]
     vals = np.array([r[1] for r in res])
     bi = _last_argmax(vals)
-    idx, peak, corr, hyp = res[bi]
+    idx, peak, corr, hyp, _ = res[bi]
     chip_width = int(math.ceil(fs / 1.023e6))
     main = idx % period
     icp = np.arange(len(corr)) % period
@@ -236,23 +254,29 @@ def correlate_code(sig, pp, cc, cc_alt, fc, num_samples, period, fs, precision="
     second = ft(cand.max()) if len(cand) else ft(-np.inf)
     if second <= 0.0:
         second = ft(1e-6)
-    return dict(best_peak=ft(peak), second_peak=ft(second), best_freq_idx=bi,
-                best_codephase=int(idx), hypothesis=hyp)
+    out = dict(best_peak=ft(peak), second_peak=ft(second), best_freq_idx=bi,
+               best_codephase=int(idx), hypothesis=hyp)
+    if grid:
+        out["grid"] = _fold_grid(res, period)
+    return out
 
 
 def acquire_single(constellation, sig, pp, fs, center_freq, search_band, prn, period,
-                   precision="f32", threads=1):
+                   precision="f32", threads=1, grid=False):
     """acquire_full (acquisition.rs:176-248) and its five twins."""
     n = len(sig)
     fc = freq_grid(center_freq, search_band)
     code = resampled_code(constellation, prn, float(period), n)
     cc, cc_alt = code_spectra(code, period, precision)
     pk = correlate_code(np.asarray(sig, np.float32), np.asarray(pp, np.float64), cc, cc_alt, fc, n,
-                        period, fs, precision, threads)
+                        period, fs, precision, threads, grid)
     cp = pk["best_codephase"] % period
-    return dict(prn=prn, signal_strength=float(pk["best_peak"]), second_peak=float(pk["second_peak"]),
-                codephase_frac=cp / float(period), frequency=float(fc[pk["best_freq_idx"]] - center_freq),
-                best_freq_idx=pk["best_freq_idx"], best_codephase=cp, hypothesis=pk["hypothesis"])
+    out = dict(prn=prn, signal_strength=float(pk["best_peak"]), second_peak=float(pk["second_peak"]),
+               codephase_frac=cp / float(period), frequency=float(fc[pk["best_freq_idx"]] - center_freq),
+               best_freq_idx=pk["best_freq_idx"], best_codephase=cp, hypothesis=pk["hypothesis"])
+    if grid:
+        out["grid"] = pk["grid"]
+    return out
 
 
 def period_samples(constellation, fs):
@@ -263,7 +287,7 @@ def period_samples(constellation, fs):
 
 
 def acquire_all(bits, fs, constellation, center_freq=GNSS_IF, search_band=SEARCH_BAND,
-                ant_filter=None, prn_filter=None, cn0=False, precision="f32", threads=1):
+                ant_filter=None, prn_filter=None, cn0=False, precision="f32", threads=1, grid=False):
     """acquire_all_* (acquisition.rs:261-396).  bits: [n_ant, n_samples] 0/1."""
     bits = np.asarray(bits)
     period = period_samples(constellation, fs)
@@ -275,7 +299,7 @@ def acquire_all(bits, fs, constellation, center_freq=GNSS_IF, search_band=SEARCH
     results = []
     for prn in prns:
         cells = [acquire_single(constellation, s, p, fs, center_freq, search_band, prn, period,
-                                precision, threads) for (s, p) in ant_data]
+                                precision, threads, grid) for (s, p) in ant_data]
         strengths = [c["signal_strength"] for c in cells]
         seconds = [c["second_peak"] for c in cells]
         phases = [c["codephase_frac"] for c in cells]

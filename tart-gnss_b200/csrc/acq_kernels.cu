@@ -1,0 +1,688 @@
+// CUDA kernels of the B200 acquisition engine (sm_100a).
+//
+// Fused path.  For a window of two code periods (N = 2P) the reference's
+// dual-hypothesis correlation (correlate.rs:91-183) is rewritten exactly:
+//
+//  1. Fold:  f = x[0:P] + x[P:2P] gives the [c,c] correlation; the [c,-c]
+//     correlation is the negacyclic correlation of g = x[0:P] - x[P:2P].
+//  2. Polyphase: the resampled code is c(n) = chip((n / S) mod Lc) * pulse(n % S)
+//     (S samples per chip, P = S * Lc).  Then for every lag tau = rho + S*t
+//        r(tau) = sum_m chip(m) z_rho(m + t),   z_rho(j) = sum_s pulse(s) f(S j + rho + s)
+//     i.e. S independent circular correlations of length Lc (the chip count,
+//     1023 / 4092 / 10230) instead of one of length 2P.  The negacyclic
+//     branch is made cyclic by the twist v(j) = exp(i pi j / Lc).
+//  3. Every Lc is 31 * 33 * M (M = 1, 4, 10), pairwise coprime, so each
+//     length-Lc DFT is a twiddle-free Good-Thomas transform: a DFT-31 stage
+//     fed straight from global memory (Z * conj(D) formed in registers), a
+//     DFT-33 stage and a DFT-M stage through shared memory.  The last stage
+//     feeds |y|^2 straight into the argmax; no correlation vector ever
+//     leaves the SM.
+//
+// Frequency-domain arrays use the digit layout [k31][kM][k33]; time-domain
+// lag digits map to natural lags by the Chinese remainder theorem.
+//
+// Generic path (any N): the reference algorithm on the GPU, with Bluestein
+// FFTs of length N built on a power-of-two Stockham FFT.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+
+#include "dft.cuh"
+#include "engine.h"
+#include "gnss_tables.h"
+
+namespace tga {
+
+static int g_launches = 0;
+int kernel_launch_count_reset() {
+  int v = g_launches;
+  g_launches = 0;
+  return v;
+}
+int kernel_launch_count() { return g_launches; }
+void kernel_launch_add(int n) { g_launches += n; }
+
+#define TGA_LAUNCHED() (++g_launches, cudaGetLastError())
+
+constexpr int modinv_c(int a, int m) {
+  a %= m;
+  for (int x = 1; x < m; ++x)
+    if ((a * x) % m == 1) return x;
+  return 0;
+}
+
+// Geometry of the Lc = 31 * 33 * M prime-factor transform.
+template <int M>
+struct Geo {
+  static constexpr int NC = M;
+  static constexpr int COLS = 33 * M;  // columns of the DFT-31 stage
+  static constexpr int LC = 31 * COLS;
+  // natural index n = (a*EA + b*EB + c*EC) mod LC for digits (a, b, c)
+  static constexpr int EA = (LC / 31) * modinv_c((LC / 31) % 31, 31);
+  static constexpr int EB = (LC / 33) * modinv_c((LC / 33) % 33, 33);
+  static constexpr int EC = (M == 1) ? 0 : (LC / M) * modinv_c((LC / M) % M, M);
+  __device__ static __forceinline__ int natural(int a, int b, int c) {
+    return (int)((unsigned)(a * EA + b * EB + c * EC) % (unsigned)LC);
+  }
+  // digit-layout offset of (a, b, c): [a][c][b]
+  __device__ static __forceinline__ int offset(int a, int b, int c) { return a * COLS + c * 33 + b; }
+};
+
+// ---------------------------------------------------------------------------
+// antenna means: mean of the +-1 samples over the whole row (acquisition.rs:285)
+// ---------------------------------------------------------------------------
+__global__ void antenna_means_kernel(const uint8_t* __restrict__ bits, size_t row_bytes,
+                                     double* __restrict__ mean) {
+  const uint8_t* row = bits + (size_t)blockIdx.x * row_bytes;
+  unsigned long long ones = 0;
+  const size_t n_words = row_bytes / 8;
+  const bool aligned = (((uintptr_t)row) & 7) == 0;
+  if (aligned) {
+    const unsigned long long* w = reinterpret_cast<const unsigned long long*>(row);
+    for (size_t i = threadIdx.x; i < n_words; i += blockDim.x) ones += __popcll(__ldg(w + i));
+    for (size_t i = n_words * 8 + threadIdx.x; i < row_bytes; i += blockDim.x) ones += __popc(row[i]);
+  } else {
+    for (size_t i = threadIdx.x; i < row_bytes; i += blockDim.x) ones += __popc(row[i]);
+  }
+  for (int o = 16; o > 0; o >>= 1) ones += __shfl_xor_sync(0xffffffffu, ones, o);
+  __shared__ unsigned long long part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = ones;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += part[i];
+    const double n = (double)(row_bytes * 8);
+    // sum of +-1 over the row is the exact integer 2*ones - n
+    mean[blockIdx.x] = (double)(2.0 * (double)t - n) / n;
+  }
+}
+
+cudaError_t launch_antenna_means(const uint8_t* d_bits, int n_rows, size_t row_bytes, double* d_mean,
+                                 cudaStream_t st) {
+  if (n_rows <= 0) return cudaSuccess;
+  antenna_means_kernel<<<n_rows, 256, 0, st>>>(d_bits, row_bytes, d_mean);
+  return TGA_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------
+// front end: carrier wipe-off (correlate.rs:110-115), fold, polyphase boxcar
+// ---------------------------------------------------------------------------
+struct FrontParams {
+  SampleSource src;
+  const double* fc;
+  int nb, P, S, Lc;
+  float pulse[kMaxPulse];
+  float2* z;
+};
+
+constexpr int kFrontJ = 64;  // chips per CTA
+
+template <bool BITS>
+__device__ __forceinline__ float2 wipe(const FrontParams& p, int row, int n, double f) {
+  float s;
+  double ph_d;
+  if (BITS) {
+    const uint8_t byte = __ldg(p.src.bits + (size_t)row * p.src.row_bytes + (n >> 3));
+    const double v = ((byte >> (7 - (n & 7))) & 1) ? 1.0 : -1.0;
+    s = (float)(v - __ldg(p.src.mean + row));        // (v - mean) as f32
+    ph_d = (p.src.pc * (double)n) * f;                // phasepoint * freq
+  } else {
+    s = __ldg(p.src.sig + (size_t)row * p.src.n_samples + n);
+    ph_d = __ldg(p.src.pp + n) * f;
+  }
+  const float ph = __double2float_rn(ph_d);           // (p * freq) as f32
+  float sn, cs;
+  sincosf(ph, &sn, &cs);
+  return make_float2(cs * s, sn * s);
+}
+
+template <bool BITS>
+__global__ void __launch_bounds__(256) frontend_kernel(FrontParams p) {
+  extern __shared__ float2 fsm[];
+  const int S = p.S, P = p.P, Lc = p.Lc;
+  const int ab = blockIdx.y;
+  const int ant_slot = ab / p.nb, bin = ab - ant_slot * p.nb;
+  const int row = p.src.ant[ant_slot];
+  const double f = p.fc[bin];
+  const int j0 = blockIdx.x * kFrontJ;
+  const int nj = min(kFrontJ, Lc - j0);
+  const int cnt = nj * S + S - 1;
+  const int span = kFrontJ * S + S;
+  float2* fsh = fsm;                         // padded: index i + i/S
+  float2* gsh = fsm + span + span / S + 1;
+  float2* tw = gsh + span + span / S + 1;    // twist per chip
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+    int m = S * j0 + i;
+    float sign = 1.f;
+    if (m >= P) {  // wrap of the last chip: f is P-periodic, g antiperiodic
+      m -= P;
+      sign = -1.f;
+    }
+    const float2 x0 = wipe<BITS>(p, row, m, f);
+    const float2 x1 = wipe<BITS>(p, row, m + P, f);
+    const int pi = i + i / S;
+    fsh[pi] = cadd(x0, x1);
+    const float2 g = csub(x0, x1);
+    gsh[pi] = make_float2(g.x * sign, g.y * sign);
+  }
+  for (int jj = threadIdx.x; jj < nj; jj += blockDim.x) {
+    double sn, cs;
+    sincospi((double)(j0 + jj) / (double)Lc, &sn, &cs);
+    tw[jj] = make_float2((float)cs, (float)sn);
+  }
+  __syncthreads();
+  const size_t seqA = ((size_t)ab * 2 + 0) * S, seqB = ((size_t)ab * 2 + 1) * S;
+  for (int o = threadIdx.x; o < S * nj; o += blockDim.x) {
+    const int rho = o / nj, jj = o - rho * nj;
+    float2 za = make_float2(0.f, 0.f), zb = make_float2(0.f, 0.f);
+    const int base = jj * S + rho;
+    for (int s = 0; s < S; ++s) {
+      const int i = base + s, pi = i + i / S;
+      const float w = p.pulse[s];
+      za.x = fmaf(w, fsh[pi].x, za.x);
+      za.y = fmaf(w, fsh[pi].y, za.y);
+      zb.x = fmaf(w, gsh[pi].x, zb.x);
+      zb.y = fmaf(w, gsh[pi].y, zb.y);
+    }
+    const int j = j0 + jj;
+    p.z[(seqA + rho) * Lc + j] = za;
+    p.z[(seqB + rho) * Lc + j] = cmul(zb, tw[jj]);
+  }
+}
+
+cudaError_t launch_frontend(const SampleSource& src, const SearchDims& dims, const PolyClass& pc,
+                            float2* d_z, cudaStream_t st) {
+  FrontParams p;
+  p.src = src;
+  p.fc = dims.fc;
+  p.nb = dims.nb;
+  p.P = pc.P;
+  p.S = pc.S;
+  p.Lc = pc.Lc;
+  for (int i = 0; i < kMaxPulse; ++i) p.pulse[i] = pc.pulse[i];
+  p.z = d_z;
+  const int span = kFrontJ * pc.S + pc.S;
+  const size_t smem = (size_t)(2 * (span + span / pc.S + 1) + kFrontJ) * sizeof(float2);
+  dim3 grid((pc.Lc + kFrontJ - 1) / kFrontJ, dims.n_ant * dims.nb);
+  if (src.bits) {
+    cudaFuncSetAttribute(frontend_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    frontend_kernel<true><<<grid, 256, smem, st>>>(p);
+  } else {
+    cudaFuncSetAttribute(frontend_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    frontend_kernel<false><<<grid, 256, smem, st>>>(p);
+  }
+  return TGA_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------
+// prime-factor transform engine
+// ---------------------------------------------------------------------------
+enum PfaMode { FWD_Z = 0, FWD_D = 1, CORR = 2, SECOND = 3 };
+
+struct PfaParams {
+  float2* z;                  // FWD_Z: sequences, transformed in place; CORR/SECOND: Z
+  const float2* D;            // CORR/SECOND: conjugated code spectra
+  float2* Dout;               // FWD_D output
+  const int8_t* chips;        // FWD_D input [n_prn][Lc]
+  int n_seq;                  // FWD modes
+  int n_items;                // CORR: n_ab*2*n_prn rows; SECOND: n_ant*n_prn
+  int n_prn, S, P, chip_width;
+  unsigned long long* keys;   // CORR output, one per row
+  BestRow* best;              // SECOND in/out
+};
+
+template <int M, int BC, int NT, int MODE>
+__global__ void __launch_bounds__(NT, 2) pfa_kernel(PfaParams p) {
+  using G = Geo<M>;
+  constexpr int COLS = G::COLS, LC = G::LC, NC = G::NC;
+  constexpr bool INV = (MODE == CORR || MODE == SECOND);
+  extern __shared__ float2 buf[];
+  __shared__ unsigned long long s_key;
+  __shared__ unsigned int s_p2;
+  const int tid = threadIdx.x;
+  const int S = p.S;
+  const int groups = INV ? (S + BC - 1) / BC : 1;
+  const int n_work = INV ? p.n_items : (p.n_seq + BC - 1) / BC;
+
+  for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
+    int ab_h = 0, prn = 0, tau_star = 0;
+    if (MODE == CORR) {
+      ab_h = w / p.n_prn;
+      prn = w - ab_h * p.n_prn;
+    } else if (MODE == SECOND) {
+      const BestRow b = p.best[w];
+      ab_h = b.ab * 2 + b.hyp;
+      prn = w % p.n_prn;
+      tau_star = b.tau;
+    }
+    const int hyp = ab_h & 1;
+    unsigned long long kbest = 0ull;
+    float pbest = 0.f;
+    if (tid == 0) {
+      s_key = 0ull;
+      s_p2 = 0u;
+    }
+
+    for (int g = 0; g < groups; ++g) {
+      // sequence of slot s in this group, or -1 when idle
+      auto seq_of = [&](int s) -> int {
+        if (INV) {
+          const int rho = g * BC + s;
+          return rho < S ? rho : -1;
+        }
+        const int q = w * BC + s;
+        return q < p.n_seq ? q : -1;
+      };
+      // epilogue for output (s, a, b, c)
+      auto epilogue = [&](int s, int a, int b, int c, float2 v) {
+        if (MODE == FWD_Z) {
+          p.z[(size_t)seq_of(s) * LC + G::offset(a, b, c)] = v;
+        } else if (MODE == FWD_D) {
+          p.Dout[(size_t)seq_of(s) * LC + G::offset(a, b, c)] = make_float2(v.x, -v.y);
+        } else {
+          const float pw = fmaf(v.x, v.x, v.y * v.y);
+          const int tau = seq_of(s) + S * G::natural(a, b, c);
+          if (MODE == CORR) {
+            const unsigned long long key =
+                ((unsigned long long)__float_as_uint(pw) << 32) | (unsigned)tau;
+            kbest = key > kbest ? key : kbest;
+          } else {
+            int d = tau - tau_star;
+            d = d < 0 ? -d : d;
+            const int dist = min(d, p.P - d);
+            if (dist > p.chip_width) pbest = fmaxf(pbest, pw);
+          }
+        }
+      };
+
+      // ---- stage 1: DFT-31 over digit a, input straight from global ----
+      for (int u = tid; u < BC * COLS; u += NT) {
+        const int s = u / COLS, col = u - s * COLS;
+        const int q = seq_of(s);
+        if (q < 0) continue;
+        float2 x[31];
+        if (MODE == CORR || MODE == SECOND) {
+          const float2* zs = p.z + ((size_t)ab_h * S + q) * LC + col;
+          const float2* ds = p.D + ((size_t)prn * 2 + hyp) * LC + col;
+#pragma unroll
+          for (int a = 0; a < 31; ++a) x[a] = cmul(__ldg(zs + a * COLS), __ldg(ds + a * COLS));
+        } else if (MODE == FWD_Z) {
+          const float2* zs = p.z + (size_t)q * LC;
+          const int c = col / 33, b = col - c * 33;
+#pragma unroll
+          for (int a = 0; a < 31; ++a) x[a] = zs[G::natural(a, b, c)];
+        } else {
+          const int pr = q >> 1, hb = q & 1;
+          const int8_t* ch = p.chips + (size_t)pr * LC;
+          const int c = col / 33, b = col - c * 33;
+#pragma unroll
+          for (int a = 0; a < 31; ++a) {
+            const int n = G::natural(a, b, c);
+            const float v = (float)__ldg(ch + n);
+            if (hb) {
+              double sn, cs;
+              sincospi((double)n / (double)LC, &sn, &cs);
+              x[a] = make_float2(v * (float)cs, v * (float)sn);
+            } else {
+              x[a] = make_float2(v, 0.f);
+            }
+          }
+        }
+        float2* dst = buf + s * LC + col;
+        dft_odd<31, INV>(x, [&](int ta, float2 v) { dst[ta * COLS] = v; });
+      }
+      __syncthreads();
+
+      // ---- stage 2: DFT-33 over digit b ----
+      for (int u = tid; u < BC * 31 * NC; u += NT) {
+        const int s = u / (31 * NC), r = u - s * 31 * NC;
+        const int a = r / NC, c = r - a * NC;
+        if (seq_of(s) < 0) continue;
+        float2* base = buf + s * LC + a * COLS + c * 33;
+        float2 x[33];
+#pragma unroll
+        for (int b = 0; b < 33; ++b) x[b] = base[b];
+        if constexpr (NC == 1) {
+          dft33<INV>(x, [&](int tb, float2 v) { epilogue(s, a, tb, 0, v); });
+        } else {
+          dft33<INV>(x, [&](int tb, float2 v) { base[tb] = v; });
+        }
+      }
+
+      // ---- stage 3: DFT-M over digit c ----
+      if constexpr (NC > 1) {
+        __syncthreads();
+        for (int u = tid; u < BC * 1023; u += NT) {
+          const int s = u / 1023, gi = u - s * 1023;
+          const int a = gi / 33, b = gi - a * 33;
+          if (seq_of(s) < 0) continue;
+          const float2* base = buf + s * LC + a * COLS + b;
+          float2 x[NC];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) x[c] = base[c * 33];
+          dft_small<NC, INV>(x, [&](int tc, float2 v) { epilogue(s, a, b, tc, v); });
+        }
+      }
+      __syncthreads();
+    }
+
+    if (MODE == CORR) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, kbest, o);
+        kbest = other > kbest ? other : kbest;
+      }
+      if ((tid & 31) == 0) atomicMax(&s_key, kbest);
+      __syncthreads();
+      if (tid == 0) p.keys[w] = s_key;
+    } else if (MODE == SECOND) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) pbest = fmaxf(pbest, __shfl_xor_sync(0xffffffffu, pbest, o));
+      if ((tid & 31) == 0) atomicMax(&s_p2, __float_as_uint(pbest));
+      __syncthreads();
+      if (tid == 0) p.best[w].p2 = __uint_as_float(s_p2);
+    }
+    __syncthreads();
+  }
+}
+
+// Launch configuration per third digit M: (slots per CTA, threads per CTA).
+template <int M>
+struct PfaCfg;
+template <>
+struct PfaCfg<1> {
+  static constexpr int BC = 8, NT = 288;  // 8 x 33 DFT-31 columns
+};
+template <>
+struct PfaCfg<4> {
+  static constexpr int BC = 2, NT = 288;  // 2 x 132 columns
+};
+template <>
+struct PfaCfg<10> {
+  static constexpr int BC = 1, NT = 352;  // 330 columns
+};
+
+template <int M, int MODE>
+static cudaError_t run_pfa(const PfaParams& p, int n_work, int num_sms, cudaStream_t st) {
+  using C = PfaCfg<M>;
+  constexpr int LC = Geo<M>::LC;
+  const size_t smem = (size_t)C::BC * LC * sizeof(float2);
+  auto kern = pfa_kernel<M, C::BC, C::NT, MODE>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, smem);
+  if (per_sm < 1) per_sm = 1;
+  int grid = num_sms * per_sm;
+  if (grid > n_work) grid = n_work;
+  if (grid < 1) return cudaSuccess;
+  kern<<<grid, C::NT, smem, st>>>(p);
+  return TGA_LAUNCHED();
+}
+
+template <int MODE>
+static cudaError_t dispatch_pfa(int M, const PfaParams& p, int n_work, int num_sms, cudaStream_t st) {
+  switch (M) {
+    case 1: return run_pfa<1, MODE>(p, n_work, num_sms, st);
+    case 4: return run_pfa<4, MODE>(p, n_work, num_sms, st);
+    case 10: return run_pfa<10, MODE>(p, n_work, num_sms, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_forward_z(const PolyClass& pc, int n_ab, float2* d_z, int num_sms, cudaStream_t st) {
+  PfaParams p = {};
+  p.z = d_z;
+  p.n_seq = n_ab * 2 * pc.S;
+  p.S = pc.S;
+  p.P = pc.P;
+  const int bc = pc.M == 1 ? PfaCfg<1>::BC : pc.M == 4 ? PfaCfg<4>::BC : PfaCfg<10>::BC;
+  return dispatch_pfa<FWD_Z>(pc.M, p, (p.n_seq + bc - 1) / bc, num_sms, st);
+}
+
+cudaError_t launch_code_spectra(const PolyClass& pc, const int8_t* d_chips, int n_prn, float2* d_D,
+                                int num_sms, cudaStream_t st) {
+  PfaParams p = {};
+  p.chips = d_chips;
+  p.Dout = d_D;
+  p.n_seq = n_prn * 2;
+  p.S = pc.S;
+  p.P = pc.P;
+  const int bc = pc.M == 1 ? PfaCfg<1>::BC : pc.M == 4 ? PfaCfg<4>::BC : PfaCfg<10>::BC;
+  return dispatch_pfa<FWD_D>(pc.M, p, (p.n_seq + bc - 1) / bc, num_sms, st);
+}
+
+cudaError_t launch_correlate(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
+                             const float2* d_D, unsigned long long* d_keys, int num_sms,
+                             cudaStream_t st) {
+  PfaParams p = {};
+  p.z = const_cast<float2*>(d_Z);
+  p.D = d_D;
+  p.keys = d_keys;
+  p.n_prn = dims.n_prn;
+  p.S = pc.S;
+  p.P = pc.P;
+  p.n_items = dims.n_ant * dims.nb * 2 * dims.n_prn;
+  return dispatch_pfa<CORR>(pc.M, p, p.n_items, num_sms, st);
+}
+
+cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
+                               const float2* d_D, BestRow* d_best, int chip_width, int num_sms,
+                               cudaStream_t st) {
+  PfaParams p = {};
+  p.z = const_cast<float2*>(d_Z);
+  p.D = d_D;
+  p.best = d_best;
+  p.n_prn = dims.n_prn;
+  p.S = pc.S;
+  p.P = pc.P;
+  p.chip_width = chip_width;
+  p.n_items = dims.n_ant * dims.n_prn;
+  return dispatch_pfa<SECOND>(pc.M, p, p.n_items, num_sms, st);
+}
+
+// ---------------------------------------------------------------------------
+// reduction over hypotheses and Doppler bins (correlate.rs:125-154)
+// ---------------------------------------------------------------------------
+__global__ void reduce_bins_kernel(int n_ant, int nb, int n_prn, const unsigned long long* __restrict__ keys,
+                                   BestRow* __restrict__ best) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_ant * n_prn) return;
+  const int ant = i / n_prn, prn = i - ant * n_prn;
+  float pb = -1.f;
+  unsigned long long kb = 0ull;
+  int hb = 0, bb = 0;
+  for (int bin = 0; bin < nb; ++bin) {
+    const size_t ab = (size_t)ant * nb + bin;
+    const unsigned long long ka = keys[(ab * 2 + 0) * n_prn + prn];
+    const unsigned long long kB = keys[(ab * 2 + 1) * n_prn + prn];
+    const float pa = __uint_as_float((unsigned)(ka >> 32)), pB = __uint_as_float((unsigned)(kB >> 32));
+    // hypotheses: [c,-c] replaces [c,c] only when strictly stronger
+    const bool useB = pB > pa;
+    const float pr = useB ? pB : pa;
+    // bins: Iterator::max_by keeps the last maximum
+    if (bin == 0 || pr >= pb) {
+      pb = pr;
+      kb = useB ? kB : ka;
+      hb = useB ? 1 : 0;
+      bb = bin;
+    }
+  }
+  BestRow r;
+  r.ab = ant * nb + bb;
+  r.hyp = hb;
+  r.tau = (int)(unsigned)(kb & 0xffffffffull);
+  r.p = pb;
+  r.p2 = 0.f;
+  best[i] = r;
+}
+
+cudaError_t launch_reduce_bins(const SearchDims& dims, const unsigned long long* d_keys, BestRow* d_best,
+                               cudaStream_t st) {
+  const int n = dims.n_ant * dims.n_prn;
+  if (n <= 0) return cudaSuccess;
+  reduce_bins_kernel<<<(n + 127) / 128, 128, 0, st>>>(dims.n_ant, dims.nb, dims.n_prn, d_keys, d_best);
+  return TGA_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------
+// ACR C/N0 (acr.rs:49-84) and result finalisation (acquisition.rs:237-247)
+// ---------------------------------------------------------------------------
+__constant__ double kAcrGps[59][2];
+__constant__ double kAcrGal[71][2];
+__constant__ double kAcrBds[79][2];
+__constant__ double kAcrL1c[79][2];
+static bool g_acr_uploaded[64] = {};
+
+static cudaError_t upload_acr_tables() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && g_acr_uploaded[dev]) return cudaSuccess;
+  cudaError_t e = cudaMemcpyToSymbol(kAcrGps, TGA_GPS_L1_CA_ACR_TABLE, sizeof(kAcrGps));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(kAcrGal, TGA_GALILEO_E1C_ACR_TABLE, sizeof(kAcrGal));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(kAcrBds, TGA_BEIDOU_B1C_ACR_TABLE, sizeof(kAcrBds));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(kAcrL1c, TGA_GPS_L1C_ACR_TABLE, sizeof(kAcrL1c));
+  if (e == cudaSuccess && dev >= 0 && dev < 64) g_acr_uploaded[dev] = true;
+  return e;
+}
+
+__device__ bool estimate_cn0_dev(double r_a, int table, double* out) {
+  const double(*t)[2];
+  int n;
+  switch (table) {
+    case 0: t = kAcrGps; n = 59; break;
+    case 1: t = kAcrGal; n = 71; break;
+    case 2: t = kAcrBds; n = 79; break;
+    default: t = kAcrL1c; n = 79; break;
+  }
+  if (!(r_a > 1.0) || !isfinite(r_a)) return false;
+  if (r_a <= t[0][0]) { *out = t[0][1]; return true; }
+  if (r_a >= t[n - 1][0]) { *out = t[n - 1][1]; return true; }
+  int lo = 0, hi = n;  // first index with r >= r_a
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (t[mid][0] < r_a) lo = mid + 1; else hi = mid;
+  }
+  if (lo == 0) { *out = t[0][1]; return true; }
+  if (lo >= n) { *out = t[n - 1][1]; return true; }
+  const double la = log(t[lo - 1][0]), lb = log(t[lo][0]);
+  const double tt = (log(r_a) - la) / (lb - la);
+  double v = t[lo - 1][1] + tt * (t[lo][1] - t[lo - 1][1]);
+  v = v < 20.0 ? 20.0 : (v > 70.0 ? 70.0 : v);
+  *out = v;
+  return true;
+}
+
+__global__ void finalize_kernel(int n_cells, int nb, int n_prn, int P, int Lc, const double* __restrict__ fc,
+                                double center, const BestRow* __restrict__ best, int table, int want_cn0,
+                                CellOut* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_cells) return;
+  const BestRow b = best[i];
+  const double scale = sqrt(2.0 * (double)P) / (double)Lc;
+  const float vm = (float)(sqrt((double)b.p) * scale);
+  float vs = (float)(sqrt((double)fmaxf(b.p2, 0.f)) * scale);
+  if (vs <= 0.f) vs = 1e-6f;  // correlate.rs:173-175
+  const int bin = b.ab % nb;
+  CellOut o;
+  o.strength = (double)vm;
+  o.second = (double)vs;
+  o.codephase_frac = (double)b.tau / (double)P;
+  o.frequency = fc[bin] - center;
+  o.bin = bin;
+  o.tau = b.tau;
+  o.hyp = b.hyp;
+  o.cn0 = 0.0;
+  o.cn0_valid = 0;
+  if (want_cn0) {
+    const double m = o.strength, s = o.second;
+    if (s > 0.0 && m > s) {
+      const double q = m / s;
+      double c;
+      if (estimate_cn0_dev(q * q, table, &c)) {
+        o.cn0 = c;
+        o.cn0_valid = 1;
+      }
+    }
+  }
+  out[i] = o;
+  (void)n_prn;
+}
+
+cudaError_t launch_finalize(const PolyClass& pc, const SearchDims& dims, const BestRow* d_best,
+                            double center_freq, int acr_table, int want_cn0, CellOut* d_out,
+                            cudaStream_t st) {
+  cudaError_t e = upload_acr_tables();
+  if (e != cudaSuccess) return e;
+  const int n = dims.n_ant * dims.n_prn;
+  if (n <= 0) return cudaSuccess;
+  finalize_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, dims.nb, dims.n_prn, pc.P, pc.Lc, dims.fc,
+                                                   center_freq, d_best, acr_table, want_cn0, d_out);
+  return TGA_LAUNCHED();
+}
+
+__global__ void acr_batch_kernel(const double* __restrict__ ra, int n, int table, double* __restrict__ cn0,
+                                 uint8_t* __restrict__ valid) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double c = 0.0;
+  const bool ok = estimate_cn0_dev(ra[i], table, &c);
+  cn0[i] = ok ? c : 0.0;
+  valid[i] = ok ? 1 : 0;
+}
+
+cudaError_t launch_acr_batch(const double* d_ra, int n, int table, double* d_cn0, uint8_t* d_valid,
+                             cudaStream_t st) {
+  cudaError_t e = upload_acr_tables();
+  if (e != cudaSuccess) return e;
+  if (n <= 0) return cudaSuccess;
+  acr_batch_kernel<<<(n + 255) / 256, 256, 0, st>>>(d_ra, n, table, d_cn0, d_valid);
+  return TGA_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------
+// antenna cross-correlation counts (observation.rs:175-195):
+// counts[i*n+j] = number of samples where antennas i and j agree
+// ---------------------------------------------------------------------------
+__global__ void xcorr_kernel(const uint8_t* __restrict__ bits, int n_ant, size_t row_bytes,
+                             unsigned long long* __restrict__ counts) {
+  const int i = blockIdx.y, j = blockIdx.x;
+  if (j < i) return;
+  const uint8_t* a = bits + (size_t)i * row_bytes;
+  const uint8_t* b = bits + (size_t)j * row_bytes;
+  unsigned long long diff = 0;
+  const bool aligned = ((((uintptr_t)a) | ((uintptr_t)b)) & 15) == 0;
+  size_t done = 0;
+  if (aligned) {
+    const size_t nv = row_bytes / 16;
+    const uint4* av = reinterpret_cast<const uint4*>(a);
+    const uint4* bv = reinterpret_cast<const uint4*>(b);
+    for (size_t k = threadIdx.x; k < nv; k += blockDim.x) {
+      const uint4 x = __ldg(av + k), y = __ldg(bv + k);
+      diff += __popc(x.x ^ y.x) + __popc(x.y ^ y.y) + __popc(x.z ^ y.z) + __popc(x.w ^ y.w);
+    }
+    done = nv * 16;
+  }
+  for (size_t k = done + threadIdx.x; k < row_bytes; k += blockDim.x) diff += __popc((unsigned)(a[k] ^ b[k]));
+  for (int o = 16; o > 0; o >>= 1) diff += __shfl_xor_sync(0xffffffffu, diff, o);
+  __shared__ unsigned long long part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = diff;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
+    const unsigned long long agree = (unsigned long long)row_bytes * 8ull - t;
+    counts[(size_t)i * n_ant + j] = agree;
+    counts[(size_t)j * n_ant + i] = agree;
+  }
+}
+
+cudaError_t launch_xcorr_matrix(const uint8_t* d_bits, int n_ant, size_t row_bytes, unsigned long long* d_counts,
+                                cudaStream_t st) {
+  if (n_ant <= 0) return cudaSuccess;
+  xcorr_kernel<<<dim3(n_ant, n_ant), 256, 0, st>>>(d_bits, n_ant, row_bytes, d_counts);
+  return TGA_LAUNCHED();
+}
+
+}  // namespace tga

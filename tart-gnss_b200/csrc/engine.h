@@ -1,0 +1,99 @@
+// Internal interface between the host orchestration (tga_api.cpp) and the
+// CUDA kernels (acq_kernels.cu).  Plain C++ types only.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace tga {
+
+constexpr int kMaxPulse = 64;  // samples per chip supported by the fused path
+constexpr int kMaxBins = 4096;
+
+// One polyphase class of the fused path: period P = S * Lc samples, a code
+// that is a chip sequence of length Lc held for S samples per chip and
+// shaped by pulse[0..S) (all +1, or the BOC(1,1) +1/-1 halves).
+struct PolyClass {
+  int P = 0, S = 0, Lc = 0, M = 0;  // M = Lc / 1023
+  float pulse[kMaxPulse] = {};
+};
+
+// Sample source of the front end.
+struct SampleSource {
+  // bits mode: packed MSB-first rows, antenna mean in d_mean (f64)
+  const uint8_t* bits = nullptr;
+  size_t row_bytes = 0;
+  const double* mean = nullptr;
+  // float mode (single-PRN API): de-meaned f32 samples and f64 phase points
+  const float* sig = nullptr;
+  const double* pp = nullptr;
+  size_t n_samples = 0;
+  // rows searched (antenna index into bits / mean / sig rows)
+  const int32_t* ant = nullptr;
+  int n_ant = 0;
+  double pc = 0.0;  // TAU / fs, bits mode phase points pc * n
+};
+
+struct SearchDims {
+  int n_ant = 0, nb = 0, n_prn = 0;
+  const double* fc = nullptr;  // device Doppler grid [nb]
+};
+
+// Per-(antenna, PRN) best row after the bin / hypothesis reduction.
+struct BestRow {
+  int32_t ab;      // antenna_slot * nb + bin
+  int32_t hyp;     // 0 [c,c], 1 [c,-c]
+  int32_t tau;     // lag in samples, [0, P)
+  float p;         // |y|^2 at the peak
+  float p2;        // second peak |y|^2 (set by the second-peak pass); 0 when none
+};
+
+// Finalised cell (device side); host converts to tga_cell.
+struct CellOut {
+  double strength, second, codephase_frac, frequency, cn0;
+  int32_t bin, tau, hyp, cn0_valid;
+};
+
+// Launchers; all asynchronous on `st`.  Return the launch error.
+cudaError_t launch_antenna_means(const uint8_t* d_bits, int n_rows, size_t row_bytes,
+                                 double* d_mean, cudaStream_t st);
+cudaError_t launch_frontend(const SampleSource& src, const SearchDims& dims, const PolyClass& pc,
+                            float2* d_z, cudaStream_t st);
+cudaError_t launch_forward_z(const PolyClass& pc, int n_ab, float2* d_z, int num_sms, cudaStream_t st);
+cudaError_t launch_code_spectra(const PolyClass& pc, const int8_t* d_chips, int n_prn, float2* d_D,
+                                int num_sms, cudaStream_t st);
+cudaError_t launch_correlate(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
+                             const float2* d_D, unsigned long long* d_keys, int num_sms,
+                             cudaStream_t st);
+cudaError_t launch_reduce_bins(const SearchDims& dims, const unsigned long long* d_keys,
+                               BestRow* d_best, cudaStream_t st);
+cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
+                               const float2* d_D, BestRow* d_best, int chip_width, int num_sms,
+                               cudaStream_t st);
+cudaError_t launch_finalize(const PolyClass& pc, const SearchDims& dims, const BestRow* d_best,
+                            double center_freq, int acr_table, int want_cn0, CellOut* d_out,
+                            cudaStream_t st);
+cudaError_t launch_acr_batch(const double* d_ra, int n, int table, double* d_cn0, uint8_t* d_valid,
+                             cudaStream_t st);
+cudaError_t launch_xcorr_matrix(const uint8_t* d_bits, int n_ant, size_t row_bytes,
+                                unsigned long long* d_counts, cudaStream_t st);
+
+// Generic path (any length N): reference algorithm with Bluestein FFTs.
+struct GenericPlan {
+  int N = 0;        // signal length
+  int Mpow2 = 0;    // Bluestein length (power of two >= 2N-1)
+  int log2M = 0;
+};
+cudaError_t launch_generic(const GenericPlan& gp, const float* d_sig, const double* d_pp,
+                           const double* d_fc, int nb, const float* d_code_a,
+                           const float* d_code_b, int period, double fs, float2* d_work,
+                           size_t work_elems, float* d_corr, int* d_result_i, float* d_result_f,
+                           cudaStream_t st);
+size_t generic_work_elems(const GenericPlan& gp, int nb);
+
+int kernel_launch_count_reset();
+void kernel_launch_add(int n);
+int kernel_launch_count();
+
+}  // namespace tga

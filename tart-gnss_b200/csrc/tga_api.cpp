@@ -1,0 +1,817 @@
+// Host side of libtga.so: context, planning and the C ABI of include/tga.h.
+//
+// Planning.  For each constellation the drivers of the reference search a
+// window of two code periods (acquisition.rs:274-275, galileo.rs:230-232,
+// beidou.rs:182-184, l1c.rs:191-193).  When the resampled code over that
+// window is exactly chip((n / S) mod Lc) * pulse(n % S) for the constellation's
+// chip count Lc (1023, 4092 or 10230) -- true at every integer number of
+// samples per chip, e.g. 16.368 MHz -- the fused polyphase kernels run.
+// Constellations that share the period, the Doppler grid and the pulse
+// (GPS/SBAS/QZSS; BeiDou/L1C) share one front end.  Anything else runs the
+// generic GPU path (the reference algorithm with Bluestein FFTs).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tga.h"
+#include "codes.h"
+#include "engine.h"
+
+using namespace tga;
+
+namespace {
+
+constexpr double kTau = 6.283185307179586;  // std::f64::consts::TAU
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+}  // namespace
+
+struct tga_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  std::map<std::string, DevBuf> bufs;
+  // cached fused-path code spectra: key -> (device D, n_prn)
+  double last_cells = 0.0;
+  int last_launches = 0;
+  double last_ms = 0.0;
+  uint64_t h2d = 0, d2h = 0;
+  // per-kernel event timing
+  bool profiling = false;
+  struct Pending {
+    std::string name;
+    int ev;
+    double flops;
+  };
+  std::vector<cudaEvent_t> evpool;
+  std::vector<Pending> pending;
+  int ev_used = 0;
+  struct KTime {
+    double ms = 0.0, flops = 0.0;
+    int launches = 0;
+  };
+  std::vector<std::pair<std::string, KTime>> ktimes;
+
+  int next_event() {
+    if (ev_used >= (int)evpool.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) throw std::runtime_error("cudaEventCreate failed");
+      evpool.push_back(e);
+    }
+    return ev_used++;
+  }
+
+  void* buf(const std::string& name, size_t bytes) {
+    DevBuf& b = bufs[name];
+    if (b.cap >= bytes && b.p) return b.p;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t want = bytes < 256 ? 256 : bytes;
+    if (cudaMalloc(&b.p, want) != cudaSuccess) {
+      cudaGetLastError();
+      throw std::runtime_error("cudaMalloc failed for " + name + " (" + std::to_string(want) + " bytes)");
+    }
+    b.cap = want;
+    return b.p;
+  }
+};
+
+namespace {
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));                \
+  } while (0)
+
+struct InvalidArg : std::invalid_argument {
+  explicit InvalidArg(const std::string& s) : std::invalid_argument(s) {}
+};
+
+template <class F>
+int guarded(tga_ctx* ctx, F&& f) {
+  if (!ctx) return TGA_ERR_INVALID_ARG;
+  try {
+    CK(cudaSetDevice(ctx->device));
+    ctx->err.clear();
+    return f();
+  } catch (const CudaError& e) {
+    ctx->err = e.what();
+    return TGA_ERR_CUDA;
+  } catch (const std::invalid_argument& e) {
+    ctx->err = e.what();
+    return TGA_ERR_INVALID_ARG;
+  } catch (const std::bad_alloc& e) {
+    ctx->err = "host allocation failed";
+    return TGA_ERR_OUT_OF_MEMORY;
+  } catch (const std::runtime_error& e) {
+    ctx->err = e.what();
+    return std::string(e.what()).find("cudaMalloc") != std::string::npos ? TGA_ERR_OUT_OF_MEMORY
+                                                                          : TGA_ERR_CUDA;
+  }
+}
+
+// acquisition.rs:188-198: n = round(2B/300) + 1 bins centred on center_freq.
+std::vector<double> freq_grid(double center, double band) {
+  const double x = 2.0 * band / 300.0;
+  double r = std::round(x);  // f64::round: half away from zero
+  size_t n = (r > 0.0) ? (size_t)r : 0;  // `as usize` saturates (NaN -> 0)
+  n += 1;
+  if (n > (size_t)kMaxBins) throw InvalidArg("search band gives too many Doppler bins");
+  std::vector<double> fc(n);
+  if (n == 1) {
+    fc[0] = center;
+  } else {
+    for (size_t i = 0; i < n; ++i) fc[i] = (center - band) + ((double)i * (2.0 * band)) / ((double)n - 1.0);
+  }
+  return fc;
+}
+
+int chip_width_of(double fs) {
+  double w = std::ceil(fs / 1.023e6);  // correlate.rs:157
+  return w > 0 ? (int)w : 0;
+}
+
+// Begin a new call: reset counters and per-kernel timing.
+void begin_call(tga_ctx* ctx) {
+  kernel_launch_count_reset();
+  ctx->last_cells = 0.0;
+  ctx->h2d = ctx->d2h = 0;
+  ctx->pending.clear();
+  ctx->ev_used = 0;
+  ctx->ktimes.clear();
+}
+
+// Launch through `fn` (returns cudaError_t), bracketed by events when profiling.
+template <class F>
+void timed(tga_ctx* ctx, const char* name, double flops, F&& fn) {
+  if (!ctx->profiling) {
+    CK(fn());
+    return;
+  }
+  const int a = ctx->next_event();
+  CK(cudaEventRecord(ctx->evpool[a], ctx->stream));
+  CK(fn());
+  const int b = ctx->next_event();
+  CK(cudaEventRecord(ctx->evpool[b], ctx->stream));
+  ctx->pending.push_back({name, a, flops});
+}
+
+// After the stream is idle: fold event pairs into per-kernel totals.
+void collect_times(tga_ctx* ctx) {
+  for (const auto& pd : ctx->pending) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->evpool[pd.ev], ctx->evpool[pd.ev + 1]));
+    auto it = ctx->ktimes.begin();
+    for (; it != ctx->ktimes.end(); ++it)
+      if (it->first == pd.name) break;
+    if (it == ctx->ktimes.end()) {
+      ctx->ktimes.push_back({pd.name, tga_ctx::KTime()});
+      it = ctx->ktimes.end() - 1;
+    }
+    it->second.ms += ms;
+    it->second.flops += pd.flops;
+    it->second.launches += 1;
+  }
+  ctx->pending.clear();
+}
+
+// FP32 operations per transform point of one length-Lc inverse transform as
+// implemented (DFT-31 1950 flops per 31 points, DFT-33 948 per 33, DFT-4 16
+// per 4, DFT-10 124 per 10; FMA = 2), excluding the input product (6) and
+// the output power (3).
+double transform_flops_per_point(int M) {
+  double f = 1950.0 / 31.0 + 948.0 / 33.0;
+  if (M == 4) f += 4.0;
+  if (M == 10) f += 12.4;
+  return f;
+}
+
+// Try to express the reference's resampled code over 2P samples as
+// chip((n/S) mod Lc) * pulse(n % S).  Returns false if it is not exact or the
+// chip count has no fused kernel.
+bool poly_class_for(int c, double samples_per_code, size_t P, size_t N, const std::vector<int>& prns,
+                    PolyClass* out) {
+  const ConstellationInfo& ci = info(c);
+  const int Lc = ci.primary_chips;
+  if (N != 2 * P || P == 0 || P % (size_t)Lc != 0) return false;
+  const size_t S = P / (size_t)Lc;
+  if (S < 1 || S > (size_t)kMaxPulse) return false;
+  if (Lc != 1023 && Lc != 4092 && Lc != 10230) return false;
+  PolyClass pc;
+  pc.P = (int)P;
+  pc.S = (int)S;
+  pc.Lc = Lc;
+  pc.M = Lc / 1023;
+  bool have_pulse = false;
+  for (int prn : prns) {
+    std::vector<int8_t> chips = primary_chips(c, prn);
+    std::vector<int8_t> code = resampled_code(c, prn, samples_per_code, N);
+    if (!have_pulse) {
+      for (size_t s = 0; s < S; ++s) pc.pulse[s] = (float)(code[s] * chips[0]);
+      have_pulse = true;
+    }
+    for (size_t n = 0; n < N; ++n) {
+      const int v = chips[(n / S) % (size_t)Lc] * (int)pc.pulse[n % S];
+      if (v != code[n]) return false;
+    }
+  }
+  *out = pc;
+  return true;
+}
+
+bool same_class(const PolyClass& a, const PolyClass& b) {
+  if (a.P != b.P || a.S != b.S || a.Lc != b.Lc) return false;
+  for (int s = 0; s < a.S; ++s)
+    if (a.pulse[s] != b.pulse[s]) return false;
+  return true;
+}
+
+// One group of constellations sharing a fused front end.
+struct ClassGroup {
+  PolyClass pc;
+  std::vector<int> consts;               // constellation ids in the group
+  std::vector<std::pair<int, int>> prns; // (constellation, prn) in search order
+};
+
+struct SearchOut {
+  std::vector<CellOut> cells;  // [n_ant][n_prn] of the group
+};
+
+// Runs the fused pipeline for one class group.  src describes the samples.
+void run_group(tga_ctx* ctx, const ClassGroup& grp, const SampleSource& src, const double* d_fc, int nb,
+               double center, int want_cn0, int chip_width, const std::string& tag, std::vector<CellOut>* out) {
+  const PolyClass& pc = grp.pc;
+  const int n_ant = src.n_ant;
+  const int n_prn = (int)grp.prns.size();
+  const int n_ab = n_ant * nb;
+  cudaStream_t st = ctx->stream;
+
+  // code chips -> device
+  std::vector<int8_t> chips((size_t)n_prn * pc.Lc);
+  for (int i = 0; i < n_prn; ++i) {
+    std::vector<int8_t> ch = primary_chips(grp.prns[i].first, grp.prns[i].second);
+    std::memcpy(&chips[(size_t)i * pc.Lc], ch.data(), (size_t)pc.Lc);
+  }
+  int8_t* d_chips = (int8_t*)ctx->buf(tag + ".chips", chips.size());
+  CK(cudaMemcpyAsync(d_chips, chips.data(), chips.size(), cudaMemcpyHostToDevice, st));
+  ctx->h2d += chips.size();
+
+  float2* d_z = (float2*)ctx->buf(tag + ".z", (size_t)n_ab * 2 * pc.S * pc.Lc * sizeof(float2));
+  float2* d_D = (float2*)ctx->buf(tag + ".D", (size_t)n_prn * 2 * pc.Lc * sizeof(float2));
+  unsigned long long* d_keys =
+      (unsigned long long*)ctx->buf(tag + ".keys", (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long));
+  BestRow* d_best = (BestRow*)ctx->buf(tag + ".best", (size_t)n_ant * n_prn * sizeof(BestRow));
+  CellOut* d_cells = (CellOut*)ctx->buf(tag + ".cells", (size_t)n_ant * n_prn * sizeof(CellOut));
+
+  SearchDims dims;
+  dims.n_ant = n_ant;
+  dims.nb = nb;
+  dims.n_prn = n_prn;
+  dims.fc = d_fc;
+
+  const double tf = transform_flops_per_point(pc.M);
+  const std::string cls = "[Lc=" + std::to_string(pc.Lc) + "]";
+  timed(ctx, ("code_spectra" + cls).c_str(), (double)n_prn * 2 * pc.Lc * tf,
+        [&] { return launch_code_spectra(pc, d_chips, n_prn, d_D, ctx->num_sms, st); });
+  timed(ctx, ("frontend" + cls).c_str(), (double)n_ab * 2 * pc.P * pc.S * 4.0,
+        [&] { return launch_frontend(src, dims, pc, d_z, st); });
+  timed(ctx, ("forward_z" + cls).c_str(), (double)n_ab * 2 * pc.P * tf,
+        [&] { return launch_forward_z(pc, n_ab, d_z, ctx->num_sms, st); });
+  timed(ctx, ("correlate" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * (tf + 9.0),
+        [&] { return launch_correlate(pc, dims, d_z, d_D, d_keys, ctx->num_sms, st); });
+  timed(ctx, ("reduce_bins" + cls).c_str(), 0.0, [&] { return launch_reduce_bins(dims, d_keys, d_best, st); });
+  timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * pc.P * (tf + 9.0),
+        [&] { return launch_second_peak(pc, dims, d_z, d_D, d_best, chip_width, ctx->num_sms, st); });
+  // finalize per constellation (ACR table differs between BeiDou and L1C)
+  out->resize((size_t)n_ant * n_prn);
+  {
+    // all constellations of a group use the same finalize except for the table;
+    // run once per table id and merge.
+    std::map<int, std::vector<int>> by_table;
+    for (int i = 0; i < n_prn; ++i) by_table[info(grp.prns[i].first).acr_table].push_back(i);
+    std::vector<CellOut> tmp((size_t)n_ant * n_prn);
+    for (auto& kv : by_table) {
+      timed(ctx, "finalize", 0.0,
+            [&] { return launch_finalize(pc, dims, d_best, center, kv.first, want_cn0, d_cells, st); });
+      CK(cudaMemcpyAsync(tmp.data(), d_cells, tmp.size() * sizeof(CellOut), cudaMemcpyDeviceToHost, st));
+      ctx->d2h += tmp.size() * sizeof(CellOut);
+      CK(cudaStreamSynchronize(st));
+      for (int a = 0; a < n_ant; ++a)
+        for (int i : kv.second) (*out)[(size_t)a * n_prn + i] = tmp[(size_t)a * n_prn + i];
+    }
+  }
+  ctx->last_cells += (double)n_ant * nb * n_prn * (double)pc.P;
+}
+
+void validate_prn(int c, int prn) {
+  const ConstellationInfo& ci = info(c);
+  if (prn < ci.prn_first || prn > ci.prn_last)
+    throw InvalidArg(std::string(ci.sv_prefix) + " PRN out of range: " + std::to_string(prn));
+}
+
+std::vector<int> prn_list(int c, const tga_all_options* opt) {
+  std::vector<int> v;
+  if (opt->prn_filter) {
+    for (size_t i = 0; i < opt->n_prn_filter; ++i) {
+      validate_prn(c, opt->prn_filter[i]);
+      v.push_back(opt->prn_filter[i]);
+    }
+  } else {
+    const ConstellationInfo& ci = info(c);
+    for (int p = ci.prn_first; p <= ci.prn_last; ++p) v.push_back(p);
+  }
+  return v;
+}
+
+int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, size_t row_bytes, double fs,
+                     const tga_all_options* opt, tga_cell* out, size_t cap, size_t* n_out) {
+  if (!opt || !n_out) throw InvalidArg("null options or n_out");
+  if (!(fs > 0.0)) throw InvalidArg("sampling frequency must be positive");
+  if (n_ant_total == 0 || row_bytes == 0) throw InvalidArg("empty observation");
+  std::vector<int32_t> ants;
+  if (opt->ant_filter) {
+    for (size_t i = 0; i < opt->n_ant_filter; ++i) {
+      if (opt->ant_filter[i] < 0 || (size_t)opt->ant_filter[i] >= n_ant_total)
+        throw InvalidArg("antenna index " + std::to_string(opt->ant_filter[i]) + " out of range (have " +
+                         std::to_string(n_ant_total) + ")");
+      ants.push_back(opt->ant_filter[i]);
+    }
+  } else {
+    for (size_t i = 0; i < n_ant_total; ++i) ants.push_back((int32_t)i);
+  }
+  if (ants.empty()) throw InvalidArg("no antennas selected");
+  size_t total = 0;
+  std::vector<int> consts;
+  std::map<int, std::vector<int>> prns;
+  for (int c = 0; c < N_CONST; ++c) {
+    if (!(opt->constellation_mask & (1u << c))) continue;
+    consts.push_back(c);
+    prns[c] = prn_list(c, opt);
+    total += prns[c].size() * ants.size();
+  }
+  *n_out = total;
+  if (total > cap || (!out && total)) return TGA_ERR_CAPACITY;
+  if (total == 0) return TGA_OK;
+
+  std::vector<double> fc = freq_grid(opt->center_freq, opt->search_band);
+  const int nb = (int)fc.size();
+  const size_t n_rec = row_bytes * 8;
+
+  // plan class groups
+  std::vector<ClassGroup> groups;
+  for (int c : consts) {
+    const size_t P = period_samples(c, fs);
+    const size_t N = std::min(2 * P, n_rec);
+    PolyClass pc;
+    if (!poly_class_for(c, (double)P, P, N, prns[c], &pc))
+      throw std::runtime_error(std::string("unsupported: ") + info(c).json_key +
+                               " at this sampling rate needs the generic path (not available for all-PRN search)");
+    bool placed = false;
+    for (auto& g : groups) {
+      if (same_class(g.pc, pc)) {
+        g.consts.push_back(c);
+        for (int p : prns[c]) g.prns.push_back({c, p});
+        placed = true;
+        break;
+      }
+    }
+    if (!placed) {
+      ClassGroup g;
+      g.pc = pc;
+      g.consts.push_back(c);
+      for (int p : prns[c]) g.prns.push_back({c, p});
+      groups.push_back(g);
+    }
+  }
+
+  cudaStream_t st = ctx->stream;
+  CK(cudaEventRecord(ctx->ev0, st));
+  // antenna means over the whole rows
+  double* d_mean = (double*)ctx->buf("mean", n_ant_total * sizeof(double));
+  timed(ctx, "antenna_means", 0.0, [&] { return launch_antenna_means(d_bits, (int)n_ant_total, row_bytes, d_mean, st); });
+  int32_t* d_ants = (int32_t*)ctx->buf("ants", ants.size() * sizeof(int32_t));
+  CK(cudaMemcpyAsync(d_ants, ants.data(), ants.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  double* d_fc = (double*)ctx->buf("fc", fc.size() * sizeof(double));
+  CK(cudaMemcpyAsync(d_fc, fc.data(), fc.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  ctx->h2d += ants.size() * sizeof(int32_t) + fc.size() * sizeof(double);
+
+  SampleSource src;
+  src.bits = d_bits;
+  src.row_bytes = row_bytes;
+  src.mean = d_mean;
+  src.ant = d_ants;
+  src.n_ant = (int)ants.size();
+  src.pc = kTau / fs;
+
+  std::map<std::pair<int, int>, CellOut> result;  // (const, prn) x ant via index below
+  std::vector<std::vector<CellOut>> gout(groups.size());
+  for (size_t gi = 0; gi < groups.size(); ++gi)
+    run_group(ctx, groups[gi], src, d_fc, nb, opt->center_freq, opt->cn0, chip_width_of(fs),
+              "g" + std::to_string(groups[gi].pc.P) + "_" + std::to_string(groups[gi].pc.Lc), &gout[gi]);
+  CK(cudaEventRecord(ctx->ev1, st));
+  CK(cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ctx->last_ms = ms;
+  ctx->last_launches = kernel_launch_count();
+  collect_times(ctx);
+
+  // assemble in (constellation, prn order, antenna) order
+  size_t k = 0;
+  for (int c : consts) {
+    for (int prn : prns[c]) {
+      // locate group / index
+      const ClassGroup* g = nullptr;
+      size_t gidx = 0, pidx = 0;
+      for (size_t gi = 0; gi < groups.size() && !g; ++gi)
+        for (size_t i = 0; i < groups[gi].prns.size(); ++i)
+          if (groups[gi].prns[i].first == c && groups[gi].prns[i].second == prn) {
+            g = &groups[gi];
+            gidx = gi;
+            pidx = i;
+            break;
+          }
+      const int n_prn_g = (int)g->prns.size();
+      for (size_t a = 0; a < ants.size(); ++a) {
+        const CellOut& o = gout[gidx][a * n_prn_g + pidx];
+        tga_cell& t = out[k++];
+        t.constellation = c;
+        t.prn = prn;
+        t.antenna = ants[a];
+        t.best_freq_idx = o.bin;
+        t.best_codephase = o.tau;
+        t.signal_strength = o.strength;
+        t.second_peak = o.second;
+        t.codephase_frac = o.codephase_frac;
+        t.frequency = o.frequency;
+        t.cn0_acr = o.cn0;
+        t.cn0_valid = o.cn0_valid;
+        t.hypothesis = o.hyp;
+      }
+    }
+  }
+  return TGA_OK;
+}
+
+// Generic path for one (signal, PRN): the reference algorithm on the GPU.
+// d_sig/d_pp are device arrays of n samples; d_fc the Doppler grid.
+tga_result generic_one(tga_ctx* ctx, int c, const float* d_sig, const double* d_pp, size_t n, double fs,
+                       const double* d_fc, const std::vector<double>& fc, double center, int prn, size_t period) {
+  if (n > (size_t)(1 << 26)) throw InvalidArg("signal too long for the generic path");
+  cudaStream_t st = ctx->stream;
+  const int nb = (int)fc.size();
+  // code replicas [c..] and [c, -c] split at min(period, n) (correlate.rs:47-58)
+  std::vector<int8_t> code = resampled_code(c, prn, (double)period, n);
+  std::vector<float> ca(n), cb(n);
+  const size_t split = std::min(period, n);
+  for (size_t i = 0; i < n; ++i) {
+    ca[i] = (float)code[i];
+    cb[i] = i < split ? ca[i] : -ca[i];
+  }
+  float* d_ca = (float*)ctx->buf("gen.ca", n * sizeof(float));
+  float* d_cb = (float*)ctx->buf("gen.cb", n * sizeof(float));
+  CK(cudaMemcpyAsync(d_ca, ca.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_cb, cb.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+  ctx->h2d += 2 * n * sizeof(float);
+  GenericPlan gp;
+  gp.N = (int)n;
+  gp.Mpow2 = 1;
+  gp.log2M = 0;
+  while (gp.Mpow2 < 2 * gp.N - 1) {
+    gp.Mpow2 <<= 1;
+    gp.log2M++;
+  }
+  if (gp.Mpow2 < 2) {
+    gp.Mpow2 = 2;
+    gp.log2M = 1;
+  }
+  const size_t welems = generic_work_elems(gp, nb);
+  float2* d_work = (float2*)ctx->buf("gen.work", welems * sizeof(float2));
+  float* d_corr = (float*)ctx->buf("gen.corr", (size_t)2 * nb * n * sizeof(float));
+  int* d_ri = (int*)ctx->buf("gen.ri", 4 * sizeof(int));
+  float* d_rf = (float*)ctx->buf("gen.rf", 4 * sizeof(float));
+  timed(ctx, "generic", 0.0, [&] {
+    return launch_generic(gp, d_sig, d_pp, d_fc, nb, d_ca, d_cb, (int)period, fs, d_work, welems, d_corr, d_ri,
+                          d_rf, st);
+  });
+  int ri[4];
+  float rf[4];
+  CK(cudaMemcpyAsync(ri, d_ri, sizeof ri, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(rf, d_rf, sizeof rf, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  ctx->d2h += sizeof ri + sizeof rf;
+  tga_result r;
+  r.prn = prn;
+  r.best_freq_idx = ri[0];
+  const size_t cp = (size_t)ri[1] % period;
+  r.best_codephase = (int64_t)cp;
+  r.signal_strength = (double)rf[0];
+  r.second_peak = (double)rf[1];
+  r.codephase_frac = (double)cp / (double)period;
+  r.frequency = fc[ri[0]] - center;
+  r.hypothesis = ri[2];
+  r.path = 1;
+  ctx->last_cells += (double)nb * (double)period;
+  return r;
+}
+
+int acquire_single_impl(tga_ctx* ctx, int c, const float* h_sig, const double* h_pp, size_t n, double fs,
+                        double center, double band, int prn, size_t period, tga_result* out) {
+  if (!h_sig || !h_pp || !out) throw InvalidArg("null pointer");
+  if (n == 0) throw InvalidArg("empty signal");
+  if (period == 0) throw InvalidArg("zero code period");
+  validate_prn(c, prn);
+  std::vector<double> fc = freq_grid(center, band);
+  const int nb = (int)fc.size();
+  PolyClass pc;
+  const bool fused = poly_class_for(c, (double)period, period, n, {prn}, &pc);
+  begin_call(ctx);
+  cudaStream_t st = ctx->stream;
+  float* d_sig = (float*)ctx->buf("single.sig", n * sizeof(float));
+  double* d_pp = (double*)ctx->buf("single.pp", n * sizeof(double));
+  CK(cudaMemcpyAsync(d_sig, h_sig, n * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_pp, h_pp, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  int32_t zero = 0;
+  int32_t* d_ant = (int32_t*)ctx->buf("single.ant", sizeof(int32_t));
+  CK(cudaMemcpyAsync(d_ant, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  double* d_fc = (double*)ctx->buf("single.fc", fc.size() * sizeof(double));
+  CK(cudaMemcpyAsync(d_fc, fc.data(), fc.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (!fused) {
+    ctx->h2d += n * (sizeof(float) + sizeof(double));
+    *out = generic_one(ctx, c, d_sig, d_pp, n, fs, d_fc, fc, center, prn, period);
+    ctx->last_launches = kernel_launch_count();
+    collect_times(ctx);
+    return TGA_OK;
+  }
+  SampleSource src;
+  src.sig = d_sig;
+  src.pp = d_pp;
+  src.n_samples = n;
+  src.ant = d_ant;
+  src.n_ant = 1;
+  ClassGroup g;
+  g.pc = pc;
+  g.consts.push_back(c);
+  g.prns.push_back({c, prn});
+  std::vector<CellOut> cells;
+  ctx->h2d += n * (sizeof(float) + sizeof(double));
+  run_group(ctx, g, src, d_fc, nb, center, 0, chip_width_of(fs), "single", &cells);
+  ctx->last_launches = kernel_launch_count();
+  collect_times(ctx);
+  const CellOut& o = cells[0];
+  out->prn = prn;
+  out->best_freq_idx = o.bin;
+  out->best_codephase = o.tau;
+  out->signal_strength = o.strength;
+  out->second_peak = o.second;
+  out->codephase_frac = o.codephase_frac;
+  out->frequency = o.frequency;
+  out->hypothesis = o.hyp;
+  out->path = 0;
+  return TGA_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+const char* tga_version(void) { return "tga 0.1.0 (sm_100a)"; }
+
+int tga_create(int device, tga_ctx** out) {
+  if (!out) return TGA_ERR_INVALID_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) {
+    cudaGetLastError();
+    return TGA_ERR_NO_DEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return TGA_ERR_NO_DEVICE;
+  if (prop.major != 10) return TGA_ERR_NO_DEVICE;  // built for sm_100a only
+  tga_ctx* ctx = new (std::nothrow) tga_ctx();
+  if (!ctx) return TGA_ERR_OUT_OF_MEMORY;
+  ctx->device = device;
+  ctx->num_sms = prop.multiProcessorCount;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
+    delete ctx;
+    return TGA_ERR_CUDA;
+  }
+  *out = ctx;
+  return TGA_OK;
+}
+
+int tga_destroy(tga_ctx* ctx) {
+  if (!ctx) return TGA_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->bufs)
+    if (kv.second.p) cudaFree(kv.second.p);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return TGA_OK;
+}
+
+const char* tga_last_error(const tga_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int tga_acquire_single(tga_ctx* ctx, int constellation, const float* h_signal_f32, const double* h_phasepoints,
+                       size_t num_samples, double sampling_freq, double center_freq, double search_band, int prn,
+                       size_t samples_per_chunk, tga_result* out) {
+  return guarded(ctx, [&] {
+    if (constellation < 0 || constellation >= N_CONST) throw InvalidArg("unknown constellation");
+    return acquire_single_impl(ctx, constellation, h_signal_f32, h_phasepoints, num_samples, sampling_freq,
+                               center_freq, search_band, prn, samples_per_chunk, out);
+  });
+}
+
+#define TGA_SINGLE_WRAPPER(name, cid)                                                                  \
+  int name(tga_ctx* ctx, const float* s, const double* pp, size_t n, double fs, double fc, double band, \
+           int prn, size_t per, tga_result* out) {                                                      \
+    return tga_acquire_single(ctx, cid, s, pp, n, fs, fc, band, prn, per, out);                         \
+  }
+TGA_SINGLE_WRAPPER(tga_acquire_full, TGA_GPS)
+TGA_SINGLE_WRAPPER(tga_acquire_sbas, TGA_SBAS)
+TGA_SINGLE_WRAPPER(tga_acquire_qzss, TGA_QZSS)
+TGA_SINGLE_WRAPPER(tga_acquire_galileo_single, TGA_GALILEO)
+TGA_SINGLE_WRAPPER(tga_acquire_beidou_single, TGA_BEIDOU)
+TGA_SINGLE_WRAPPER(tga_acquire_l1c_single, TGA_L1C)
+
+int tga_acquire_all_device(tga_ctx* ctx, const uint8_t* d_packed_bits, size_t n_ant, size_t row_bytes,
+                           double sampling_freq, const tga_all_options* opt, tga_cell* out, size_t out_capacity,
+                           size_t* n_out) {
+  return guarded(ctx, [&] {
+    if (!d_packed_bits) throw InvalidArg("null bits");
+    begin_call(ctx);
+    return acquire_all_impl(ctx, d_packed_bits, n_ant, row_bytes, sampling_freq, opt, out, out_capacity, n_out);
+  });
+}
+
+int tga_acquire_all(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, size_t row_bytes,
+                    double sampling_freq, const tga_all_options* opt, tga_cell* out, size_t out_capacity,
+                    size_t* n_out) {
+  return guarded(ctx, [&] {
+    if (!h_packed_bits) throw InvalidArg("null bits");
+    const size_t bytes = n_ant * row_bytes;
+    begin_call(ctx);
+    uint8_t* d_bits = (uint8_t*)ctx->buf("bits", bytes);
+    CK(cudaMemcpyAsync(d_bits, h_packed_bits, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->h2d += bytes;
+    return acquire_all_impl(ctx, d_bits, n_ant, row_bytes, sampling_freq, opt, out, out_capacity, n_out);
+  });
+}
+
+int tga_all_cell_count(size_t n_ant, const tga_all_options* opt, size_t* n_cells) {
+  if (!opt || !n_cells) return TGA_ERR_INVALID_ARG;
+  try {
+    size_t na = opt->ant_filter ? opt->n_ant_filter : n_ant, t = 0;
+    for (int c = 0; c < N_CONST; ++c)
+      if (opt->constellation_mask & (1u << c)) t += prn_list(c, opt).size() * na;
+    *n_cells = t;
+    return TGA_OK;
+  } catch (...) {
+    return TGA_ERR_INVALID_ARG;
+  }
+}
+
+int tga_last_search_stats(const tga_ctx* ctx, double* cells, int32_t* launches, double* device_ms) {
+  if (!ctx) return TGA_ERR_INVALID_ARG;
+  if (cells) *cells = ctx->last_cells;
+  if (launches) *launches = ctx->last_launches;
+  if (device_ms) *device_ms = ctx->last_ms;
+  return TGA_OK;
+}
+
+int tga_last_transfer_bytes(const tga_ctx* ctx, uint64_t* h2d, uint64_t* d2h) {
+  if (!ctx) return TGA_ERR_INVALID_ARG;
+  if (h2d) *h2d = ctx->h2d;
+  if (d2h) *d2h = ctx->d2h;
+  return TGA_OK;
+}
+
+void* tga_stream(tga_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int tga_set_profiling(tga_ctx* ctx, int enable) {
+  if (!ctx) return TGA_ERR_INVALID_ARG;
+  ctx->profiling = enable != 0;
+  return TGA_OK;
+}
+
+int tga_kernel_times(const tga_ctx* ctx, int cap, const char** names, double* ms, int32_t* launches,
+                     double* flops, int* n) {
+  if (!ctx || !n) return TGA_ERR_INVALID_ARG;
+  *n = (int)ctx->ktimes.size();
+  for (int i = 0; i < *n && i < cap; ++i) {
+    if (names) names[i] = ctx->ktimes[i].first.c_str();
+    if (ms) ms[i] = ctx->ktimes[i].second.ms;
+    if (launches) launches[i] = ctx->ktimes[i].second.launches;
+    if (flops) flops[i] = ctx->ktimes[i].second.flops;
+  }
+  return *n > cap ? TGA_ERR_CAPACITY : TGA_OK;
+}
+
+int tga_acr_cn0(tga_ctx* ctx, const double* h_r_a, size_t n, int table, double* h_cn0, uint8_t* h_valid) {
+  return guarded(ctx, [&] {
+    if (table < 0 || table > 3) throw InvalidArg("unknown ACR table");
+    if (n == 0) return TGA_OK;
+    if (!h_r_a || !h_cn0 || !h_valid) throw InvalidArg("null pointer");
+    double* d_ra = (double*)ctx->buf("acr.ra", n * sizeof(double));
+    double* d_c = (double*)ctx->buf("acr.cn0", n * sizeof(double));
+    uint8_t* d_v = (uint8_t*)ctx->buf("acr.valid", n);
+    CK(cudaMemcpyAsync(d_ra, h_r_a, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_acr_batch(d_ra, (int)n, table, d_c, d_v, ctx->stream));
+    CK(cudaMemcpyAsync(h_cn0, d_c, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(h_valid, d_v, n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TGA_OK;
+  });
+}
+
+int tga_antenna_xcorr_matrix(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant, size_t row_bytes, double* out) {
+  return guarded(ctx, [&] {
+    if (!h_bits || !out || n_ant == 0 || row_bytes == 0) throw InvalidArg("bad arguments");
+    uint8_t* d_bits = (uint8_t*)ctx->buf("xc.bits", n_ant * row_bytes);
+    unsigned long long* d_cnt = (unsigned long long*)ctx->buf("xc.cnt", n_ant * n_ant * 8);
+    CK(cudaMemcpyAsync(d_bits, h_bits, n_ant * row_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_xcorr_matrix(d_bits, (int)n_ant, row_bytes, d_cnt, ctx->stream));
+    std::vector<unsigned long long> cnt(n_ant * n_ant);
+    CK(cudaMemcpyAsync(cnt.data(), d_cnt, cnt.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double n = (double)(row_bytes * 8);
+    // sum of +-1 products = agree - disagree = 2*agree - n (exact), / n
+    for (size_t i = 0; i < cnt.size(); ++i) out[i] = (2.0 * (double)cnt[i] - n) / n;
+    return TGA_OK;
+  });
+}
+
+int tga_antenna_xcorr(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant, size_t row_bytes, int i, int j,
+                      double* out) {
+  return guarded(ctx, [&] {
+    if (!h_bits || !out || row_bytes == 0) throw InvalidArg("bad arguments");
+    if (i < 0 || (size_t)i >= n_ant) throw InvalidArg("antenna index " + std::to_string(i) + " out of range");
+    if (j < 0 || (size_t)j >= n_ant) throw InvalidArg("antenna index " + std::to_string(j) + " out of range");
+    uint8_t* d_bits = (uint8_t*)ctx->buf("xc.pair", 2 * row_bytes);
+    CK(cudaMemcpyAsync(d_bits, h_bits + (size_t)i * row_bytes, row_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_bits + row_bytes, h_bits + (size_t)j * row_bytes, row_bytes, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    unsigned long long* d_cnt = (unsigned long long*)ctx->buf("xc.cnt2", 4 * 8);
+    CK(launch_xcorr_matrix(d_bits, 2, row_bytes, d_cnt, ctx->stream));
+    unsigned long long cnt[4];
+    CK(cudaMemcpyAsync(cnt, d_cnt, sizeof cnt, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double n = (double)(row_bytes * 8);
+    *out = (2.0 * (double)cnt[1] - n) / n;
+    return TGA_OK;
+  });
+}
+
+int tga_code_chips(int constellation, int prn, int8_t* out, size_t capacity, size_t* n) {
+  try {
+    std::vector<int8_t> s = resample_sequence(constellation, prn);
+    if (n) *n = s.size();
+    if (!out) return TGA_OK;
+    if (capacity < s.size()) return TGA_ERR_CAPACITY;
+    std::memcpy(out, s.data(), s.size());
+    return TGA_OK;
+  } catch (...) {
+    return TGA_ERR_INVALID_ARG;
+  }
+}
+
+int tga_code_resampled(int constellation, int prn, double samples_per_code, size_t num_samples, float* out) {
+  try {
+    if (!out && num_samples) return TGA_ERR_INVALID_ARG;
+    std::vector<int8_t> s = resampled_code(constellation, prn, samples_per_code, num_samples);
+    for (size_t i = 0; i < num_samples; ++i) out[i] = (float)s[i];
+    return TGA_OK;
+  } catch (...) {
+    return TGA_ERR_INVALID_ARG;
+  }
+}
+
+}  // extern "C"

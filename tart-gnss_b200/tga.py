@@ -1,0 +1,331 @@
+"""Python binding of libtga.so (ctypes), mirroring tart-gnss-acquire's API.
+
+Function names, arguments and results follow the reference crate:
+
+* acquire_full / acquire_sbas / acquire_qzss / acquire_galileo_single /
+  acquire_beidou_single / acquire_l1c_single  (acquisition.rs:176,
+  sbas.rs:132, qzss.rs:135, galileo.rs:133, beidou.rs:85, l1c.rs:94)
+  -> AcquisitionResult(prn, signal_strength, second_peak, codephase_frac,
+     frequency)
+* acquire_all(...) -> {constellation: {"antenna_numbers", "results"}} with the
+  per-PRN result dicts of acquire_all_* (acquisition.rs:261-396): sv,
+  strengths, phases, freqs, cn0_acr (only with cn0), phase_median,
+  phase_mad, freq_median, freq_mad (only with >1 antenna), sorted by sv.
+* estimate_cn0_batch (acr.rs:49), correlate (observation.rs:175),
+  code generators (generate_*_code / *_resampled).
+
+The compute runs in libtga.so on the GPU; there is no CPU fallback.  A
+missing library or device raises.
+"""
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtga.so")
+
+GPS, GALILEO, BEIDOU, SBAS, L1C, QZSS = range(6)
+NAMES = ["gps", "galileo", "beidou", "sbas", "l1c", "qzss"]
+ALL = 0x3F
+GPS_IF = 4.092e6
+GPS_SEARCH_BAND = 6000.0
+ACR_TABLE = {GPS: 0, SBAS: 0, QZSS: 0, GALILEO: 1, BEIDOU: 2, L1C: 3}
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no sm_100 device", 4: "out of memory",
+          5: "unsupported", 6: "timeout", 7: "capacity"}
+
+
+class TgaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (STATUS.get(code, "error"), code, msg))
+        self.code = code
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("prn", ctypes.c_int32), ("best_freq_idx", ctypes.c_int32), ("best_codephase", ctypes.c_int64),
+                ("signal_strength", ctypes.c_double), ("second_peak", ctypes.c_double),
+                ("codephase_frac", ctypes.c_double), ("frequency", ctypes.c_double),
+                ("hypothesis", ctypes.c_int32), ("path", ctypes.c_int32)]
+
+
+class Cell(ctypes.Structure):
+    _fields_ = [("constellation", ctypes.c_int32), ("prn", ctypes.c_int32), ("antenna", ctypes.c_int32),
+                ("best_freq_idx", ctypes.c_int32), ("best_codephase", ctypes.c_int64),
+                ("signal_strength", ctypes.c_double), ("second_peak", ctypes.c_double),
+                ("codephase_frac", ctypes.c_double), ("frequency", ctypes.c_double),
+                ("cn0_acr", ctypes.c_double), ("cn0_valid", ctypes.c_int32), ("hypothesis", ctypes.c_int32)]
+
+
+class AllOptions(ctypes.Structure):
+    _fields_ = [("constellation_mask", ctypes.c_uint32), ("ant_filter", ctypes.POINTER(ctypes.c_int32)),
+                ("n_ant_filter", ctypes.c_size_t), ("prn_filter", ctypes.POINTER(ctypes.c_int32)),
+                ("n_prn_filter", ctypes.c_size_t), ("center_freq", ctypes.c_double),
+                ("search_band", ctypes.c_double), ("cn0", ctypes.c_int32), ("debug", ctypes.c_int32)]
+
+
+CELL_DTYPE = np.dtype([("constellation", "<i4"), ("prn", "<i4"), ("antenna", "<i4"), ("best_freq_idx", "<i4"),
+                       ("best_codephase", "<i8"), ("signal_strength", "<f8"), ("second_peak", "<f8"),
+                       ("codephase_frac", "<f8"), ("frequency", "<f8"), ("cn0_acr", "<f8"),
+                       ("cn0_valid", "<i4"), ("hypothesis", "<i4")])
+assert CELL_DTYPE.itemsize == ctypes.sizeof(Cell)
+
+_lib = None
+_P = ctypes.c_void_p
+
+
+def lib():
+    """Load libtga.so (built in-tree by __graft_entry__.build() / make)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libtga.so not built at %s (run `make -C tart-gnss_b200`)" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    i32, sz, dbl = ctypes.c_int, ctypes.c_size_t, ctypes.c_double
+    L.tga_create.argtypes = [i32, ctypes.POINTER(_P)]
+    L.tga_destroy.argtypes = [_P]
+    L.tga_last_error.argtypes = [_P]
+    L.tga_last_error.restype = ctypes.c_char_p
+    L.tga_version.restype = ctypes.c_char_p
+    single = [_P, i32, _P, _P, sz, dbl, dbl, dbl, i32, sz, ctypes.POINTER(Result)]
+    L.tga_acquire_single.argtypes = single
+    for nm in ("tga_acquire_full", "tga_acquire_sbas", "tga_acquire_qzss", "tga_acquire_galileo_single",
+               "tga_acquire_beidou_single", "tga_acquire_l1c_single"):
+        getattr(L, nm).argtypes = [_P, _P, _P, sz, dbl, dbl, dbl, i32, sz, ctypes.POINTER(Result)]
+    L.tga_acquire_all.argtypes = [_P, _P, sz, sz, dbl, ctypes.POINTER(AllOptions), _P, sz, ctypes.POINTER(sz)]
+    L.tga_acquire_all_device.argtypes = L.tga_acquire_all.argtypes
+    L.tga_all_cell_count.argtypes = [sz, ctypes.POINTER(AllOptions), ctypes.POINTER(sz)]
+    L.tga_last_search_stats.argtypes = [_P, ctypes.POINTER(dbl), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(dbl)]
+    L.tga_acr_cn0.argtypes = [_P, _P, sz, i32, _P, _P]
+    L.tga_antenna_xcorr.argtypes = [_P, _P, sz, sz, i32, i32, ctypes.POINTER(dbl)]
+    L.tga_antenna_xcorr_matrix.argtypes = [_P, _P, sz, sz, _P]
+    L.tga_code_chips.argtypes = [i32, i32, _P, sz, ctypes.POINTER(sz)]
+    L.tga_code_resampled.argtypes = [i32, i32, dbl, sz, _P]
+    L.tga_stream.argtypes = [_P]
+    L.tga_stream.restype = ctypes.c_void_p
+    L.tga_set_profiling.argtypes = [_P, i32]
+    L.tga_last_transfer_bytes.argtypes = [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    L.tga_kernel_times.argtypes = [_P, i32, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_int)]
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+# ---------------------------------------------------------------------------
+# host-side code tables (no GPU needed)
+# ---------------------------------------------------------------------------
+def code_chips(constellation, prn):
+    """generate_*_code: +-1 chips (BOC half-chips for BeiDou / L1C)."""
+    n = ctypes.c_size_t()
+    rc = lib().tga_code_chips(constellation, prn, None, 0, ctypes.byref(n))
+    if rc:
+        raise TgaError(rc, "bad constellation/PRN")
+    out = np.empty(n.value, dtype=np.int8)
+    lib().tga_code_chips(constellation, prn, _ptr(out), n.value, ctypes.byref(n))
+    return out
+
+
+def code_resampled(constellation, prn, samples_per_code, num_samples):
+    out = np.empty(num_samples, dtype=np.float32)
+    rc = lib().tga_code_resampled(constellation, prn, float(samples_per_code), num_samples, _ptr(out))
+    if rc:
+        raise TgaError(rc, "bad constellation/PRN")
+    return out
+
+
+@dataclass
+class AcquisitionResult:
+    prn: int
+    signal_strength: float
+    second_peak: float
+    codephase_frac: float
+    frequency: float
+    best_freq_idx: int = 0
+    best_codephase: int = 0
+    hypothesis: int = 0
+    path: int = 0
+
+
+def _median(x):
+    """stats.rs:10-20."""
+    s = sorted(x)
+    m = len(s) // 2
+    return (s[m - 1] + s[m]) / 2.0 if len(s) % 2 == 0 else s[m]
+
+
+def _mad(x, med):
+    return _median([abs(v - med) for v in x])
+
+
+SV_FMT = {GPS: "GPS{:02d}", GALILEO: "GSAT{:02d}", BEIDOU: "BEIDOU{:02d}", SBAS: "SBAS{:03d}",
+          L1C: "GPSL1C{:02d}", QZSS: "QZSS{:03d}"}
+
+
+class Context:
+    """One engine context on one GPU (tga_create / tga_destroy)."""
+
+    def __init__(self, device=0):
+        self._h = _P()
+        rc = lib().tga_create(device, ctypes.byref(self._h))
+        if rc:
+            raise TgaError(rc, "tga_create(device=%d) failed" % device)
+
+    def close(self):
+        if self._h:
+            lib().tga_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc:
+            raise TgaError(rc, lib().tga_last_error(self._h).decode())
+
+    # ---- single PRN --------------------------------------------------------
+    def acquire_single(self, constellation, signal_f32, phasepoints, sampling_freq, center_freq, search_band, prn,
+                       samples_per_chunk):
+        sig = np.ascontiguousarray(signal_f32, dtype=np.float32)
+        pp = np.ascontiguousarray(phasepoints, dtype=np.float64)
+        if len(pp) < len(sig):
+            raise ValueError("phasepoints shorter than signal")
+        r = Result()
+        self._check(lib().tga_acquire_single(self._h, constellation, _ptr(sig), _ptr(pp), len(sig),
+                                             float(sampling_freq), float(center_freq), float(search_band), int(prn),
+                                             int(samples_per_chunk), ctypes.byref(r)))
+        return AcquisitionResult(r.prn, r.signal_strength, r.second_peak, r.codephase_frac, r.frequency,
+                                 r.best_freq_idx, r.best_codephase, r.hypothesis, r.path)
+
+    def acquire_full(self, *a):
+        return self.acquire_single(GPS, *a)
+
+    def acquire_sbas(self, *a):
+        return self.acquire_single(SBAS, *a)
+
+    def acquire_qzss(self, *a):
+        return self.acquire_single(QZSS, *a)
+
+    def acquire_galileo_single(self, *a):
+        return self.acquire_single(GALILEO, *a)
+
+    def acquire_beidou_single(self, *a):
+        return self.acquire_single(BEIDOU, *a)
+
+    def acquire_l1c_single(self, *a):
+        return self.acquire_single(L1C, *a)
+
+    # ---- all PRNs, all antennas -------------------------------------------
+    def _options(self, mask, ant_filter, prn_filter, center_freq, search_band, cn0, debug):
+        o = AllOptions()
+        o.constellation_mask = mask
+        keep = []
+        if ant_filter is not None:
+            a = np.ascontiguousarray(ant_filter, dtype=np.int32)
+            keep.append(a)
+            o.ant_filter = a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+            o.n_ant_filter = len(a)
+        if prn_filter is not None:
+            p = np.ascontiguousarray(prn_filter, dtype=np.int32)
+            keep.append(p)
+            o.prn_filter = p.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+            o.n_prn_filter = len(p)
+        o.center_freq = center_freq
+        o.search_band = search_band
+        o.cn0 = 1 if cn0 else 0
+        o.debug = 1 if debug else 0
+        return o, keep
+
+    def acquire_cells(self, packed_bits, sampling_freq, mask=ALL, ant_filter=None, prn_filter=None,
+                      center_freq=GPS_IF, search_band=GPS_SEARCH_BAND, cn0=False, device_bits=None, n_ant=None,
+                      row_bytes=None):
+        """Raw per-(constellation, prn, antenna) cells as a numpy record array.
+
+        packed_bits: [n_ant, row_bytes] uint8 host array, or pass device_bits
+        (an integer device pointer, e.g. torch tensor .data_ptr()) with
+        n_ant and row_bytes."""
+        o, keep = self._options(mask, ant_filter, prn_filter, center_freq, search_band, cn0, False)
+        if device_bits is None:
+            bits = np.ascontiguousarray(packed_bits, dtype=np.uint8)
+            n_ant, row_bytes = bits.shape
+        n = ctypes.c_size_t()
+        self._check(lib().tga_all_cell_count(n_ant, ctypes.byref(o), ctypes.byref(n)))
+        out = np.zeros(n.value, dtype=CELL_DTYPE)
+        fn = lib().tga_acquire_all if device_bits is None else lib().tga_acquire_all_device
+        src = _ptr(bits) if device_bits is None else ctypes.c_void_p(device_bits)
+        self._check(fn(self._h, src, n_ant, row_bytes, float(sampling_freq), ctypes.byref(o), _ptr(out),
+                       len(out), ctypes.byref(n)))
+        del keep
+        return out
+
+    def acquire_all(self, packed_bits, sampling_freq, mask=ALL, ant_filter=None, prn_filter=None,
+                    center_freq=GPS_IF, search_band=GPS_SEARCH_BAND, cn0=False, debug=False):
+        """acquire_all_* for every constellation in mask, grouped like the
+        reference's *AllAcquisitionOutput (per-PRN results sorted by sv)."""
+        cells = self.acquire_cells(packed_bits, sampling_freq, mask, ant_filter, prn_filter, center_freq,
+                                   search_band, cn0)
+        n_ant = np.asarray(packed_bits).shape[0]
+        ants = list(ant_filter) if ant_filter is not None else list(range(n_ant))
+        out = {}
+        for c in range(6):
+            if not (mask >> c) & 1:
+                continue
+            sel = cells[cells["constellation"] == c]
+            results = []
+            for prn in dict.fromkeys(sel["prn"].tolist()):
+                rows = sel[sel["prn"] == prn]
+                r = {"sv": SV_FMT[c].format(prn), "strengths": rows["signal_strength"].tolist(),
+                     "phases": rows["codephase_frac"].tolist(), "freqs": rows["frequency"].tolist(),
+                     "second_peaks": rows["second_peak"].tolist(),
+                     "best_freq_idx": rows["best_freq_idx"].tolist(),
+                     "best_codephase": rows["best_codephase"].tolist()}
+                if cn0:
+                    vals = [float(v) if ok else None for v, ok in zip(rows["cn0_acr"], rows["cn0_valid"])]
+                    r["cn0_acr"] = None if all(v is None for v in vals) else vals
+                if len(rows) > 1:
+                    pm, fm = _median(r["phases"]), _median(r["freqs"])
+                    r.update(phase_median=pm, phase_mad=_mad(r["phases"], pm), freq_median=fm,
+                             freq_mad=_mad(r["freqs"], fm))
+                results.append(r)
+            results.sort(key=lambda r: r["sv"])
+            out[NAMES[c]] = {"antenna_numbers": ants, "results": results}
+        return out
+
+    def last_stats(self):
+        cells, launches, ms = ctypes.c_double(), ctypes.c_int32(), ctypes.c_double()
+        lib().tga_last_search_stats(self._h, ctypes.byref(cells), ctypes.byref(launches), ctypes.byref(ms))
+        return {"cells": cells.value, "kernel_launches": launches.value, "device_ms": ms.value}
+
+    # ---- ACR and antenna correlation ---------------------------------------
+    def estimate_cn0_batch(self, r_a, table):
+        ra = np.ascontiguousarray(r_a, dtype=np.float64)
+        cn0 = np.zeros(len(ra))
+        valid = np.zeros(len(ra), dtype=np.uint8)
+        self._check(lib().tga_acr_cn0(self._h, _ptr(ra), len(ra), table, _ptr(cn0), _ptr(valid)))
+        return [float(c) if v else None for c, v in zip(cn0, valid)]
+
+    def correlate(self, packed_bits, i, j):
+        bits = np.ascontiguousarray(packed_bits, dtype=np.uint8)
+        out = ctypes.c_double()
+        self._check(lib().tga_antenna_xcorr(self._h, _ptr(bits), bits.shape[0], bits.shape[1], i, j,
+                                            ctypes.byref(out)))
+        return out.value
+
+    def correlation_matrix(self, packed_bits):
+        bits = np.ascontiguousarray(packed_bits, dtype=np.uint8)
+        out = np.zeros((bits.shape[0], bits.shape[0]))
+        self._check(lib().tga_antenna_xcorr_matrix(self._h, _ptr(bits), bits.shape[0], bits.shape[1], _ptr(out)))
+        return out
