@@ -166,6 +166,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--n-ant", type=int, default=N_ANT, help="antennas per GPU (profiling runs use fewer)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -184,7 +186,7 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    bits_np, _ = synth_observation(SEED + rank)
+    bits_np, _ = synth_observation(SEED + rank, n_ant=args.n_ant)
     n_ant, row_bytes = bits_np.shape
     pinned = torch.empty((n_ant, row_bytes), dtype=torch.uint8, pin_memory=True)
     pinned.numpy()[:] = bits_np
@@ -254,7 +256,7 @@ def main():
     # end to end through the C ABI from pinned host memory
     host = pinned.numpy()
     e2e_times = []
-    for i in range(args.warmup + args.steps):
+    for i in range(0 if args.no_e2e else args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ctx.acquire_cells(host, FS, mask=tga.ALL, cn0=True)
@@ -265,7 +267,7 @@ def main():
     lib.tga_last_transfer_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
                                             ctypes.POINTER(ctypes.c_uint64)]
     lib.tga_last_transfer_bytes(ctx._h, ctypes.byref(h2d), ctypes.byref(d2h))
-    e2e_s = statistics.mean(e2e_times)
+    e2e_s = statistics.mean(e2e_times) if e2e_times else float("nan")
     if world > 1:
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -209,6 +209,39 @@ int tga_antenna_xcorr(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant,
 int tga_antenna_xcorr_matrix(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant,
                              size_t row_bytes, double* out);
 
+/* ---- result aggregation and JSON (host) --------------------------------------
+ * Groups the cells of tga_acquire_all into the reference's output structs
+ * and serialises them as serde_json::to_string_pretty does for
+ * CombinedOutput (lib.rs:32-45; per-PRN fields acquisition.rs:32-66, ACR
+ * :341-357, median/MAD :365-377, sort by sv :393).  filter_phase_mad /
+ * filter_freq_mad (NaN = off) drop results whose MAD exceeds the threshold,
+ * like apply_mad_filters (main.rs:242-256); *n_filtered counts them.
+ * *json is malloc'd: release it with tga_free. */
+int tga_results_json(const tga_cell* cells, size_t n_cells, const int32_t* antenna_numbers,
+                     size_t n_ant, uint32_t constellation_mask, int cn0, double filter_phase_mad,
+                     double filter_freq_mad, char** json, size_t* n_filtered);
+/* One f64 in the JSON number format above (shortest round-trip digits). */
+int tga_format_f64(double v, char* out, size_t capacity);
+void tga_free(void* p);
+
+/* ---- observation files (host) -----------------------------------------------
+ * Replaces Observation::from_hdf5 (observation.rs:48-92): reads the
+ * `config` JSON (num_antenna, sampling_frequency; config.rs:10-19), the
+ * `timestamp` string and the packed `data` rows of a TART HDF5 file.  The
+ * bits stay packed (the kernels unpack in registers), unlike the reference
+ * which expands them to one byte per sample (observation.rs:232-240). */
+typedef struct {
+  uint32_t num_antenna;
+  double sampling_frequency;
+  size_t row_bytes;          /* packed bytes per antenna row                  */
+  char timestamp[64];
+  char* config_json;         /* malloc'd; freed by tga_observation_free       */
+  uint8_t* data;             /* malloc'd num_antenna * row_bytes packed bits  */
+  char error[256];           /* message when the call fails                   */
+} tga_observation;
+int tga_observation_read_hdf5(const char* path, tga_observation* out);
+void tga_observation_free(tga_observation* obs);
+
 /* ---- code tables (host) -----------------------------------------------------
  * +-1 primary chips of one PRN: generate_ca_code (acquisition.rs:130),
  * generate_sbas_ca_code (sbas.rs:111), generate_qzss_ca_code (qzss.rs:111),

@@ -575,8 +575,8 @@ __device__ bool estimate_cn0_dev(double r_a, int table, double* out) {
 }
 
 __global__ void finalize_kernel(int n_cells, int nb, int n_prn, int P, int Lc, const double* __restrict__ fc,
-                                double center, const BestRow* __restrict__ best, int table, int want_cn0,
-                                CellOut* __restrict__ out) {
+                                double center, const BestRow* __restrict__ best, const int8_t* __restrict__ tables,
+                                int want_cn0, CellOut* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_cells) return;
   const BestRow b = best[i];
@@ -600,25 +600,24 @@ __global__ void finalize_kernel(int n_cells, int nb, int n_prn, int P, int Lc, c
     if (s > 0.0 && m > s) {
       const double q = m / s;
       double c;
-      if (estimate_cn0_dev(q * q, table, &c)) {
+      if (estimate_cn0_dev(q * q, tables[i % n_prn], &c)) {
         o.cn0 = c;
         o.cn0_valid = 1;
       }
     }
   }
   out[i] = o;
-  (void)n_prn;
 }
 
 cudaError_t launch_finalize(const PolyClass& pc, const SearchDims& dims, const BestRow* d_best,
-                            double center_freq, int acr_table, int want_cn0, CellOut* d_out,
+                            double center_freq, const int8_t* d_tables, int want_cn0, CellOut* d_out,
                             cudaStream_t st) {
   cudaError_t e = upload_acr_tables();
   if (e != cudaSuccess) return e;
   const int n = dims.n_ant * dims.n_prn;
   if (n <= 0) return cudaSuccess;
   finalize_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, dims.nb, dims.n_prn, pc.P, pc.Lc, dims.fc,
-                                                   center_freq, d_best, acr_table, want_cn0, d_out);
+                                                   center_freq, d_best, d_tables, want_cn0, d_out);
   return TGA_LAUNCHED();
 }
 

@@ -71,8 +71,9 @@ cudaError_t launch_reduce_bins(const SearchDims& dims, const unsigned long long*
 cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
                                const float2* d_D, BestRow* d_best, int chip_width, int num_sms,
                                cudaStream_t st);
+// d_tables: ACR table id (TGA_ACR_*) per PRN of the group.
 cudaError_t launch_finalize(const PolyClass& pc, const SearchDims& dims, const BestRow* d_best,
-                            double center_freq, int acr_table, int want_cn0, CellOut* d_out,
+                            double center_freq, const int8_t* d_tables, int want_cn0, CellOut* d_out,
                             cudaStream_t st);
 cudaError_t launch_acr_batch(const double* d_ra, int n, int table, double* d_cn0, uint8_t* d_valid,
                              cudaStream_t st);
@@ -91,6 +92,8 @@ cudaError_t launch_generic(const GenericPlan& gp, const float* d_sig, const doub
                            size_t work_elems, float* d_corr, int* d_result_i, float* d_result_f,
                            cudaStream_t st);
 size_t generic_work_elems(const GenericPlan& gp, int nb);
+cudaError_t launch_bits_to_signal(const uint8_t* d_bits, size_t row_bytes, int row, const double* d_mean, int n,
+                                  double pc, float* d_sig, double* d_pp, cudaStream_t st);
 
 int kernel_launch_count_reset();
 void kernel_launch_add(int n);

@@ -277,7 +277,26 @@ __global__ void select_second_kernel(const float* __restrict__ corr, const unsig
   }
 }
 
+// acquisition.rs:281-294 on the GPU: +-1 samples minus the row mean, first n
+// as f32, and phase points TAU/fs * i in f64.
+__global__ void bits_to_signal_kernel(const uint8_t* __restrict__ bits, size_t row_bytes, int row,
+                                      const double* __restrict__ mean, int n, double pc, float* __restrict__ sig,
+                                      double* __restrict__ pp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t byte = bits[(size_t)row * row_bytes + (i >> 3)];
+  const double v = ((byte >> (7 - (i & 7))) & 1) ? 1.0 : -1.0;
+  sig[i] = (float)(v - mean[row]);
+  pp[i] = pc * (double)i;
+}
+
 }  // namespace
+
+cudaError_t launch_bits_to_signal(const uint8_t* d_bits, size_t row_bytes, int row, const double* d_mean, int n,
+                                  double pc, float* d_sig, double* d_pp, cudaStream_t st) {
+  bits_to_signal_kernel<<<nblk(n, 256), 256, 0, st>>>(d_bits, row_bytes, row, d_mean, n, pc, d_sig, d_pp);
+  return TGA_GLAUNCHED();
+}
 
 size_t generic_work_elems(const GenericPlan& gp, int nb) {
   const size_t N = gp.N, M = gp.Mpow2, batch = 2 * nb > 2 ? 2 * nb : 2;

@@ -11,6 +11,7 @@
 // generic GPU path (the reference algorithm with Bluestein FFTs).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -23,6 +24,7 @@
 #include "../../include/tga.h"
 #include "codes.h"
 #include "engine.h"
+#include "gnss_tables.h"
 
 using namespace tga;
 
@@ -64,6 +66,30 @@ struct tga_ctx {
     int launches = 0;
   };
   std::vector<std::pair<std::string, KTime>> ktimes;
+  // planning caches: verified polyphase classes, host chips, uploaded chips
+  struct ClassCache {
+    bool structure_ok = false;
+    PolyClass pc;
+    std::map<int, bool> prn_ok;
+  };
+  std::map<std::string, ClassCache> class_cache;
+  std::map<std::pair<int, int>, std::vector<int8_t>> chip_cache;
+  std::map<std::string, std::vector<std::pair<int, int>>> uploaded;  // device chips buffer -> PRN list
+  // pinned host staging for results
+  void* pinned = nullptr;
+  size_t pinned_cap = 0;
+  void* host_pinned(size_t bytes) {
+    if (pinned_cap >= bytes && pinned) return pinned;
+    if (pinned) cudaFreeHost(pinned);
+    pinned = nullptr;
+    pinned_cap = 0;
+    if (cudaMallocHost(&pinned, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      throw std::runtime_error("cudaMallocHost failed");
+    }
+    pinned_cap = bytes;
+    return pinned;
+  }
 
   int next_event() {
     if (ev_used >= (int)evpool.size()) {
@@ -206,36 +232,60 @@ double transform_flops_per_point(int M) {
   return f;
 }
 
+const std::vector<int8_t>& cached_chips(tga_ctx* ctx, int c, int prn) {
+  auto key = std::make_pair(c, prn);
+  auto it = ctx->chip_cache.find(key);
+  if (it != ctx->chip_cache.end()) return it->second;
+  return ctx->chip_cache[key] = primary_chips(c, prn);
+}
+
 // Try to express the reference's resampled code over 2P samples as
 // chip((n/S) mod Lc) * pulse(n % S).  Returns false if it is not exact or the
-// chip count has no fused kernel.
-bool poly_class_for(int c, double samples_per_code, size_t P, size_t N, const std::vector<int>& prns,
-                    PolyClass* out) {
+// chip count has no fused kernel.  The check is exact (every sample of every
+// PRN is compared with the reference's resampling rule) and cached per
+// context, since it depends only on (constellation, rate, period, PRN).
+bool poly_class_for(tga_ctx* ctx, int c, double samples_per_code, size_t P, size_t N,
+                    const std::vector<int>& prns, PolyClass* out) {
   const ConstellationInfo& ci = info(c);
   const int Lc = ci.primary_chips;
   if (N != 2 * P || P == 0 || P % (size_t)Lc != 0) return false;
   const size_t S = P / (size_t)Lc;
   if (S < 1 || S > (size_t)kMaxPulse) return false;
   if (Lc != 1023 && Lc != 4092 && Lc != 10230) return false;
-  PolyClass pc;
-  pc.P = (int)P;
-  pc.S = (int)S;
-  pc.Lc = Lc;
-  pc.M = Lc / 1023;
-  bool have_pulse = false;
+  char keybuf[96];
+  uint64_t spc_bits;
+  std::memcpy(&spc_bits, &samples_per_code, 8);
+  std::snprintf(keybuf, sizeof keybuf, "%d/%zu/%zu/%llx", c, P, N, (unsigned long long)spc_bits);
+  tga_ctx::ClassCache& cc = ctx->class_cache[keybuf];
   for (int prn : prns) {
-    std::vector<int8_t> chips = primary_chips(c, prn);
-    std::vector<int8_t> code = resampled_code(c, prn, samples_per_code, N);
-    if (!have_pulse) {
-      for (size_t s = 0; s < S; ++s) pc.pulse[s] = (float)(code[s] * chips[0]);
-      have_pulse = true;
+    auto hit = cc.prn_ok.find(prn);
+    if (hit != cc.prn_ok.end()) {
+      if (!hit->second) return false;
+      continue;
     }
-    for (size_t n = 0; n < N; ++n) {
-      const int v = chips[(n / S) % (size_t)Lc] * (int)pc.pulse[n % S];
-      if (v != code[n]) return false;
+    const std::vector<int8_t>& chips = cached_chips(ctx, c, prn);
+    std::vector<int8_t> code = resampled_code(c, prn, samples_per_code, N);
+    PolyClass pc;
+    pc.P = (int)P;
+    pc.S = (int)S;
+    pc.Lc = Lc;
+    pc.M = Lc / 1023;
+    for (size_t s2 = 0; s2 < S; ++s2) pc.pulse[s2] = (float)(code[s2] * chips[0]);
+    bool ok = true;
+    for (size_t n = 0; n < N && ok; ++n)
+      ok = chips[(n / S) % (size_t)Lc] * (int)pc.pulse[n % S] == code[n];
+    if (ok && cc.structure_ok) {
+      for (size_t s2 = 0; s2 < S; ++s2) ok = ok && pc.pulse[s2] == cc.pc.pulse[s2];
+    }
+    cc.prn_ok[prn] = ok;
+    if (!ok) return false;
+    if (!cc.structure_ok) {
+      cc.pc = pc;
+      cc.structure_ok = true;
     }
   }
-  *out = pc;
+  if (!cc.structure_ok) return false;
+  *out = cc.pc;
   return true;
 }
 
@@ -257,24 +307,34 @@ struct SearchOut {
   std::vector<CellOut> cells;  // [n_ant][n_prn] of the group
 };
 
-// Runs the fused pipeline for one class group.  src describes the samples.
+// Runs the fused pipeline for one class group, asynchronously on the
+// context stream.  The finalised cells land in host_out (pinned memory,
+// n_ant * n_prn CellOut) once the stream reaches that point.
 void run_group(tga_ctx* ctx, const ClassGroup& grp, const SampleSource& src, const double* d_fc, int nb,
-               double center, int want_cn0, int chip_width, const std::string& tag, std::vector<CellOut>* out) {
+               double center, int want_cn0, int chip_width, const std::string& tag, CellOut* host_out) {
   const PolyClass& pc = grp.pc;
   const int n_ant = src.n_ant;
   const int n_prn = (int)grp.prns.size();
   const int n_ab = n_ant * nb;
   cudaStream_t st = ctx->stream;
 
-  // code chips -> device
-  std::vector<int8_t> chips((size_t)n_prn * pc.Lc);
-  for (int i = 0; i < n_prn; ++i) {
-    std::vector<int8_t> ch = primary_chips(grp.prns[i].first, grp.prns[i].second);
-    std::memcpy(&chips[(size_t)i * pc.Lc], ch.data(), (size_t)pc.Lc);
+  // code chips and ACR table ids -> device (re-uploaded only when the PRN list changes)
+  const size_t chip_bytes = (size_t)n_prn * pc.Lc;
+  int8_t* d_chips = (int8_t*)ctx->buf(tag + ".chips", chip_bytes + (size_t)n_prn);
+  auto up = ctx->uploaded.find(tag + ".chips");
+  if (up == ctx->uploaded.end() || up->second != grp.prns) {
+    std::vector<int8_t> chips(chip_bytes + (size_t)n_prn);
+    for (int i = 0; i < n_prn; ++i) {
+      const std::vector<int8_t>& ch = cached_chips(ctx, grp.prns[i].first, grp.prns[i].second);
+      std::memcpy(&chips[(size_t)i * pc.Lc], ch.data(), (size_t)pc.Lc);
+      chips[chip_bytes + i] = (int8_t)info(grp.prns[i].first).acr_table;
+    }
+    CK(cudaMemcpyAsync(d_chips, chips.data(), chips.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));  // chips is a host temporary
+    ctx->h2d += chips.size();
+    ctx->uploaded[tag + ".chips"] = grp.prns;
   }
-  int8_t* d_chips = (int8_t*)ctx->buf(tag + ".chips", chips.size());
-  CK(cudaMemcpyAsync(d_chips, chips.data(), chips.size(), cudaMemcpyHostToDevice, st));
-  ctx->h2d += chips.size();
+  const int8_t* d_tables = d_chips + chip_bytes;
 
   float2* d_z = (float2*)ctx->buf(tag + ".z", (size_t)n_ab * 2 * pc.S * pc.Lc * sizeof(float2));
   float2* d_D = (float2*)ctx->buf(tag + ".D", (size_t)n_prn * 2 * pc.Lc * sizeof(float2));
@@ -302,24 +362,10 @@ void run_group(tga_ctx* ctx, const ClassGroup& grp, const SampleSource& src, con
   timed(ctx, ("reduce_bins" + cls).c_str(), 0.0, [&] { return launch_reduce_bins(dims, d_keys, d_best, st); });
   timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * pc.P * (tf + 9.0),
         [&] { return launch_second_peak(pc, dims, d_z, d_D, d_best, chip_width, ctx->num_sms, st); });
-  // finalize per constellation (ACR table differs between BeiDou and L1C)
-  out->resize((size_t)n_ant * n_prn);
-  {
-    // all constellations of a group use the same finalize except for the table;
-    // run once per table id and merge.
-    std::map<int, std::vector<int>> by_table;
-    for (int i = 0; i < n_prn; ++i) by_table[info(grp.prns[i].first).acr_table].push_back(i);
-    std::vector<CellOut> tmp((size_t)n_ant * n_prn);
-    for (auto& kv : by_table) {
-      timed(ctx, "finalize", 0.0,
-            [&] { return launch_finalize(pc, dims, d_best, center, kv.first, want_cn0, d_cells, st); });
-      CK(cudaMemcpyAsync(tmp.data(), d_cells, tmp.size() * sizeof(CellOut), cudaMemcpyDeviceToHost, st));
-      ctx->d2h += tmp.size() * sizeof(CellOut);
-      CK(cudaStreamSynchronize(st));
-      for (int a = 0; a < n_ant; ++a)
-        for (int i : kv.second) (*out)[(size_t)a * n_prn + i] = tmp[(size_t)a * n_prn + i];
-    }
-  }
+  timed(ctx, ("finalize" + cls).c_str(), 0.0,
+        [&] { return launch_finalize(pc, dims, d_best, center, d_tables, want_cn0, d_cells, st); });
+  CK(cudaMemcpyAsync(host_out, d_cells, (size_t)n_ant * n_prn * sizeof(CellOut), cudaMemcpyDeviceToHost, st));
+  ctx->d2h += (size_t)n_ant * n_prn * sizeof(CellOut);
   ctx->last_cells += (double)n_ant * nb * n_prn * (double)pc.P;
 }
 
@@ -342,6 +388,13 @@ std::vector<int> prn_list(int c, const tga_all_options* opt) {
   }
   return v;
 }
+
+tga_result generic_one(tga_ctx* ctx, int c, const float* d_sig, const double* d_pp, size_t n, double fs,
+                       const double* d_fc, const std::vector<double>& fc, double center, int prn, size_t period);
+
+// acr.rs:49-84 on the host, for cells of the generic path (the fused path
+// evaluates the same rule in its finalize kernel).
+bool estimate_cn0_host(double r_a, int table, double* out);
 
 int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, size_t row_bytes, double fs,
                      const tga_all_options* opt, tga_cell* out, size_t cap, size_t* n_out) {
@@ -377,15 +430,19 @@ int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, si
   const int nb = (int)fc.size();
   const size_t n_rec = row_bytes * 8;
 
-  // plan class groups
+  // plan class groups; constellations the fused kernels cannot express go
+  // to the generic path
   std::vector<ClassGroup> groups;
+  std::vector<int> generic_consts;
   for (int c : consts) {
     const size_t P = period_samples(c, fs);
+    if (P == 0) throw InvalidArg("sampling frequency too low for " + std::string(info(c).json_key));
     const size_t N = std::min(2 * P, n_rec);
     PolyClass pc;
-    if (!poly_class_for(c, (double)P, P, N, prns[c], &pc))
-      throw std::runtime_error(std::string("unsupported: ") + info(c).json_key +
-                               " at this sampling rate needs the generic path (not available for all-PRN search)");
+    if (!poly_class_for(ctx, c, (double)P, P, N, prns[c], &pc)) {
+      generic_consts.push_back(c);
+      continue;
+    }
     bool placed = false;
     for (auto& g : groups) {
       if (same_class(g.pc, pc)) {
@@ -423,11 +480,56 @@ int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, si
   src.n_ant = (int)ants.size();
   src.pc = kTau / fs;
 
-  std::map<std::pair<int, int>, CellOut> result;  // (const, prn) x ant via index below
-  std::vector<std::vector<CellOut>> gout(groups.size());
+  size_t n_group_cells = 0;
+  for (const auto& g : groups) n_group_cells += ants.size() * g.prns.size();
+  CellOut* pinned = (CellOut*)ctx->host_pinned((n_group_cells ? n_group_cells : 1) * sizeof(CellOut));
+  std::vector<CellOut*> gout(groups.size());
+  {
+    size_t off = 0;
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+      gout[gi] = pinned + off;
+      off += ants.size() * groups[gi].prns.size();
+    }
+  }
   for (size_t gi = 0; gi < groups.size(); ++gi)
     run_group(ctx, groups[gi], src, d_fc, nb, opt->center_freq, opt->cn0, chip_width_of(fs),
-              "g" + std::to_string(groups[gi].pc.P) + "_" + std::to_string(groups[gi].pc.Lc), &gout[gi]);
+              "g" + std::to_string(groups[gi].pc.P) + "_" + std::to_string(groups[gi].pc.Lc), gout[gi]);
+  // generic path: per (constellation, antenna, PRN), reference algorithm on the GPU
+  std::map<int, std::vector<CellOut>> gen_out;  // constellation -> [prn][ant]
+  for (int c : generic_consts) {
+    const size_t P = period_samples(c, fs);
+    const size_t N = std::min(2 * P, n_rec);
+    float* d_sig = (float*)ctx->buf("gen.sig", N * sizeof(float));
+    double* d_pp = (double*)ctx->buf("gen.pp", N * sizeof(double));
+    std::vector<CellOut>& v = gen_out[c];
+    v.resize(prns[c].size() * ants.size());
+    for (size_t a = 0; a < ants.size(); ++a) {
+      timed(ctx, "bits_to_signal", 0.0, [&] {
+        return launch_bits_to_signal(d_bits, row_bytes, ants[a], d_mean, (int)N, kTau / fs, d_sig, d_pp, st);
+      });
+      for (size_t i = 0; i < prns[c].size(); ++i) {
+        tga_result r = generic_one(ctx, c, d_sig, d_pp, N, fs, d_fc, fc, opt->center_freq, prns[c][i], P);
+        CellOut o{};
+        o.strength = r.signal_strength;
+        o.second = r.second_peak;
+        o.codephase_frac = r.codephase_frac;
+        o.frequency = r.frequency;
+        o.bin = r.best_freq_idx;
+        o.tau = (int32_t)r.best_codephase;
+        o.hyp = r.hypothesis;
+        o.cn0_valid = 0;
+        if (opt->cn0 && o.second > 0.0 && o.strength > o.second) {
+          const double q = o.strength / o.second;
+          double cn0 = 0.0;
+          if (estimate_cn0_host(q * q, info(c).acr_table, &cn0)) {
+            o.cn0 = cn0;
+            o.cn0_valid = 1;
+          }
+        }
+        v[i * ants.size() + a] = o;
+      }
+    }
+  }
   CK(cudaEventRecord(ctx->ev1, st));
   CK(cudaEventSynchronize(ctx->ev1));
   float ms = 0.f;
@@ -440,6 +542,26 @@ int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, si
   size_t k = 0;
   for (int c : consts) {
     for (int prn : prns[c]) {
+      if (gen_out.count(c)) {
+        const size_t i = std::find(prns[c].begin(), prns[c].end(), prn) - prns[c].begin();
+        for (size_t a = 0; a < ants.size(); ++a) {
+          const CellOut& o = gen_out[c][i * ants.size() + a];
+          tga_cell& t = out[k++];
+          t.constellation = c;
+          t.prn = prn;
+          t.antenna = ants[a];
+          t.best_freq_idx = o.bin;
+          t.best_codephase = o.tau;
+          t.signal_strength = o.strength;
+          t.second_peak = o.second;
+          t.codephase_frac = o.codephase_frac;
+          t.frequency = o.frequency;
+          t.cn0_acr = o.cn0;
+          t.cn0_valid = o.cn0_valid;
+          t.hypothesis = o.hyp;
+        }
+        continue;
+      }
       // locate group / index
       const ClassGroup* g = nullptr;
       size_t gidx = 0, pidx = 0;
@@ -453,7 +575,7 @@ int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, si
           }
       const int n_prn_g = (int)g->prns.size();
       for (size_t a = 0; a < ants.size(); ++a) {
-        const CellOut& o = gout[gidx][a * n_prn_g + pidx];
+        const CellOut o = gout[gidx][a * n_prn_g + pidx];
         tga_cell& t = out[k++];
         t.constellation = c;
         t.prn = prn;
@@ -544,7 +666,7 @@ int acquire_single_impl(tga_ctx* ctx, int c, const float* h_sig, const double* h
   std::vector<double> fc = freq_grid(center, band);
   const int nb = (int)fc.size();
   PolyClass pc;
-  const bool fused = poly_class_for(c, (double)period, period, n, {prn}, &pc);
+  const bool fused = poly_class_for(ctx, c, (double)period, period, n, {prn}, &pc);
   begin_call(ctx);
   cudaStream_t st = ctx->stream;
   float* d_sig = (float*)ctx->buf("single.sig", n * sizeof(float));
@@ -573,12 +695,13 @@ int acquire_single_impl(tga_ctx* ctx, int c, const float* h_sig, const double* h
   g.pc = pc;
   g.consts.push_back(c);
   g.prns.push_back({c, prn});
-  std::vector<CellOut> cells;
   ctx->h2d += n * (sizeof(float) + sizeof(double));
-  run_group(ctx, g, src, d_fc, nb, center, 0, chip_width_of(fs), "single", &cells);
+  CellOut* cell = (CellOut*)ctx->host_pinned(sizeof(CellOut));
+  run_group(ctx, g, src, d_fc, nb, center, 0, chip_width_of(fs), "single", cell);
+  CK(cudaStreamSynchronize(st));
   ctx->last_launches = kernel_launch_count();
   collect_times(ctx);
-  const CellOut& o = cells[0];
+  const CellOut o = *cell;
   out->prn = prn;
   out->best_freq_idx = o.bin;
   out->best_codephase = o.tau;
@@ -589,6 +712,32 @@ int acquire_single_impl(tga_ctx* ctx, int c, const float* h_sig, const double* h
   out->hypothesis = o.hyp;
   out->path = 0;
   return TGA_OK;
+}
+
+bool estimate_cn0_host(double r_a, int table, double* out) {
+  const double(*t)[2];
+  int n;
+  switch (table) {
+    case TGA_ACR_GPS_L1_CA: t = TGA_GPS_L1_CA_ACR_TABLE; n = 59; break;
+    case TGA_ACR_GALILEO_E1C: t = TGA_GALILEO_E1C_ACR_TABLE; n = 71; break;
+    case TGA_ACR_BEIDOU_B1C: t = TGA_BEIDOU_B1C_ACR_TABLE; n = 79; break;
+    default: t = TGA_GPS_L1C_ACR_TABLE; n = 79; break;
+  }
+  if (!(r_a > 1.0) || !std::isfinite(r_a)) return false;
+  if (r_a <= t[0][0]) { *out = t[0][1]; return true; }
+  if (r_a >= t[n - 1][0]) { *out = t[n - 1][1]; return true; }
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) / 2;
+    if (t[mid][0] < r_a) lo = mid + 1; else hi = mid;
+  }
+  if (lo == 0) { *out = t[0][1]; return true; }
+  if (lo >= n) { *out = t[n - 1][1]; return true; }
+  const double la = std::log(t[lo - 1][0]), lb = std::log(t[lo][0]);
+  const double tt = (std::log(r_a) - la) / (lb - la);
+  double v = t[lo - 1][1] + tt * (t[lo][1] - t[lo - 1][1]);
+  *out = std::min(70.0, std::max(20.0, v));
+  return true;
 }
 
 }  // namespace
@@ -633,6 +782,7 @@ int tga_destroy(tga_ctx* ctx) {
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return TGA_OK;
