@@ -168,6 +168,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--n-ant", type=int, default=N_ANT, help="antennas per GPU (profiling runs use fewer)")
+    ap.add_argument("--variant10", type=int, default=None, help="launch-shape variant of the Lc=10230 kernels")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -192,6 +193,8 @@ def main():
     pinned.numpy()[:] = bits_np
     d_bits = pinned.to("cuda", non_blocking=False)
     ctx = tga.Context(local)
+    if args.variant10 is not None:
+        tga.lib().tga_set_variant(ctx._h, 10230, args.variant10)
     stream = torch.cuda.ExternalStream(tga.lib().tga_stream(ctx._h))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     lib = tga.lib()

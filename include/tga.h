@@ -191,6 +191,10 @@ void* tga_stream(tga_ctx* ctx);
  * on the context stream).  tga_kernel_times returns, for the last call, up
  * to cap entries of (kernel name, total ms, launches, algorithmic FLOPs). */
 int tga_set_profiling(tga_ctx* ctx, int enable);
+/* Launch-shape variant of the transform kernels for chip count lc (1023,
+ * 4092, 10230): 0 = default; 1 (10230 only) = two polyphase branches per
+ * CTA sharing the code spectrum.  Results are identical; only speed varies. */
+int tga_set_variant(tga_ctx* ctx, int lc, int variant);
 int tga_kernel_times(const tga_ctx* ctx, int cap, const char** names, double* ms,
                      int32_t* launches, double* flops, int* n);
 

@@ -232,8 +232,8 @@ struct PfaParams {
   BestRow* best;              // SECOND in/out
 };
 
-template <int M, int BC, int NT, int MODE>
-__global__ void __launch_bounds__(NT, 2) pfa_kernel(PfaParams p) {
+template <int M, int BC, int NT, int MINB, int MODE>
+__global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
   using G = Geo<M>;
   constexpr int COLS = G::COLS, LC = G::LC, NC = G::NC;
   constexpr bool INV = (MODE == CORR || MODE == SECOND);
@@ -257,7 +257,17 @@ __global__ void __launch_bounds__(NT, 2) pfa_kernel(PfaParams p) {
       tau_star = b.tau;
     }
     const int hyp = ab_h & 1;
-    unsigned long long kbest = 0ull;
+    // CORR: running maximum of |y|^2 and a compact code of its position
+    // ((rho*31 + a)*33 + b)*16 + c; the lag is decoded only on ties and once
+    // per item, which keeps the per-output epilogue to a compare and selects.
+    float pmax = -1.f;
+    int cmax = 0;
+    auto lag_of = [&](int code) -> int {
+      const int c = code & 15, q = code >> 4;
+      const int b = q % 33, q2 = q / 33;
+      const int a = q2 % 31, rho = q2 / 31;
+      return rho + S * G::natural(a, b, c);
+    };
     float pbest = 0.f;
     if (tid == 0) {
       s_key = 0ull;
@@ -282,12 +292,16 @@ __global__ void __launch_bounds__(NT, 2) pfa_kernel(PfaParams p) {
           p.Dout[(size_t)seq_of(s) * LC + G::offset(a, b, c)] = make_float2(v.x, -v.y);
         } else {
           const float pw = fmaf(v.x, v.x, v.y * v.y);
-          const int tau = seq_of(s) + S * G::natural(a, b, c);
           if (MODE == CORR) {
-            const unsigned long long key =
-                ((unsigned long long)__float_as_uint(pw) << 32) | (unsigned)tau;
-            kbest = key > kbest ? key : kbest;
+            const int code = ((seq_of(s) * 31 + a) * 33 + b) * 16 + c;
+            if (pw == pmax) {
+              // exact tie: the reference keeps the later lag (Iterator::max_by)
+              if (lag_of(code) > lag_of(cmax)) cmax = code;
+            }
+            cmax = pw > pmax ? code : cmax;
+            pmax = fmaxf(pw, pmax);
           } else {
+            const int tau = seq_of(s) + S * G::natural(a, b, c);
             int d = tau - tau_star;
             d = d < 0 ? -d : d;
             const int dist = min(d, p.P - d);
@@ -306,7 +320,9 @@ __global__ void __launch_bounds__(NT, 2) pfa_kernel(PfaParams p) {
           const float2* zs = p.z + ((size_t)ab_h * S + q) * LC + col;
           const float2* ds = p.D + ((size_t)prn * 2 + hyp) * LC + col;
 #pragma unroll
-          for (int a = 0; a < 31; ++a) x[a] = cmul(__ldg(zs + a * COLS), __ldg(ds + a * COLS));
+          // Z is read once per (row, rho): keep it out of L1 so the code
+          // spectrum D, reused by every rho of the row, stays there.
+          for (int a = 0; a < 31; ++a) x[a] = cmul(__ldcg(zs + a * COLS), __ldg(ds + a * COLS));
         } else if (MODE == FWD_Z) {
           const float2* zs = p.z + (size_t)q * LC;
           const int c = col / 33, b = col - c * 33;
@@ -368,6 +384,8 @@ __global__ void __launch_bounds__(NT, 2) pfa_kernel(PfaParams p) {
     }
 
     if (MODE == CORR) {
+      unsigned long long kbest =
+          pmax < 0.f ? 0ull : (((unsigned long long)__float_as_uint(pmax) << 32) | (unsigned)lag_of(cmax));
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long other = __shfl_xor_sync(0xffffffffu, kbest, o);
@@ -387,33 +405,46 @@ __global__ void __launch_bounds__(NT, 2) pfa_kernel(PfaParams p) {
   }
 }
 
-// Launch configuration per third digit M: (slots per CTA, threads per CTA).
-template <int M>
+// Launch configurations: (third digit M, slots per CTA, threads, min CTAs/SM).
+// Variant 0 is the default; the other variants are alternatives kept for
+// tuning (selected with tga_set_variant).
+template <int M, int V>
 struct PfaCfg;
 template <>
-struct PfaCfg<1> {
-  static constexpr int BC = 8, NT = 288;  // 8 x 33 DFT-31 columns
+struct PfaCfg<1, 0> {
+  static constexpr int BC = 8, NT = 288, MINB = 2;  // 8 x 33 DFT-31 columns
 };
 template <>
-struct PfaCfg<4> {
-  static constexpr int BC = 2, NT = 288;  // 2 x 132 columns
+struct PfaCfg<4, 0> {
+  static constexpr int BC = 2, NT = 288, MINB = 2;  // 2 x 132 columns
 };
 template <>
-struct PfaCfg<10> {
-  static constexpr int BC = 1, NT = 352;  // 330 columns
+struct PfaCfg<10, 0> {
+  static constexpr int BC = 1, NT = 352, MINB = 2;  // 330 columns
+};
+template <>
+struct PfaCfg<10, 1> {
+  static constexpr int BC = 2, NT = 704, MINB = 1;  // two rho slots share D in L1
 };
 
-template <int M, int MODE>
-static cudaError_t run_pfa(const PfaParams& p, int n_work, int num_sms, cudaStream_t st) {
-  using C = PfaCfg<M>;
+static int g_variant10 = 0;
+void set_pfa_variant(int M, int v) {
+  if (M == 10) g_variant10 = v;
+}
+
+template <int M, int V, int MODE>
+static cudaError_t run_pfa(const PfaParams& p, int n_work_slots, int num_sms, cudaStream_t st) {
+  using C = PfaCfg<M, V>;
   constexpr int LC = Geo<M>::LC;
   const size_t smem = (size_t)C::BC * LC * sizeof(float2);
-  auto kern = pfa_kernel<M, C::BC, C::NT, MODE>;
+  auto kern = pfa_kernel<M, C::BC, C::NT, C::MINB, MODE>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, smem);
   if (per_sm < 1) per_sm = 1;
+  // FWD modes: n_work_slots counts sequences, grouped BC per work unit
+  const int n_work = (MODE == FWD_Z || MODE == FWD_D) ? (n_work_slots + C::BC - 1) / C::BC : n_work_slots;
   int grid = num_sms * per_sm;
   if (grid > n_work) grid = n_work;
   if (grid < 1) return cudaSuccess;
@@ -422,11 +453,13 @@ static cudaError_t run_pfa(const PfaParams& p, int n_work, int num_sms, cudaStre
 }
 
 template <int MODE>
-static cudaError_t dispatch_pfa(int M, const PfaParams& p, int n_work, int num_sms, cudaStream_t st) {
+static cudaError_t dispatch_pfa(int M, const PfaParams& p, int n_work_slots, int num_sms, cudaStream_t st) {
   switch (M) {
-    case 1: return run_pfa<1, MODE>(p, n_work, num_sms, st);
-    case 4: return run_pfa<4, MODE>(p, n_work, num_sms, st);
-    case 10: return run_pfa<10, MODE>(p, n_work, num_sms, st);
+    case 1: return run_pfa<1, 0, MODE>(p, n_work_slots, num_sms, st);
+    case 4: return run_pfa<4, 0, MODE>(p, n_work_slots, num_sms, st);
+    case 10:
+      if (g_variant10 == 1 && (MODE == CORR || MODE == SECOND)) return run_pfa<10, 1, MODE>(p, n_work_slots, num_sms, st);
+      return run_pfa<10, 0, MODE>(p, n_work_slots, num_sms, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -437,8 +470,7 @@ cudaError_t launch_forward_z(const PolyClass& pc, int n_ab, float2* d_z, int num
   p.n_seq = n_ab * 2 * pc.S;
   p.S = pc.S;
   p.P = pc.P;
-  const int bc = pc.M == 1 ? PfaCfg<1>::BC : pc.M == 4 ? PfaCfg<4>::BC : PfaCfg<10>::BC;
-  return dispatch_pfa<FWD_Z>(pc.M, p, (p.n_seq + bc - 1) / bc, num_sms, st);
+  return dispatch_pfa<FWD_Z>(pc.M, p, p.n_seq, num_sms, st);
 }
 
 cudaError_t launch_code_spectra(const PolyClass& pc, const int8_t* d_chips, int n_prn, float2* d_D,
@@ -449,8 +481,7 @@ cudaError_t launch_code_spectra(const PolyClass& pc, const int8_t* d_chips, int 
   p.n_seq = n_prn * 2;
   p.S = pc.S;
   p.P = pc.P;
-  const int bc = pc.M == 1 ? PfaCfg<1>::BC : pc.M == 4 ? PfaCfg<4>::BC : PfaCfg<10>::BC;
-  return dispatch_pfa<FWD_D>(pc.M, p, (p.n_seq + bc - 1) / bc, num_sms, st);
+  return dispatch_pfa<FWD_D>(pc.M, p, p.n_seq, num_sms, st);
 }
 
 cudaError_t launch_correlate(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,

@@ -95,6 +95,10 @@ size_t generic_work_elems(const GenericPlan& gp, int nb);
 cudaError_t launch_bits_to_signal(const uint8_t* d_bits, size_t row_bytes, int row, const double* d_mean, int n,
                                   double pc, float* d_sig, double* d_pp, cudaStream_t st);
 
+// Selects an alternative launch configuration of the transform kernels for
+// third digit M (tuning; 0 = default).
+void set_pfa_variant(int M, int v);
+
 int kernel_launch_count_reset();
 void kernel_launch_add(int n);
 int kernel_launch_count();

@@ -866,6 +866,12 @@ int tga_last_transfer_bytes(const tga_ctx* ctx, uint64_t* h2d, uint64_t* d2h) {
 
 void* tga_stream(tga_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
+int tga_set_variant(tga_ctx* ctx, int lc, int variant) {
+  if (!ctx || (lc != 1023 && lc != 4092 && lc != 10230) || variant < 0 || variant > 1) return TGA_ERR_INVALID_ARG;
+  set_pfa_variant(lc / 1023, variant);
+  return TGA_OK;
+}
+
 int tga_set_profiling(tga_ctx* ctx, int enable) {
   if (!ctx) return TGA_ERR_INVALID_ARG;
   ctx->profiling = enable != 0;
