@@ -148,6 +148,34 @@ int tga_acquire_l1c_single(tga_ctx* ctx, const float* h_signal_f32, const double
                            double search_band, int prn, size_t samples_per_chunk,
                            tga_result* out);
 
+/* ---- single-PRN search without allocation ------------------------------------
+ * Has no counterpart in the reference.  For callers that cannot call
+ * cudaMalloc while they run: a real-time receiver loop (cudaMalloc can
+ * synchronise the device and take unbounded time), a process whose device
+ * memory is already held by another framework's caching allocator, or a
+ * host that only allows memory reserved when the library was loaded.  Same
+ * search and result as tga_acquire_single on the fused path, but inputs and
+ * the result are DEVICE pointers (n samples, n phase points, one
+ * tga_result) and the work is queued on `stream` (a cudaStream_t; NULL =
+ * default stream) without synchronising.  It needs no context.
+ *
+ * Scratch comes from one fixed 16 MiB array in the library's device memory
+ * (held on every GPU that loads the library until the process exits).  A
+ * search needs n_bins * 2 * samples_per_chunk * 8 bytes plus ~0.2 MB: for
+ * example GPS / SBAS / QZSS at 16.368 MHz with up to 61 bins (the
+ * reference's +-6 kHz / 300 Hz grid has 41), or any constellation at the
+ * reference's 1.023-2.046 MHz test rates.  Larger searches return
+ * TGA_ERR_CAPACITY; windows other than two periods with a whole number of
+ * samples per chip return TGA_ERR_UNSUPPORTED.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) and uploads
+ * constant tables: make it before any stream capture.  Every call shares the
+ * array and leaves its contents behind (each call writes every part it
+ * reads first); calls that overlap on the GPU race on it, so serialise them. */
+int tga_acquire_single_static(int constellation, const float* d_signal_f32,
+                              const double* d_phasepoints, size_t num_samples,
+                              double sampling_freq, double center_freq, double search_band,
+                              int prn, size_t samples_per_chunk, tga_result* d_out, void* stream);
+
 /* ---- all-PRN, all-antenna search ------------------------------------------
  * Replaces acquire_all_gps (acquisition.rs:261), acquire_all_sbas
  * (sbas.rs:216), acquire_all_qzss (qzss.rs:219), acquire_all_galileo

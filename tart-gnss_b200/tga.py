@@ -107,6 +107,7 @@ def lib():
     L.tga_stream.restype = ctypes.c_void_p
     L.tga_set_profiling.argtypes = [_P, i32]
     L.tga_set_variant.argtypes = [_P, i32, i32]
+    L.tga_acquire_single_static.argtypes = [i32, _P, _P, sz, dbl, dbl, dbl, i32, sz, _P, _P]
     L.tga_last_transfer_bytes.argtypes = [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.tga_kernel_times.argtypes = [_P, i32, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_int)]
     _lib = L
