@@ -169,6 +169,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--n-ant", type=int, default=N_ANT, help="antennas per GPU (profiling runs use fewer)")
     ap.add_argument("--variant10", type=int, default=None, help="launch-shape variant of the Lc=10230 kernels")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16tc"],
+                    help="search arithmetic: FP32 CUDA cores, or FP16 tensor-core DFT-31 with FP32 refinement")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -195,6 +197,8 @@ def main():
     ctx = tga.Context(local)
     if args.variant10 is not None:
         tga.lib().tga_set_variant(ctx._h, 10230, args.variant10)
+    if args.precision == "fp16tc":
+        ctx.set_precision(tga.PRECISION_FP16_TC)
     stream = torch.cuda.ExternalStream(tga.lib().tga_stream(ctx._h))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     lib = tga.lib()
@@ -290,7 +294,7 @@ def main():
 
     line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f16-tc+f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "n_ant": n_ant, "cells_per_step_per_gpu": cells,
                        "l2": "256 MB buffer written between timed steps; 3.9 GB intermediate per step",
                        "parallelism": "replicas (weak scaling: one 24-antenna observation per GPU)"},

@@ -219,6 +219,17 @@ void* tga_stream(tga_ctx* ctx);
  * on the context stream).  tga_kernel_times returns, for the last call, up
  * to cap entries of (kernel name, total ms, launches, algorithmic FLOPs). */
 int tga_set_profiling(tga_ctx* ctx, int enable);
+/* Arithmetic of the correlation search.
+ *  TGA_PRECISION_FP32 (default): every transform stage in FP32 on the CUDA
+ *    cores; results within 1e-4 of the reference algorithm.
+ *  TGA_PRECISION_FP16_TC: the DFT-31 stage of the search runs on the tensor
+ *    cores (tcgen05, FP16 operands, FP32 accumulation); the row chosen for
+ *    every (antenna, PRN) is then re-evaluated in FP32, so reported peak, lag
+ *    and second peak are FP32 values; only the choice of Doppler bin and
+ *    hypothesis among near-equal candidates can differ from the FP32 mode. */
+#define TGA_PRECISION_FP32 0
+#define TGA_PRECISION_FP16_TC 1
+int tga_set_precision(tga_ctx* ctx, int precision);
 /* Launch-shape variant of the transform kernels for chip count lc (1023,
  * 4092, 10230): 0 = default; 1 (10230 only) = two polyphase branches per
  * CTA sharing the code spectrum.  Results are identical; only speed varies. */

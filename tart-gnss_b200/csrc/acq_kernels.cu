@@ -31,6 +31,7 @@
 #include "dft.cuh"
 #include "engine.h"
 #include "gnss_tables.h"
+#include "pfa_common.cuh"
 
 namespace tga {
 
@@ -44,30 +45,6 @@ int kernel_launch_count() { return g_launches; }
 void kernel_launch_add(int n) { g_launches += n; }
 
 #define TGA_LAUNCHED() (++g_launches, cudaGetLastError())
-
-constexpr int modinv_c(int a, int m) {
-  a %= m;
-  for (int x = 1; x < m; ++x)
-    if ((a * x) % m == 1) return x;
-  return 0;
-}
-
-// Geometry of the Lc = 31 * 33 * M prime-factor transform.
-template <int M>
-struct Geo {
-  static constexpr int NC = M;
-  static constexpr int COLS = 33 * M;  // columns of the DFT-31 stage
-  static constexpr int LC = 31 * COLS;
-  // natural index n = (a*EA + b*EB + c*EC) mod LC for digits (a, b, c)
-  static constexpr int EA = (LC / 31) * modinv_c((LC / 31) % 31, 31);
-  static constexpr int EB = (LC / 33) * modinv_c((LC / 33) % 33, 33);
-  static constexpr int EC = (M == 1) ? 0 : (LC / M) * modinv_c((LC / M) % M, M);
-  __device__ static __forceinline__ int natural(int a, int b, int c) {
-    return (int)((unsigned)(a * EA + b * EB + c * EC) % (unsigned)LC);
-  }
-  // digit-layout offset of (a, b, c): [a][c][b]
-  __device__ static __forceinline__ int offset(int a, int b, int c) { return a * COLS + c * 33 + b; }
-};
 
 // ---------------------------------------------------------------------------
 // antenna means: mean of the +-1 samples over the whole row (acquisition.rs:285)
@@ -218,25 +195,12 @@ cudaError_t launch_frontend(const SampleSource& src, const SearchDims& dims, con
 // ---------------------------------------------------------------------------
 // prime-factor transform engine
 // ---------------------------------------------------------------------------
-enum PfaMode { FWD_Z = 0, FWD_D = 1, CORR = 2, SECOND = 3 };
-
-struct PfaParams {
-  float2* z;                  // FWD_Z: sequences, transformed in place; CORR/SECOND: Z
-  const float2* D;            // CORR/SECOND: conjugated code spectra
-  float2* Dout;               // FWD_D output
-  const int8_t* chips;        // FWD_D input [n_prn][Lc]
-  int n_seq;                  // FWD modes
-  int n_items;                // CORR: n_ab*2*n_prn rows; SECOND: n_ant*n_prn
-  int n_prn, S, P, chip_width;
-  unsigned long long* keys;   // CORR output, one per row
-  BestRow* best;              // SECOND in/out
-};
-
 template <int M, int BC, int NT, int MINB, int MODE>
 __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
   using G = Geo<M>;
   constexpr int COLS = G::COLS, LC = G::LC, NC = G::NC;
-  constexpr bool INV = (MODE == CORR || MODE == SECOND);
+  constexpr bool INV = (MODE == CORR || MODE == SECOND || MODE == REFINE);
+  constexpr bool ARGMAX = (MODE == CORR || MODE == REFINE);
   extern __shared__ float2 buf[];
   __shared__ unsigned long long s_key;
   __shared__ unsigned int s_p2;
@@ -250,7 +214,7 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
     if (MODE == CORR) {
       ab_h = w / p.n_prn;
       prn = w - ab_h * p.n_prn;
-    } else if (MODE == SECOND) {
+    } else if (MODE == SECOND || MODE == REFINE) {
       const BestRow b = p.best[w];
       ab_h = b.ab * 2 + b.hyp;
       prn = w % p.n_prn;
@@ -292,7 +256,7 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
           p.Dout[(size_t)seq_of(s) * LC + G::offset(a, b, c)] = make_float2(v.x, -v.y);
         } else {
           const float pw = fmaf(v.x, v.x, v.y * v.y);
-          if (MODE == CORR) {
+          if (ARGMAX) {
             const int code = ((seq_of(s) * 31 + a) * 33 + b) * 16 + c;
             if (pw == pmax) {
               // exact tie: the reference keeps the later lag (Iterator::max_by)
@@ -316,7 +280,7 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
         const int q = seq_of(s);
         if (q < 0) continue;
         float2 x[31];
-        if (MODE == CORR || MODE == SECOND) {
+        if (INV) {
           const float2* zs = p.z + ((size_t)ab_h * S + q) * LC + col;
           const float2* ds = p.D + ((size_t)prn * 2 + hyp) * LC + col;
 #pragma unroll
@@ -383,7 +347,7 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
       __syncthreads();
     }
 
-    if (MODE == CORR) {
+    if (ARGMAX) {
       unsigned long long kbest =
           pmax < 0.f ? 0ull : (((unsigned long long)__float_as_uint(pmax) << 32) | (unsigned)lag_of(cmax));
 #pragma unroll
@@ -393,7 +357,14 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
       }
       if ((tid & 31) == 0) atomicMax(&s_key, kbest);
       __syncthreads();
-      if (tid == 0) p.keys[w] = s_key;
+      if (tid == 0) {
+        if (MODE == CORR) {
+          p.keys[w] = s_key;
+        } else {
+          p.best[w].tau = (int)(unsigned)(s_key & 0xffffffffull);
+          p.best[w].p = __uint_as_float((unsigned)(s_key >> 32));
+        }
+      }
     } else if (MODE == SECOND) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) pbest = fmaxf(pbest, __shfl_xor_sync(0xffffffffu, pbest, o));
@@ -458,7 +429,8 @@ static cudaError_t dispatch_pfa(int M, const PfaParams& p, int n_work_slots, int
     case 1: return run_pfa<1, 0, MODE>(p, n_work_slots, num_sms, st);
     case 4: return run_pfa<4, 0, MODE>(p, n_work_slots, num_sms, st);
     case 10:
-      if (g_variant10 == 1 && (MODE == CORR || MODE == SECOND)) return run_pfa<10, 1, MODE>(p, n_work_slots, num_sms, st);
+      if (g_variant10 == 1 && (MODE == CORR || MODE == SECOND || MODE == REFINE))
+        return run_pfa<10, 1, MODE>(p, n_work_slots, num_sms, st);
       return run_pfa<10, 0, MODE>(p, n_work_slots, num_sms, st);
   }
   return cudaErrorInvalidValue;
@@ -511,6 +483,19 @@ cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, cons
   p.chip_width = chip_width;
   p.n_items = dims.n_ant * dims.n_prn;
   return dispatch_pfa<SECOND>(pc.M, p, p.n_items, num_sms, st);
+}
+
+cudaError_t launch_refine(const PolyClass& pc, const SearchDims& dims, const float2* d_Z, const float2* d_D,
+                          BestRow* d_best, int num_sms, cudaStream_t st) {
+  PfaParams p = {};
+  p.z = const_cast<float2*>(d_Z);
+  p.D = d_D;
+  p.best = d_best;
+  p.n_prn = dims.n_prn;
+  p.S = pc.S;
+  p.P = pc.P;
+  p.n_items = dims.n_ant * dims.n_prn;
+  return dispatch_pfa<REFINE>(pc.M, p, p.n_items, num_sms, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -66,6 +66,14 @@ cudaError_t launch_code_spectra(const PolyClass& pc, const int8_t* d_chips, int 
 cudaError_t launch_correlate(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
                              const float2* d_D, unsigned long long* d_keys, int num_sms,
                              cudaStream_t st);
+// FP32 re-evaluation of each (antenna, PRN)'s selected row: rewrites best.p / best.tau.
+cudaError_t launch_refine(const PolyClass& pc, const SearchDims& dims, const float2* d_Z, const float2* d_D,
+                          BestRow* d_best, int num_sms, cudaStream_t st);
+// Tensor-core correlator (FP16 operands, FP32 accumulation in TMEM) for the
+// DFT-31 stage; keys hold |y|^2 scaled by 2^-2k (comparisons only).  *d_err
+// is set non-zero when a bounded wait on the tensor cores expired.
+cudaError_t launch_correlate_tc(const PolyClass& pc, const SearchDims& dims, const float2* d_Z, const float2* d_D,
+                                unsigned long long* d_keys, int* d_err, int num_sms, cudaStream_t st);
 cudaError_t launch_reduce_bins(const SearchDims& dims, const unsigned long long* d_keys,
                                BestRow* d_best, cudaStream_t st);
 cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,

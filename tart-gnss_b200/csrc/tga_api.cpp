@@ -51,6 +51,7 @@ struct tga_ctx {
   int last_launches = 0;
   double last_ms = 0.0;
   uint64_t h2d = 0, d2h = 0;
+  int precision = 0;  // TGA_PRECISION_*
   // per-kernel event timing
   bool profiling = false;
   struct Pending {
@@ -66,6 +67,7 @@ struct tga_ctx {
     int launches = 0;
   };
   std::vector<std::pair<std::string, KTime>> ktimes;
+  int* tc_err_pending = nullptr;  // device flag of the last tensor-core launch
   // planning caches: verified polyphase classes, host chips, uploaded chips
   struct ClassCache {
     bool structure_ok = false;
@@ -129,6 +131,10 @@ struct CudaError : std::runtime_error {
       throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));                \
   } while (0)
 
+struct TimeoutError : std::runtime_error {
+  explicit TimeoutError(const std::string& s) : std::runtime_error(s) {}
+};
+
 struct InvalidArg : std::invalid_argument {
   explicit InvalidArg(const std::string& s) : std::invalid_argument(s) {}
 };
@@ -143,6 +149,9 @@ int guarded(tga_ctx* ctx, F&& f) {
   } catch (const CudaError& e) {
     ctx->err = e.what();
     return TGA_ERR_CUDA;
+  } catch (const TimeoutError& e) {
+    ctx->err = e.what();
+    return TGA_ERR_TIMEOUT;
   } catch (const std::invalid_argument& e) {
     ctx->err = e.what();
     return TGA_ERR_INVALID_ARG;
@@ -219,6 +228,15 @@ void collect_times(tga_ctx* ctx) {
     it->second.launches += 1;
   }
   ctx->pending.clear();
+}
+
+// After the stream is idle: did a tensor-core wait expire?
+void check_tc_error(tga_ctx* ctx) {
+  if (!ctx->tc_err_pending) return;
+  int flag = 0;
+  CK(cudaMemcpy(&flag, ctx->tc_err_pending, sizeof(int), cudaMemcpyDeviceToHost));
+  ctx->tc_err_pending = nullptr;
+  if (flag) throw TimeoutError("tensor-core correlator: a bounded wait on the MMA pipeline expired");
 }
 
 // FP32 operations per transform point of one length-Lc inverse transform as
@@ -357,9 +375,22 @@ void run_group(tga_ctx* ctx, const ClassGroup& grp, const SampleSource& src, con
         [&] { return launch_frontend(src, dims, pc, d_z, st); });
   timed(ctx, ("forward_z" + cls).c_str(), (double)n_ab * 2 * pc.P * tf,
         [&] { return launch_forward_z(pc, n_ab, d_z, ctx->num_sms, st); });
-  timed(ctx, ("correlate" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * (tf + 9.0),
-        [&] { return launch_correlate(pc, dims, d_z, d_D, d_keys, ctx->num_sms, st); });
+  if (ctx->precision == TGA_PRECISION_FP16_TC) {
+    int* d_err = (int*)ctx->buf("tc.err", sizeof(int));
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    // tensor-core FLOPs per point: 2 x 64 x 64 / 31 (DFT-31 GEMM) + FP32 rest
+    const double tc_flops = 2.0 * 64 * 64 / 31.0;
+    timed(ctx, ("correlate_tc" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * (tc_flops + tf - 1950.0 / 31.0 + 9.0),
+          [&] { return launch_correlate_tc(pc, dims, d_z, d_D, d_keys, d_err, ctx->num_sms, st); });
+    ctx->tc_err_pending = d_err;
+  } else {
+    timed(ctx, ("correlate" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * (tf + 9.0),
+          [&] { return launch_correlate(pc, dims, d_z, d_D, d_keys, ctx->num_sms, st); });
+  }
   timed(ctx, ("reduce_bins" + cls).c_str(), 0.0, [&] { return launch_reduce_bins(dims, d_keys, d_best, st); });
+  if (ctx->precision == TGA_PRECISION_FP16_TC)
+    timed(ctx, ("refine" + cls).c_str(), (double)n_ant * n_prn * pc.P * (tf + 9.0),
+          [&] { return launch_refine(pc, dims, d_z, d_D, d_best, ctx->num_sms, st); });
   timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * pc.P * (tf + 9.0),
         [&] { return launch_second_peak(pc, dims, d_z, d_D, d_best, chip_width, ctx->num_sms, st); });
   timed(ctx, ("finalize" + cls).c_str(), 0.0,
@@ -537,6 +568,7 @@ int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, si
   ctx->last_ms = ms;
   ctx->last_launches = kernel_launch_count();
   collect_times(ctx);
+  check_tc_error(ctx);
 
   // assemble in (constellation, prn order, antenna) order
   size_t k = 0;
@@ -701,6 +733,7 @@ int acquire_single_impl(tga_ctx* ctx, int c, const float* h_sig, const double* h
   CK(cudaStreamSynchronize(st));
   ctx->last_launches = kernel_launch_count();
   collect_times(ctx);
+  check_tc_error(ctx);
   const CellOut o = *cell;
   out->prn = prn;
   out->best_freq_idx = o.bin;
@@ -865,6 +898,12 @@ int tga_last_transfer_bytes(const tga_ctx* ctx, uint64_t* h2d, uint64_t* d2h) {
 }
 
 void* tga_stream(tga_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int tga_set_precision(tga_ctx* ctx, int precision) {
+  if (!ctx || (precision != TGA_PRECISION_FP32 && precision != TGA_PRECISION_FP16_TC)) return TGA_ERR_INVALID_ARG;
+  ctx->precision = precision;
+  return TGA_OK;
+}
 
 int tga_set_variant(tga_ctx* ctx, int lc, int variant) {
   if (!ctx || (lc != 1023 && lc != 4092 && lc != 10230) || variant < 0 || variant > 1) return TGA_ERR_INVALID_ARG;

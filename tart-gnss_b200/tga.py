@@ -32,6 +32,7 @@ ALL = 0x3F
 GPS_IF = 4.092e6
 GPS_SEARCH_BAND = 6000.0
 ACR_TABLE = {GPS: 0, SBAS: 0, QZSS: 0, GALILEO: 1, BEIDOU: 2, L1C: 3}
+PRECISION_FP32, PRECISION_FP16_TC = 0, 1
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no sm_100 device", 4: "out of memory",
           5: "unsupported", 6: "timeout", 7: "capacity"}
@@ -107,6 +108,7 @@ def lib():
     L.tga_stream.restype = ctypes.c_void_p
     L.tga_set_profiling.argtypes = [_P, i32]
     L.tga_set_variant.argtypes = [_P, i32, i32]
+    L.tga_set_precision.argtypes = [_P, i32]
     L.tga_acquire_single_static.argtypes = [i32, _P, _P, sz, dbl, dbl, dbl, i32, sz, _P, _P]
     L.tga_last_transfer_bytes.argtypes = [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.tga_kernel_times.argtypes = [_P, i32, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_int)]
@@ -305,6 +307,10 @@ class Context:
             results.sort(key=lambda r: r["sv"])
             out[NAMES[c]] = {"antenna_numbers": ants, "results": results}
         return out
+
+    def set_precision(self, precision):
+        """0 = FP32 (default), 1 = FP16 tensor-core search with FP32 refinement."""
+        self._check(lib().tga_set_precision(self._h, int(precision)))
 
     def last_stats(self):
         cells, launches, ms = ctypes.c_double(), ctypes.c_int32(), ctypes.c_double()
