@@ -1,35 +1,45 @@
 // Tensor-core correlator (sm_100a, tcgen05): reduced-precision search.
 //
-// Same transform as pfa_kernel<..,CORR> (acq_kernels.cu), but the DFT-31 stage
-// -- half of the FP32 work -- runs on the 5th-generation tensor cores:
+// The inverse transform of every product Z * conj(C) (length Lc = 31 R2 R3,
+// (R2, R3) = (3, 11), (12, 11), (30, 11) for Lc = 1023, 4092, 10230) is a
+// Good-Thomas prime-factor transform whose three stages -- DFT-31, DFT-R2,
+// DFT-R3 -- all run on the 5th-generation tensor cores as GEMMs:
 //
-//   U[col][ta] = sum_ka X[col][ka] * W31^(ta*ka)        (inverse DFT, 31 points)
+//   stage i:  D_i[row][n] = sum_k A_i[row][k] * B_i[n][k]
+//     A_i   = data, one row per transform column, K = 2 R_i halves
+//             (R_i complex FP16 inputs as interleaved (re, im)), K-major
+//     B_i   = the inverse DFT-R_i as a real 2R_i x 2R_i matrix, FP16
+//     D_i   = FP32 accumulator in tensor memory (TMEM), one lane per row.
 //
-// is one GEMM per group of transform columns, D = A * B^T with
-//   A = data, M = 128 columns per tile, K = 64 = 31 complex inputs as
-//       interleaved (re, im) FP16 pairs + 2 zeros,
-//   B = DFT-31 as a real 64 x 64 matrix (N = 31 complex outputs interleaved),
-//   D = FP32 accumulator in tensor memory (TMEM), one lane per column.
-// Both operands are K-major with the 128-byte swizzle in shared memory.  One
-// elected thread issues 4 K-steps of tcgen05.mma (M128 N64 K16) per tile and
-// commits to an mbarrier; each warp then reads its 32 TMEM lanes
-// (tcgen05.ld 32x32b) straight into the FP32 shared buffer of the DFT-33 /
-// DFT-M stages, which aliases the operand tiles (the MMA has completed).
+// Between stages the warps read D_i from TMEM (tcgen05.ld 32x32b), round it
+// to FP16 and scatter it into the next stage's operand rows; this is the
+// transposition of the prime-factor map.  The last stage's accumulator is
+// read straight into the |y|^2 maximum, so no intermediate leaves the SM.
+// The products are formed in FP16 (HMUL2/HFMA2) from FP16 copies of Z and
+// conj(C) in a frequency layout matched to the (31, R2, R3) map
+// (tc_pack_kernel), and a CTA keeps its Z in registers for all PRNs, so the
+// search reads only the code spectra from L2.
 //
-// FP16 range: the complex products Z*conj(C) are scaled by 2^-k with
-// 4 S Lc^2 2^-k <= 32768 (an upper bound on |Z*D|), so no operand overflows.
+// Scaling: Z and conj(C) are stored as Z 2^-kz and conj(C) 2^-kd with
+// kz + kd = k and 4 S Lc^2 2^-k <= 32768.  Then |Z 2^-kz| <= 4 S Lc 2^-kz and
+// |C 2^-kd| <= Lc 2^-kd stay inside FP16, every product is below 32768 and so
+// is every correlation value; stage outputs are rounded with satfinite.
 // Keys carry |y|^2 2^-2k and are only compared; the selected row of every
 // (antenna, PRN) is re-evaluated in FP32 afterwards (launch_refine), so the
 // reported peak, lag and second peak are FP32 values.
 //
-// Waits on the tensor cores are bounded: on expiry the kernel sets *err,
-// drains (again bounded), frees its TMEM and returns.
+// One CTA per (row, group of BC code-phase residues); two CTAs per SM share
+// the SM's 512 TMEM columns and overlap one CTA's tensor-core work with the
+// other's SIMT work.  Waits on the tensor cores are bounded: on expiry the
+// kernel sets *err, drains (again bounded), frees its TMEM and returns.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
+#include <cstring>
+#include <vector>
 
-#include "dft.cuh"
 #include "engine.h"
 #include "pfa_common.cuh"
 
@@ -94,260 +104,532 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 128-byte rows,
-// 8-row groups 1024 bytes apart, sm_100 descriptor version 1.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
-  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr)
+               : "memory");
 }
-// Instruction descriptor: kind::f16, A = B = FP16, D = FP32, both K-major,
-// N = 64, M = 128.
-constexpr uint32_t kIdescF16 = (1u << 4) | (0u << 7) | (0u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
-
-// byte offset of 16-byte chunk j of row r inside a 128B-swizzled K-major tile
-__device__ __forceinline__ uint32_t sw128_off(int r, int j) {
-  return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((j ^ (r & 7)) << 4));
-}
-
-__device__ __forceinline__ uint32_t pack_h2(float lo, float hi) {
-  const __half2 h = __floats2half2_rn(lo, hi);
-  return *reinterpret_cast<const uint32_t*>(&h);
+// Reads 16 N16 TMEM columns of this warp's 32 lanes starting at taddr and
+// waits once.
+template <int N16>
+__device__ __forceinline__ void tmem_ld_cols(uint32_t taddr, uint32_t (&v)[16 * N16]) {
+#pragma unroll
+  for (int c = 0; c < N16; ++c) {
+    uint32_t(&r)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[16 * c]);
+    tmem_ld16(taddr + 16 * c, r);
+  }
+  tmem_wait_ld();
 }
 
-constexpr int kTcThreads = 384;  // 12 warps: 3 tiles x 4 TMEM lane quadrants
+// K-major layouts of the DFT matrices with the 128-byte (KB = 128) or
+// 64-byte (KB = 64) swizzle: rows of KB bytes, 8-row groups of 8 KB bytes;
+// the 16-byte chunk j of row r is stored at chunk j ^ (r & 7) (128B) or
+// j ^ ((r >> 1) & 3) (64B).
+template <int KB>
+struct Lay {
+  static_assert(KB == 128 || KB == 64, "layout");
+  __host__ __device__ static __forceinline__ uint32_t off(int r, int j) {
+    if (KB == 128) return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((j ^ (r & 7)) << 4));
+    return (uint32_t)((r >> 3) * 512 + (r & 7) * 64 + ((j ^ ((r >> 1) & 3)) << 4));
+  }
+  // shared-memory matrix descriptor (sm_100, version 1): start address,
+  // stride between 8-row groups, swizzle mode 2 (128B) or 4 (64B)
+  __device__ static __forceinline__ uint64_t desc(uint32_t addr) {
+    const uint64_t mode = KB == 128 ? 2 : 4;
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)((8 * KB) >> 4) << 32) |
+           ((uint64_t)1 << 46) | (mode << 61);
+  }
+};
+
+// Data operands use the un-swizzled K-major layout with every row 16 bytes
+// from the next inside a column of 8-half (16-byte) K chunks and chunk
+// columns lbo = rows * 16 + 16 bytes apart: byte(r, chunk c) = r * 16 + c * lbo.
+// Any store pattern is then affine in the row index, and the 16-byte pad
+// puts chunk c of a row 4 banks after chunk c - 1, so a warp writing one
+// row's K entries hits 32 different banks.
+__device__ __forceinline__ uint64_t desc_kchunks(uint32_t addr, uint32_t lbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) | ((uint64_t)(128 >> 4) << 32) |
+         ((uint64_t)1 << 46);
+}
+
+// instruction descriptor: kind::f16, A = B = FP16, D = FP32, K-major, M = 128
+constexpr uint32_t idesc_f16(int n) { return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((128u >> 4) << 24); }
+constexpr int pad16(int x) { return (x + 15) / 16 * 16; }
+constexpr int cmax3(int a, int b, int c) { return a > b ? (a > c ? a : c) : (b > c ? b : c); }
+
+constexpr int kTcThreads = 384;  // 12 warps: a multiple of the 4 TMEM lane quadrants
 constexpr int kTcTmemCols = 256;
 constexpr long long kWaitPolls = 1LL << 22;
 
-template <int M, int BC>
-struct TcGeo {
-  static constexpr int COLS = 33 * M, LC = 31 * COLS;
-  static constexpr int NCOL = BC * COLS;                  // transform columns per group
-  static constexpr int TILES = (NCOL + 127) / 128;         // 128-row MMA tiles
-  static constexpr int A_BYTES = TILES * 16384;
-  static constexpr int BUF_BYTES = BC * LC * 8;
-  static constexpr int R_BYTES = ((A_BYTES > BUF_BYTES ? A_BYTES : BUF_BYTES) + 1023) / 1024 * 1024;
+// factorisation Lc = 31 * R2 * R3 and the number of code-phase residues
+// (transforms) a CTA runs together
+template <int M>
+struct Tc3Cfg;
+template <>
+struct Tc3Cfg<1> {
+  static constexpr int R2 = 3, R3 = 11, BC = 4;
+};
+template <>
+struct Tc3Cfg<4> {
+  static constexpr int R2 = 12, R3 = 11, BC = 2;
+};
+template <>
+struct Tc3Cfg<10> {
+  static constexpr int R2 = 30, R3 = 11, BC = 1;
+};
+
+template <int M>
+struct T3 {
+  static constexpr int R2 = Tc3Cfg<M>::R2, R3 = Tc3Cfg<M>::R3, BC = Tc3Cfg<M>::BC;
+  static constexpr int LC = 1023 * M, OCOLS = 33 * M;
+  static_assert(31 * R2 * R3 == LC, "factorisation");
+  static_assert(R3 == 11, "the epilogue reads 22 TMEM columns");
+  // rows (transform columns) of each stage for one residue
+  static constexpr int ROWS1 = R2 * R3, ROWS2 = 31 * R3, ROWS3 = 31 * R2;
+  static constexpr int NR1 = BC * ROWS1, NR2 = BC * ROWS2, NR3 = BC * ROWS3;
+  static constexpr int TILES1 = (NR1 + 127) / 128, TILES2 = (NR2 + 127) / 128, TILES3 = (NR3 + 127) / 128;
+  static constexpr int K1 = 64, K2 = pad16(2 * R2), K3 = pad16(2 * R3);
+  static_assert(K2 <= 64 && K3 <= 64, "one swizzle atom per matrix row");
+  static constexpr int N1 = K1, N2 = K2, N3 = K3;
+  static constexpr int KB1 = 128, KB2 = K2 == 64 ? 128 : 64, KB3 = K3 == 64 ? 128 : 64;
+  static_assert(TILES1 * N1 <= kTcTmemCols && TILES2 * N2 <= kTcTmemCols && TILES3 * N3 <= kTcTmemCols, "TMEM");
+  // data operand regions: rows padded to whole tiles, K chunks lbo apart
+  static constexpr int LBO1 = TILES1 * 128 * 16 + 16, LBO2 = TILES2 * 128 * 16 + 16, LBO3 = TILES3 * 128 * 16 + 16;
+  static constexpr int A_RAW = cmax3(K1 / 8 * LBO1, K2 / 8 * LBO2, K3 / 8 * LBO3);
+  static constexpr int A_BYTES = (A_RAW + 1023) / 1024 * 1024;
+  static constexpr int B1_BYTES = N1 * KB1, B2_BYTES = N2 * KB2, B3_BYTES = N3 * KB3;
+  static_assert(B1_BYTES % 1024 == 0 && B2_BYTES % 1024 == 0 && B3_BYTES % 1024 == 0, "1024-byte aligned regions");
+  // product units: (row, 16-byte chunk of 4 complex inputs); U per thread
+  static constexpr int UNITS = NR1 * 8;
+  static constexpr int U = (UNITS + kTcThreads - 1) / kTcThreads;
+  static_assert(8 * ROWS1 < 65536 && 8 * LBO1 < 65536, "packed unit offsets");
+  static constexpr int SMEM_RAW = A_BYTES + B1_BYTES + B2_BYTES + B3_BYTES + 1024;
   // at least 80 KB so that no more than two CTAs (2 x 256 TMEM columns) share an SM
-  static constexpr int SMEM_RAW = R_BYTES + 8192 + 1024;
   static constexpr int SMEM = SMEM_RAW > 81920 ? SMEM_RAW : 81920;
-  static_assert(TILES <= 3, "TMEM budget: 3 tiles x 64 columns");
+  // CRT output map of the (31, R2, R3) transform: lag digits -> natural index
+  static constexpr int E1 = (LC / 31) * modinv_c((LC / 31) % 31, 31);
+  static constexpr int E2 = (LC / R2) * modinv_c((LC / R2) % R2, R2);
+  static constexpr int E3 = (LC / R3) * modinv_c((LC / R3) % R3, R3);
+  __device__ static __forceinline__ int natural(int t1, int t2, int t3) {
+    return (int)((unsigned)(t1 * E1 + t2 * E2 + t3 * E3) % (unsigned)LC);
+  }
+  // frequency digits: digit d of radix R holds natural frequency k with
+  // k = d (LC / R) (mod R); the (31, 33, M) layout of the FP32 engine follows
+  // the same rule, so both hold X[k] under digits that differ only in R2/R3
+  __device__ static __forceinline__ int freq_part(int d, int R, int E) { return ((d * (LC / R)) % R) * E; }
+  static constexpr int UB = modinv_c((LC / 33) % 33, 33);
+  static constexpr int UC = M == 1 ? 0 : modinv_c((LC / M) % M, M);
 };
 
-struct TcParams {
-  PfaParams p;
-  float in_scale;  // 2^-k applied to the products before FP16 conversion
+__device__ __forceinline__ uint32_t h2_bits(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
+__device__ __forceinline__ __half2 bits_h2(uint32_t u) { return *reinterpret_cast<__half2*>(&u); }
+__device__ __forceinline__ uint32_t pack_h2(float lo, float hi) { return h2_bits(__floats2half2_rn(lo, hi)); }
+// round two FP32 values to FP16, clamping to +-65504 instead of overflowing
+__device__ __forceinline__ uint32_t pack_h2_sat(float lo, float hi) {
+  uint32_t d;
+  asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
+// z * c for FP16 complex z = (zr, zi), c = (cr, ci), crot = (-ci, cr)
+__device__ __forceinline__ uint32_t cmul_h2(uint32_t z, uint32_t c, uint32_t crot) {
+  const __half2 zz = bits_h2(z);
+  const __half2 t = __hmul2(__low2half2(zz), bits_h2(c));
+  return h2_bits(__hfma2(__high2half2(zz), bits_h2(crot), t));
+}
+__device__ __forceinline__ void st_shared_u32(unsigned char* p, uint32_t v) { *reinterpret_cast<uint32_t*>(p) = v; }
+
+// inverse DFT-R as a real N x K matrix in layout KB, built on the host in
+// double precision and rounded once to FP16: row n = 2 t + (0 re | 1 im),
+// column k = 2 d + (0 re | 1 im), entries of exp(+2 pi i t d / R); zero
+// outside 2R x 2R
+template <int R, int N, int KB>
+void host_idft_matrix(unsigned char* dst) {
+  const double kPi = 3.14159265358979323846;
+  for (int n = 0; n < N; ++n)
+    for (int k = 0; k < KB / 2; ++k) {
+      double val = 0.0;
+      if (n < 2 * R && k < 2 * R) {
+        const int t = n >> 1, u = n & 1, d = k >> 1, v = k & 1;
+        const double ang = 2.0 * kPi * (double)((t * d) % R) / (double)R;
+        const double c = std::cos(ang), sn = std::sin(ang);
+        val = (u == 0) ? (v == 0 ? c : -sn) : (v == 0 ? sn : c);
+      }
+      const __half h = __float2half_rn((float)val);
+      std::memcpy(dst + Lay<KB>::off(n, k >> 3) + (k & 7) * 2, &h, 2);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP16 operands in the (31, R2, R3) frequency layout.  Unit (seq, j, u) with
+// u = d3 R2 + d2 holds inputs d1 = 4j .. 4j+3 of stage-1 row u: 4 half2 for Z
+// (16 bytes), 4 x (c, c rotated by i) for the code spectra (32 bytes).
+// ---------------------------------------------------------------------------
+template <int M, bool CODE>
+__global__ void __launch_bounds__(256) tc_pack_kernel(const float2* __restrict__ src, uint4* __restrict__ dst,
+                                                      long long n_units, float scale) {
+  using T = T3<M>;
+  constexpr int PER_SEQ = 8 * T::ROWS1;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n_units;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long seq = e / PER_SEQ;
+    const int rem = (int)(e - seq * PER_SEQ);
+    const int j = rem / T::ROWS1, u = rem - j * T::ROWS1;
+    const int d3 = u / T::R2, d2 = u - d3 * T::R2;
+    const int kpart = T::freq_part(d2, T::R2, T::E2) + T::freq_part(d3, T::R3, T::E3);
+    const float2* s = src + seq * T::LC;
+    uint32_t h[4], hr[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int d1 = 4 * j + i;
+      float2 v = make_float2(0.f, 0.f);
+      if (d1 < 31) {
+        // the 31-digit is the same in both layouts: (31, 33, M) digit a = d1
+        const int k = (T::freq_part(d1, 31, T::E1) + kpart) % T::LC;
+        const int kb = (T::UB * k) % 33, kc = M == 1 ? 0 : (T::UC * k) % M;
+        v = __ldg(s + d1 * T::OCOLS + kc * 33 + kb);
+        v.x *= scale;
+        v.y *= scale;
+      }
+      h[i] = pack_h2(v.x, v.y);
+      hr[i] = pack_h2(-v.y, v.x);
+    }
+    if (CODE) {
+      dst[2 * e] = make_uint4(h[0], hr[0], h[1], hr[1]);
+      dst[2 * e + 1] = make_uint4(h[2], hr[2], h[3], hr[3]);
+    } else {
+      dst[e] = make_uint4(h[0], h[1], h[2], h[3]);
+    }
+  }
+}
+
+struct Tc3Params {
+  const uint4* bmat;  // the three DFT matrices in their shared-memory layouts
+  const uint4* z16;   // [n_ab*2][S] sequences of 8*ROWS1 units
+  const uint4* d16;   // [n_prn][2] spectra of 8*ROWS1 double units
+  unsigned long long* keys;
   int* err;
+  int n_items;  // n_ab * 2 * groups
+  int groups;   // ceil(S / BC)
+  int n_prn, S;
 };
 
-template <int M, int BC>
-__global__ void __launch_bounds__(kTcThreads, 2) pfa_tc_kernel(TcParams tp) {
-  using G = Geo<M>;
-  using T = TcGeo<M, BC>;
-  constexpr int COLS = G::COLS, LC = G::LC, NC = G::NC, NT = kTcThreads;
-  const PfaParams& p = tp.p;
+// Code of an output of the inverse transform -> its lag.  The code packs
+// (residue slot s, t1, t2, t3) as ((s * 31 + t1) * R2 + t2) * R3 + t3; the lag
+// is rho + S * natural(t1, t2, t3) with rho = rho0 + s.  Out of line: it runs
+// once per PRN and thread, and on exact ties.
+template <int M>
+__device__ __noinline__ int tc_lag_of(int code, int rho0, int S) {
+  using T = T3<M>;
+  const int t3 = code % T::R3;
+  int q = code / T::R3;
+  const int t2 = q % T::R2;
+  q /= T::R2;
+  const int t1 = q % 31, s = q / 31;
+  return rho0 + s + S * T::natural(t1, t2, t3);
+}
+
+template <int M>
+__global__ void __launch_bounds__(kTcThreads, 2) pfa_tc3_kernel(Tc3Params p) {
+  using T = T3<M>;
+  constexpr int NT = kTcThreads, NW = NT / 32, R2 = T::R2, R3 = T::R3, BC = T::BC, U = T::U;
+  static_assert(NW % 4 == 0, "a warp task keeps its TMEM lane quadrant");
+  // TMEM columns read by one warp task in the transposition phases
+  constexpr int CS1 = T::N1 / 32, CS2 = T::N2 >= 32 ? T::N2 / 32 : 1;
+  constexpr int W2 = T::N2 >= 32 ? 32 : T::N2;
+  constexpr int kBatch = (U + 1) / 2;
   extern __shared__ unsigned char smem_raw[];
   __shared__ uint64_t s_bar;
   __shared__ uint32_t s_tmem;
-  __shared__ unsigned long long s_key;
-  // 1024-aligned regions: R (operand tiles / FP32 transform buffer), B (DFT-31)
+  __shared__ unsigned long long s_key[2];
   const uint32_t raw = smem_addr(smem_raw);
-  unsigned char* R = smem_raw + ((1024 - (raw & 1023)) & 1023);
-  unsigned char* Bm = R + T::R_BYTES;
-  float2* buf = reinterpret_cast<float2*>(R);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  unsigned char* A = smem_raw + ((1024 - (raw & 1023)) & 1023);
+  unsigned char* B1 = A + T::A_BYTES;
+  unsigned char* B2 = B1 + T::B1_BYTES;
+  unsigned char* B3 = B2 + T::B2_BYTES;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quad = warp & 3;
   const int S = p.S;
 
   if (warp == 0) {
     tmem_alloc(&s_tmem, kTcTmemCols);
     tmem_relinquish();
   }
-  if (tid == 0) mbar_init(&s_bar, 1);
-  // B[n][k]: inverse DFT-31 as a real 64x64 matrix, n = 2 ta + (0 re | 1 im),
-  // k = 2 ka + (0 re | 1 im); rows and columns 62, 63 are zero.
-  for (int e = tid; e < 64 * 8; e += NT) {
-    const int n = e >> 3, j = e & 7;
-    uint32_t w[4];
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      float v[2];
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int k = 8 * j + 2 * h + q;
-        float val = 0.f;
-        if (n < 62 && k < 62) {
-          const int ta = n >> 1, u = n & 1, ka = k >> 1, vv = k & 1;
-          const int m = (ta * ka) % 31;
-          const float c = kCos31[m], sn = kSin31[m];
-          val = (u == 0) ? (vv == 0 ? c : -sn) : (vv == 0 ? sn : c);
-        }
-        v[q] = val;
-      }
-      w[h] = pack_h2(v[0], v[1]);
-    }
-    *reinterpret_cast<uint4*>(Bm + sw128_off(n, j)) = make_uint4(w[0], w[1], w[2], w[3]);
+  if (tid == 0) {
+    mbar_init(&s_bar, 1);
+    s_key[0] = s_key[1] = 0ull;
   }
+  // operand rows and K entries that no stage writes (padding) must hold
+  // finite values: they meet zeros of the DFT matrices
+  for (int i = tid; i < T::A_BYTES / 16; i += NT) reinterpret_cast<uint4*>(A)[i] = make_uint4(0u, 0u, 0u, 0u);
+  constexpr int B_CHUNKS = (T::B1_BYTES + T::B2_BYTES + T::B3_BYTES) / 16;
+  for (int i = tid; i < B_CHUNKS; i += NT) reinterpret_cast<uint4*>(B1)[i] = __ldg(p.bmat + i);
   fence_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = s_tmem;
-  const uint64_t db = sw128_desc(smem_addr(Bm));
+  const uint32_t a_addr = smem_addr(A);
+  const uint64_t db1 = Lay<T::KB1>::desc(smem_addr(B1));
+  const uint64_t db2 = Lay<T::KB2>::desc(smem_addr(B2));
+  const uint64_t db3 = Lay<T::KB3>::desc(smem_addr(B3));
+  const uint32_t lane_off = (uint32_t)(quad * 32) << 16;
+
+  // product units of this thread: unit e = tid + k NT is (row r, chunk j);
+  // packed (code-spectrum unit index << 16) | shared-memory byte offset
+  uint32_t uoff[U];
+#pragma unroll
+  for (int k = 0; k < U; ++k) {
+    const int e = tid + k * NT;
+    const int j = e / T::NR1, r = e - j * T::NR1;
+    const int u = r - (r / T::ROWS1) * T::ROWS1;
+    uoff[k] = e < T::UNITS ? ((uint32_t)(j * T::ROWS1 + u) << 16) | (uint32_t)(r * 16 + j * T::LBO1) : 0u;
+  }
+
   uint32_t phase = 0;
   bool failed = false;
+  unsigned it = 0;      // PRN iterations of this CTA (key slot parity)
+  long long pend = -1;  // thread 0: key index awaiting its flush
 
-  const int groups = (S + BC - 1) / BC;
+  // bounded wait for the last commit; false when the tensor cores did not
+  // answer.  One warp polls the mbarrier; the others wait at the CTA barrier
+  // and issue nothing, which leaves the SM to the co-resident CTA.
+  auto wait_mma = [&]() -> bool {
+    uint32_t done = 1;
+    if (warp == 0) {
+      done = 0;
+      for (long long k = 0; k < kWaitPolls && !done; ++k) done = mbar_try_wait(&s_bar, phase);
+    }
+    if (__syncthreads_or(!done)) return false;
+    phase ^= 1u;
+    tc_fence_after();
+    return true;
+  };
+  auto issue_sync = [&]() {
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+  };
+
   for (int w = blockIdx.x; w < p.n_items && !failed; w += gridDim.x) {
-    const int ab_h = w / p.n_prn, prn = w - ab_h * p.n_prn, hyp = ab_h & 1;
-    float pmax = -1.f;
-    int cmax = 0;
-    auto lag_of = [&](int code) -> int {
-      const int c = code & 15, q = code >> 4;
-      const int b = q % 33, q2 = q / 33;
-      const int a = q2 % 31, rho = q2 / 31;
-      return rho + S * G::natural(a, b, c);
-    };
-    if (tid == 0) s_key = 0ull;
-
-    for (int g = 0; g < groups; ++g) {
-      auto seq_of = [&](int s) -> int {
+    const int ab_h = w / p.groups, g = w - ab_h * p.groups, hyp = ab_h & 1;
+    // this CTA's Z units, kept in registers for every PRN
+    uint4 zr[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int e = tid + k * NT;
+      zr[k] = make_uint4(0u, 0u, 0u, 0u);
+      if (e < T::UNITS) {
+        const int j = e / T::NR1, r = e - j * T::NR1;
+        const int s = r / T::ROWS1, u = r - s * T::ROWS1;
         const int rho = g * BC + s;
-        return rho < S ? rho : -1;
-      };
-      auto epilogue = [&](int s, int a, int b, int c, float2 v) {
-        const float pw = fmaf(v.x, v.x, v.y * v.y);
-        const int code = ((seq_of(s) * 31 + a) * 33 + b) * 16 + c;
-        if (pw == pmax) {
-          if (lag_of(code) > lag_of(cmax)) cmax = code;
-        }
-        cmax = pw > pmax ? code : cmax;
-        pmax = fmaxf(pw, pmax);
-      };
-
-      // ---- stage 1a: products -> FP16 operand rows (one row per column) ----
-      for (int u = tid; u < T::NCOL; u += NT) {
-        const int s = u / COLS, col = u - s * COLS;
-        const int q = seq_of(s);
-        if (q < 0) continue;
-        const float2* zs = p.z + ((size_t)ab_h * S + q) * LC + col;
-        const float2* ds = p.D + ((size_t)prn * 2 + hyp) * LC + col;
-        uint32_t pk[32];
-#pragma unroll
-        for (int a = 0; a < 31; ++a) {
-          const float2 x = cmul(__ldcg(zs + a * COLS), __ldg(ds + a * COLS));
-          pk[a] = pack_h2(x.x * tp.in_scale, x.y * tp.in_scale);
-        }
-        pk[31] = 0u;
-        unsigned char* rowp = R + (u >> 7) * 16384;
-        const int r = u & 127;
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-          *reinterpret_cast<uint4*>(rowp + sw128_off(r, j)) = make_uint4(pk[4 * j], pk[4 * j + 1], pk[4 * j + 2], pk[4 * j + 3]);
+        if (rho < S) zr[k] = __ldcs(p.z16 + (((size_t)ab_h * S + rho) * 8 + j) * T::ROWS1 + u);
       }
-      fence_async_smem();
-      tc_fence_before();
-      __syncthreads();
+    }
+    // |y|^2 of the 11 outputs of stage-3 row task (warp-collective TMEM
+    // read); returns the code of t3 = 0, or -1 when the row is padding
+    auto p4_row = [&](int task, float(&pw)[11]) -> int {
+      const int t = task >> 2;
+      const int r = t * 128 + quad * 32 + lane;
+      const int s = r / T::ROWS3, q = r - s * T::ROWS3;
+      const int t1 = q / R2, t2 = q - t1 * R2;
+      const uint32_t taddr = tmem_base + lane_off + (uint32_t)(t * T::N3);
+      uint32_t v[16], v2[8];
+      tmem_ld16(taddr, v);
+      tmem_ld8(taddr + 16, v2);
+      tmem_wait_ld();
+#pragma unroll
+      for (int h = 0; h < 8; ++h)
+        pw[h] = fmaf(__uint_as_float(v[2 * h]), __uint_as_float(v[2 * h]),
+                     __uint_as_float(v[2 * h + 1]) * __uint_as_float(v[2 * h + 1]));
+#pragma unroll
+      for (int h = 0; h < 3; ++h)
+        pw[8 + h] = fmaf(__uint_as_float(v2[2 * h]), __uint_as_float(v2[2 * h]),
+                         __uint_as_float(v2[2 * h + 1]) * __uint_as_float(v2[2 * h + 1]));
+      const bool valid = r < T::NR3 && g * BC + s < S;
+      return valid ? ((s * 31 + t1) * R2 + t2) * R3 : -1;
+    };
 
-      // ---- stage 1b: DFT-31 on the tensor cores ----
-      if (tid == 0) {
-        tc_fence_after();
+    for (int prn = 0; prn < p.n_prn; ++prn, ++it) {
+      // ---- P1: FP16 products -> stage-1 operand rows ----
+      const uint4* dsrc = p.d16 + (size_t)2 * (((size_t)prn * 2 + hyp) * 8) * T::ROWS1;
+      // two batches of units: all code-spectrum loads of a batch are in
+      // flight before its products are formed
 #pragma unroll
-        for (int t = 0; t < T::TILES; ++t) {
-          const uint64_t da = sw128_desc(smem_addr(R + t * 16384));
+      for (int k0 = 0; k0 < U; k0 += kBatch) {
+        uint4 c[2 * kBatch];
 #pragma unroll
-          for (int ks = 0; ks < 4; ++ks)
-            mma_f16(tmem_base + (uint32_t)(t * 64), da + (uint64_t)(2 * ks), db + (uint64_t)(2 * ks), kIdescF16,
-                    ks > 0 ? 1u : 0u);
+        for (int i = 0; i < kBatch; ++i) {
+          const int k = k0 + i;
+          if (k < U && (k < U - 1 || tid + k * NT < T::UNITS)) {
+            const uint4* src = dsrc + 2 * (uoff[k] >> 16);
+            c[2 * i] = __ldcg(src);
+            c[2 * i + 1] = __ldcg(src + 1);
+          }
         }
-        mma_commit(&s_bar);
-      }
-      uint32_t done = 0;
-      for (long long it = 0; it < kWaitPolls && !done; ++it) done = mbar_try_wait(&s_bar, phase);
-      if (__syncthreads_or(!done)) {
-        failed = true;
-        break;
-      }
-      phase ^= 1u;
-      tc_fence_after();
-
-      // ---- stage 1c: TMEM -> FP32 transform buffer (aliases the operand tiles) ----
-      {
-        const int t = warp >> 2, quad = warp & 3;
-        if (t < T::TILES) {
-          const int u = t * 128 + quad * 32 + lane;  // this thread's TMEM lane = column
-          const int s = u / COLS, col = u - s * COLS;
-          const bool valid = u < T::NCOL && seq_of(s) >= 0;
-          const uint32_t taddr = tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(t * 64);
 #pragma unroll
-          for (int chunk = 0; chunk < 4; ++chunk) {
-            uint32_t r[16];
-            tmem_ld16(taddr + (uint32_t)(16 * chunk), r);
-            tmem_wait_ld();
-            if (valid) {
-              float2* dst = buf + s * LC + col;
-#pragma unroll
-              for (int h = 0; h < 8; ++h) {
-                const int ta = chunk * 8 + h;
-                if (ta < 31) dst[ta * COLS] = make_float2(__uint_as_float(r[2 * h]), __uint_as_float(r[2 * h + 1]));
-              }
-            }
+        for (int i = 0; i < kBatch; ++i) {
+          const int k = k0 + i;
+          if (k < U && (k < U - 1 || tid + k * NT < T::UNITS)) {
+            const uint4 c0 = c[2 * i], c1 = c[2 * i + 1], z = zr[k];
+            *reinterpret_cast<uint4*>(A + (uoff[k] & 0xFFFFu)) =
+                make_uint4(cmul_h2(z.x, c0.x, c0.y), cmul_h2(z.y, c0.z, c0.w), cmul_h2(z.z, c1.x, c1.y),
+                           cmul_h2(z.w, c1.z, c1.w));
           }
         }
       }
-      tc_fence_before();
-      __syncthreads();
+      issue_sync();
+      if (tid == 0) {
+        if (pend >= 0) {
+          // every warp of the previous PRN has folded its key into the other slot
+          atomicMax(p.keys + pend, s_key[(it + 1) & 1]);
+          s_key[(it + 1) & 1] = 0ull;
+        }
+        tc_fence_after();
+#pragma unroll 1
+        for (int t = 0; t < T::TILES1; ++t)
+#pragma unroll 1
+          for (int ks = 0; ks < T::K1 / 16; ++ks)
+            mma_f16(tmem_base + (uint32_t)(t * T::N1),
+                    desc_kchunks(a_addr + t * 2048, T::LBO1) + (uint64_t)(2 * ks * (T::LBO1 >> 4)), db1 + 2 * ks,
+                    idesc_f16(T::N1), ks > 0 ? 1u : 0u);
+        mma_commit(&s_bar);
+        pend = (long long)ab_h * p.n_prn + prn;
+      }
+      if (!wait_mma()) {
+        failed = true;
+        break;
+      }
 
-      // ---- stage 2: DFT-33 over digit b (FP32) ----
-      for (int u = tid; u < BC * 31 * NC; u += NT) {
-        const int s = u / (31 * NC), r = u - s * 31 * NC;
-        const int a = r / NC, c = r - a * NC;
-        if (seq_of(s) < 0) continue;
-        float2* base = buf + s * LC + a * COLS + c * 33;
-        float2 x[33];
+      // ---- P2: stage-1 accumulators -> stage-2 rows (t1, d3), K = d2 ----
+      for (int task = warp; task < T::TILES1 * 4 * CS1; task += NW) {
+        const int t = task / (4 * CS1), half = (task >> 2) % CS1;
+        const int r = t * 128 + quad * 32 + lane;
+        const bool valid = r < T::NR1;
+        const int s = r / T::ROWS1, u = r - s * T::ROWS1;
+        const int d3 = u / R2, d2 = u - d3 * R2;
+        // stage-2 row (t1, d3) = s ROWS2 + t1 R3 + d3, K entry d2
+        unsigned char* dst = A + (s * T::ROWS2 + d3) * 16 + (d2 >> 2) * T::LBO2 + (d2 & 3) * 4;
+        uint32_t v[32];
+        tmem_ld_cols<2>(tmem_base + lane_off + (uint32_t)(t * T::N1 + 32 * half), v);
 #pragma unroll
-        for (int b = 0; b < 33; ++b) x[b] = base[b];
-        if constexpr (NC == 1) {
-          dft33<true>(x, [&](int tb, float2 v) { epilogue(s, a, tb, 0, v); });
-        } else {
-          dft33<true>(x, [&](int tb, float2 v) { base[tb] = v; });
+        for (int h = 0; h < 16; ++h) {
+          const int t1 = 16 * half + h;
+          if (valid && t1 < 31)
+            st_shared_u32(dst + t1 * R3 * 16, pack_h2_sat(__uint_as_float(v[2 * h]), __uint_as_float(v[2 * h + 1])));
         }
       }
-      // ---- stage 3: DFT-M over digit c (FP32) ----
-      if constexpr (NC > 1) {
-        __syncthreads();
-        for (int u = tid; u < BC * 1023; u += NT) {
-          const int s = u / 1023, gi = u - s * 1023;
-          const int a = gi / 33, b = gi - a * 33;
-          if (seq_of(s) < 0) continue;
-          const float2* base = buf + s * LC + a * COLS + b;
-          float2 x[NC];
+      issue_sync();
+      if (tid == 0) {
+        tc_fence_after();
+#pragma unroll 1
+        for (int t = 0; t < T::TILES2; ++t)
+#pragma unroll 1
+          for (int ks = 0; ks < T::K2 / 16; ++ks)
+            mma_f16(tmem_base + (uint32_t)(t * T::N2),
+                    desc_kchunks(a_addr + t * 2048, T::LBO2) + (uint64_t)(2 * ks * (T::LBO2 >> 4)), db2 + 2 * ks,
+                    idesc_f16(T::N2), ks > 0 ? 1u : 0u);
+        mma_commit(&s_bar);
+      }
+      if (!wait_mma()) {
+        failed = true;
+        break;
+      }
+
+      // ---- P3: stage-2 accumulators -> stage-3 rows (t1, t2), K = d3 ----
+      for (int task = warp; task < T::TILES2 * 4 * CS2; task += NW) {
+        const int t = task / (4 * CS2), half = (task >> 2) % CS2;
+        const int r = t * 128 + quad * 32 + lane;
+        const bool valid = r < T::NR2;
+        const int s = r / T::ROWS2, q = r - s * T::ROWS2;
+        const int t1 = q / R3, d3 = q - t1 * R3;
+        // stage-3 row (t1, t2) = s ROWS3 + t1 R2 + t2, K entry d3
+        unsigned char* dst = A + (s * T::ROWS3 + t1 * R2) * 16 + (d3 >> 2) * T::LBO3 + (d3 & 3) * 4;
+        uint32_t v[W2];
+        tmem_ld_cols<W2 / 16>(tmem_base + lane_off + (uint32_t)(t * T::N2 + W2 * half), v);
 #pragma unroll
-          for (int c = 0; c < NC; ++c) x[c] = base[c * 33];
-          dft_small<NC, true>(x, [&](int tc, float2 v) { epilogue(s, a, b, tc, v); });
+        for (int h = 0; h < W2 / 2; ++h) {
+          const int t2 = (W2 / 2) * half + h;
+          if (valid && t2 < R2)
+            st_shared_u32(dst + t2 * 16, pack_h2_sat(__uint_as_float(v[2 * h]), __uint_as_float(v[2 * h + 1])));
         }
       }
-      __syncthreads();
-    }
-    if (failed) break;
+      issue_sync();
+      if (tid == 0) {
+        tc_fence_after();
+#pragma unroll 1
+        for (int t = 0; t < T::TILES3; ++t)
+#pragma unroll 1
+          for (int ks = 0; ks < T::K3 / 16; ++ks)
+            mma_f16(tmem_base + (uint32_t)(t * T::N3),
+                    desc_kchunks(a_addr + t * 2048, T::LBO3) + (uint64_t)(2 * ks * (T::LBO3 >> 4)), db3 + 2 * ks,
+                    idesc_f16(T::N3), ks > 0 ? 1u : 0u);
+        mma_commit(&s_bar);
+      }
+      if (!wait_mma()) {
+        failed = true;
+        break;
+      }
 
-    unsigned long long kbest =
-        pmax < 0.f ? 0ull : (((unsigned long long)__float_as_uint(pmax) << 32) | (unsigned)lag_of(cmax));
+      // ---- P4: |y|^2 maximum over stage-3 rows (t1, t2), t3 ----
+      // Branch-free per row: the row maximum, the mask of its positions and
+      // the last of them.  The reference keeps the later lag on exact ties
+      // (Iterator::max_by); a thread whose maximum is reached more than once
+      // resolves it exactly in a second pass, which almost never runs.
+      float best = -1.f;
+      int bcode = 0;
+      bool tie = false;
+      for (int task = warp; task < T::TILES3 * 4; task += NW) {
+        float pw[11];
+        const int code0 = p4_row(task, pw);
+        if (code0 >= 0) {
+          float m = pw[0];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long other = __shfl_xor_sync(0xffffffffu, kbest, o);
-      kbest = other > kbest ? other : kbest;
+          for (int h = 1; h < 11; ++h) m = fmaxf(m, pw[h]);
+          unsigned mask = 0u;
+#pragma unroll
+          for (int h = 0; h < 11; ++h) mask |= (pw[h] == m ? 1u : 0u) << h;
+          if (m > best) {
+            best = m;
+            bcode = code0 + (31 - __clz(mask));
+            tie = __popc(mask) > 1;
+          } else if (m == best) {
+            tie = true;
+          }
+        }
+      }
+      int blag = best < 0.f ? 0 : tc_lag_of<M>(bcode, g * BC, S);
+      if (__any_sync(0xffffffffu, tie)) {
+        for (int task = warp; task < T::TILES3 * 4; task += NW) {
+          float pw[11];
+          const int code0 = p4_row(task, pw);
+          if (tie && code0 >= 0) {
+#pragma unroll
+            for (int h = 0; h < 11; ++h)
+              if (pw[h] == best) blag = max(blag, tc_lag_of<M>(code0 + h, g * BC, S));
+          }
+        }
+      }
+      unsigned long long kbest =
+          best < 0.f ? 0ull : (((unsigned long long)__float_as_uint(best) << 32) | (unsigned)blag);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, kbest, o);
+        kbest = other > kbest ? other : kbest;
+      }
+      if (lane == 0) atomicMax(&s_key[it & 1], kbest);
     }
-    if (lane == 0) atomicMax(&s_key, kbest);
-    __syncthreads();
-    if (tid == 0) p.keys[w] = s_key;
-    __syncthreads();
   }
 
   if (failed) {
     // the tensor cores did not answer in time: flag it, give the in-flight
     // MMAs a second bounded window to finish, then release TMEM
-    if (tid == 0) atomicExch(tp.err, 1);
+    if (tid == 0) atomicExch(p.err, 1);
     uint32_t done = 0;
-    for (long long it = 0; it < kWaitPolls && !done; ++it) done = mbar_try_wait(&s_bar, phase);
+    for (long long k = 0; k < kWaitPolls && !done; ++k) done = mbar_try_wait(&s_bar, phase);
     __syncthreads();
+  } else {
+    __syncthreads();
+    if (tid == 0 && pend >= 0) atomicMax(p.keys + pend, s_key[(it + 1) & 1]);
   }
   tc_fence_before();
   __syncthreads();
@@ -355,46 +637,113 @@ __global__ void __launch_bounds__(kTcThreads, 2) pfa_tc_kernel(TcParams tp) {
   if (warp == 0) tmem_dealloc(tmem_base, kTcTmemCols);
 }
 
-template <int M, int BC>
-cudaError_t run_tc(const TcParams& tp, int num_sms, cudaStream_t st) {
-  using T = TcGeo<M, BC>;
-  auto kern = pfa_tc_kernel<M, BC>;
+template <int M>
+cudaError_t run_tc3(const PolyClass& pc, const SearchDims& dims, const void* d_bmat, const void* d_z16,
+                    const void* d_d16, unsigned long long* d_keys, int* d_err, int num_sms, cudaStream_t st) {
+  using T = T3<M>;
+  Tc3Params p = {};
+  p.bmat = static_cast<const uint4*>(d_bmat);
+  p.z16 = static_cast<const uint4*>(d_z16);
+  p.d16 = static_cast<const uint4*>(d_d16);
+  p.keys = d_keys;
+  p.err = d_err;
+  p.n_prn = dims.n_prn;
+  p.S = pc.S;
+  p.groups = (pc.S + T::BC - 1) / T::BC;
+  p.n_items = dims.n_ant * dims.nb * 2 * p.groups;
+  auto kern = pfa_tc3_kernel<M>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, T::SMEM);
   if (e != cudaSuccess) return e;
-  int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTcThreads, T::SMEM);
-  if (per_sm < 1) per_sm = 1;
-  if (per_sm > 2) per_sm = 2;  // TMEM: 2 x 256 columns per SM
-  int grid = num_sms * per_sm;
-  if (grid > tp.p.n_items) grid = tp.p.n_items;
+  // two CTAs per SM: T::SMEM >= 80 KB keeps a third one out, so the two
+  // 256-column TMEM allocations always fit
+  int grid = num_sms * 2;
+  if (grid > p.n_items) grid = p.n_items;
   if (grid < 1) return cudaSuccess;
-  kern<<<grid, kTcThreads, T::SMEM, st>>>(tp);
+  kern<<<grid, kTcThreads, T::SMEM, st>>>(p);
   kernel_launch_add(1);
   return cudaGetLastError();
 }
 
-}  // namespace
-
-cudaError_t launch_correlate_tc(const PolyClass& pc, const SearchDims& dims, const float2* d_Z, const float2* d_D,
-                                unsigned long long* d_keys, int* d_err, int num_sms, cudaStream_t st) {
-  TcParams tp = {};
-  tp.p.z = const_cast<float2*>(d_Z);
-  tp.p.D = d_D;
-  tp.p.keys = d_keys;
-  tp.p.n_prn = dims.n_prn;
-  tp.p.S = pc.S;
-  tp.p.P = pc.P;
-  tp.p.n_items = dims.n_ant * dims.nb * 2 * dims.n_prn;
-  tp.err = d_err;
-  // 2^-k with 4 S Lc^2 2^-k <= 32768
+// FP16 scale exponents (kz, kd) of Z and the code spectra, kz + kd = k with
+// 4 S Lc^2 2^-k <= 32768
+void tc_scales(const PolyClass& pc, int* kz, int* kd) {
   const double bound = 4.0 * pc.S * (double)pc.Lc * (double)pc.Lc;
   int k = 0;
   while (bound / (double)(1ull << k) > 32768.0 && k < 60) ++k;
-  tp.in_scale = (float)(1.0 / (double)(1ull << k));
+  *kz = (k + 1) / 2;
+  *kd = k - *kz;
+}
+
+template <int M, bool CODE>
+cudaError_t run_pack(const float2* src, long long n_seq, void* dst, float scale, int num_sms, cudaStream_t st) {
+  const long long n_units = n_seq * 8 * T3<M>::ROWS1;
+  if (n_units == 0) return cudaSuccess;
+  long long blocks = (n_units + 255) / 256;
+  if (blocks > (long long)num_sms * 16) blocks = (long long)num_sms * 16;
+  tc_pack_kernel<M, CODE><<<(int)blocks, 256, 0, st>>>(src, static_cast<uint4*>(dst), n_units, scale);
+  kernel_launch_add(1);
+  return cudaGetLastError();
+}
+
+template <int M>
+std::vector<unsigned char> build_matrices() {
+  using T = T3<M>;
+  std::vector<unsigned char> b((size_t)(T::B1_BYTES + T::B2_BYTES + T::B3_BYTES), 0);
+  host_idft_matrix<31, T::N1, T::KB1>(b.data());
+  host_idft_matrix<T::R2, T::N2, T::KB2>(b.data() + T::B1_BYTES);
+  host_idft_matrix<T::R3, T::N3, T::KB3>(b.data() + T::B1_BYTES + T::B2_BYTES);
+  return b;
+}
+
+}  // namespace
+
+size_t tc_operand_bytes(const PolyClass& pc, long long n_seq, bool code) {
+  const int rows1 = pc.Lc / 31;  // R2 * R3
+  return (size_t)n_seq * 8 * rows1 * (code ? 32 : 16);
+}
+
+double tc_gemm_flops_per_point(int M) {
+  // real-embedded DFT-R as a dense 2R x 2R GEMM: 8 R FLOPs per complex point and stage
+  switch (M) {
+    case 1: return 8.0 * (31 + Tc3Cfg<1>::R2 + Tc3Cfg<1>::R3);
+    case 4: return 8.0 * (31 + Tc3Cfg<4>::R2 + Tc3Cfg<4>::R3);
+    case 10: return 8.0 * (31 + Tc3Cfg<10>::R2 + Tc3Cfg<10>::R3);
+  }
+  return 0.0;
+}
+
+std::vector<unsigned char> tc_dft_matrices(int M) {
+  switch (M) {
+    case 1: return build_matrices<1>();
+    case 4: return build_matrices<4>();
+    case 10: return build_matrices<10>();
+  }
+  return {};
+}
+
+cudaError_t launch_tc_pack(const PolyClass& pc, const float2* d_src, long long n_seq, bool code, void* d_dst,
+                           int num_sms, cudaStream_t st) {
+  int kz = 0, kd = 0;
+  tc_scales(pc, &kz, &kd);
+  const float scale = (float)(1.0 / (double)(1ull << (code ? kd : kz)));
   switch (pc.M) {
-    case 1: return run_tc<1, 8>(tp, num_sms, st);
-    case 4: return run_tc<4, 2>(tp, num_sms, st);
-    case 10: return run_tc<10, 1>(tp, num_sms, st);
+    case 1: return code ? run_pack<1, true>(d_src, n_seq, d_dst, scale, num_sms, st)
+                        : run_pack<1, false>(d_src, n_seq, d_dst, scale, num_sms, st);
+    case 4: return code ? run_pack<4, true>(d_src, n_seq, d_dst, scale, num_sms, st)
+                        : run_pack<4, false>(d_src, n_seq, d_dst, scale, num_sms, st);
+    case 10: return code ? run_pack<10, true>(d_src, n_seq, d_dst, scale, num_sms, st)
+                         : run_pack<10, false>(d_src, n_seq, d_dst, scale, num_sms, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_correlate_tc(const PolyClass& pc, const SearchDims& dims, const void* d_bmat, const void* d_z16,
+                                const void* d_d16, unsigned long long* d_keys, int* d_err, int num_sms,
+                                cudaStream_t st) {
+  switch (pc.M) {
+    case 1: return run_tc3<1>(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, num_sms, st);
+    case 4: return run_tc3<4>(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, num_sms, st);
+    case 10: return run_tc3<10>(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, num_sms, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace tga {
 
@@ -69,11 +70,21 @@ cudaError_t launch_correlate(const PolyClass& pc, const SearchDims& dims, const 
 // FP32 re-evaluation of each (antenna, PRN)'s selected row: rewrites best.p / best.tau.
 cudaError_t launch_refine(const PolyClass& pc, const SearchDims& dims, const float2* d_Z, const float2* d_D,
                           BestRow* d_best, int num_sms, cudaStream_t st);
-// Tensor-core correlator (FP16 operands, FP32 accumulation in TMEM) for the
-// DFT-31 stage; keys hold |y|^2 scaled by 2^-2k (comparisons only).  *d_err
-// is set non-zero when a bounded wait on the tensor cores expired.
-cudaError_t launch_correlate_tc(const PolyClass& pc, const SearchDims& dims, const float2* d_Z, const float2* d_D,
-                                unsigned long long* d_keys, int* d_err, int num_sms, cudaStream_t st);
+// Tensor-core search: FP16 operands in the (31, R2, R3) frequency layout
+// (launch_tc_pack of Z and of the code spectra), then the three-stage tcgen05
+// correlator (FP32 accumulation in TMEM).  Keys hold |y|^2 scaled by 2^-2k
+// (comparisons only) and must be zeroed before the launch; *d_err is set
+// non-zero when a bounded wait on the tensor cores expired.
+size_t tc_operand_bytes(const PolyClass& pc, long long n_seq, bool code);
+double tc_gemm_flops_per_point(int M);
+// the three inverse-DFT matrices of class M in the correlator's shared-memory
+// layouts (FP16), to be uploaded once and passed as d_bmat
+std::vector<unsigned char> tc_dft_matrices(int M);
+cudaError_t launch_tc_pack(const PolyClass& pc, const float2* d_src, long long n_seq, bool code, void* d_dst,
+                           int num_sms, cudaStream_t st);
+cudaError_t launch_correlate_tc(const PolyClass& pc, const SearchDims& dims, const void* d_bmat, const void* d_z16,
+                                const void* d_d16, unsigned long long* d_keys, int* d_err, int num_sms,
+                                cudaStream_t st);
 cudaError_t launch_reduce_bins(const SearchDims& dims, const unsigned long long* d_keys,
                                BestRow* d_best, cudaStream_t st);
 cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,

@@ -377,11 +377,30 @@ void run_group(tga_ctx* ctx, const ClassGroup& grp, const SampleSource& src, con
         [&] { return launch_forward_z(pc, n_ab, d_z, ctx->num_sms, st); });
   if (ctx->precision == TGA_PRECISION_FP16_TC) {
     int* d_err = (int*)ctx->buf("tc.err", sizeof(int));
+    const long long n_zseq = (long long)n_ab * 2 * pc.S;
+    void* d_z16 = ctx->buf(tag + ".z16", tc_operand_bytes(pc, n_zseq, false));
+    void* d_d16 = ctx->buf(tag + ".d16", tc_operand_bytes(pc, (long long)n_prn * 2, true));
+    // DFT matrices of the class (they depend on Lc only), uploaded once per context
+    const std::string mat_name = "tcmat." + std::to_string(pc.M);
+    void* d_bmat = nullptr;
+    if (!ctx->uploaded.count(mat_name)) {
+      const std::vector<unsigned char> mats = tc_dft_matrices(pc.M);
+      d_bmat = ctx->buf(mat_name, mats.size());
+      CK(cudaMemcpy(d_bmat, mats.data(), mats.size(), cudaMemcpyHostToDevice));
+      ctx->uploaded[mat_name] = {};
+    } else {
+      d_bmat = ctx->buf(mat_name, 0);
+    }
+    timed(ctx, ("tc_pack" + cls).c_str(), 0.0, [&] {
+      cudaError_t e = launch_tc_pack(pc, d_z, n_zseq, false, d_z16, ctx->num_sms, st);
+      if (e == cudaSuccess) e = launch_tc_pack(pc, d_D, (long long)n_prn * 2, true, d_d16, ctx->num_sms, st);
+      return e;
+    });
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
-    // tensor-core FLOPs per point: 2 x 64 x 64 / 31 (DFT-31 GEMM) + FP32 rest
-    const double tc_flops = 2.0 * 64 * 64 / 31.0;
-    timed(ctx, ("correlate_tc" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * (tc_flops + tf - 1950.0 / 31.0 + 9.0),
-          [&] { return launch_correlate_tc(pc, dims, d_z, d_D, d_keys, d_err, ctx->num_sms, st); });
+    CK(cudaMemsetAsync(d_keys, 0, (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long), st));
+    // tensor-core FLOPs of the three DFT stages as dense real GEMMs
+    timed(ctx, ("correlate_tc" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * tc_gemm_flops_per_point(pc.M),
+          [&] { return launch_correlate_tc(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, ctx->num_sms, st); });
     ctx->tc_err_pending = d_err;
   } else {
     timed(ctx, ("correlate" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * (tf + 9.0),
