@@ -13,8 +13,13 @@ uniform, Doppler uniform +-4 kHz, random +-1 sign per code epoch, C/N0 uniform
 (0x5EED2026 + 1 + rank).
 
 Output: one JSON line (rank 0).  `value` is device time with the packed bits
-already in HBM; `e2e` goes through the C ABI (tga_acquire_all) from pinned
-host memory with the H2D copy and the result D2H inside the timed region.
+already in HBM, for the tensor-core search (FP16 tcgen05 transform, FP32
+accumulation, selected rows re-evaluated in FP32) unless --precision fp32;
+`compare` holds the same measurement for the other arithmetic (the FP32
+fused search by default) and whether both detect the same cells with the same
+code phase, Doppler bin and hypothesis.  `e2e` goes through the C ABI
+(tga_acquire_all) from pinned host memory with the H2D copy and the result
+D2H inside the timed region.
 `--impl reference` times the CPU restatement of the reference algorithm (the
 reference itself is Rust and cannot be built here) on a bounded sample.
 """
@@ -159,6 +164,22 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def load_peaks():
+    """Measured peaks of this GPU pool (driver-written), or None."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(path))
+    except Exception:
+        return None
+
+
+def detections(cells):
+    """Detected cells (strength / second >= 2, i.e. r_A >= 4) and their
+    (code phase, Doppler bin, hypothesis)."""
+    det = cells["signal_strength"] >= 2.0 * cells["second_peak"]
+    return det, np.stack([cells["best_codephase"], cells["best_freq_idx"], cells["hypothesis"]], axis=1)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -169,8 +190,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--n-ant", type=int, default=N_ANT, help="antennas per GPU (profiling runs use fewer)")
     ap.add_argument("--variant10", type=int, default=None, help="launch-shape variant of the Lc=10230 kernels")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16tc"],
-                    help="search arithmetic: FP32 CUDA cores, or FP16 tensor-core DFT-31 with FP32 refinement")
+    ap.add_argument("--precision", default="fp16tc", choices=["fp32", "fp16tc"],
+                    help="search arithmetic of the headline: FP16 tensor-core transform with FP32 refinement "
+                         "(default), or FP32 CUDA cores")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the second arithmetic (the FP32 fused search beside the tensor-core one)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -197,12 +221,11 @@ def main():
     ctx = tga.Context(local)
     if args.variant10 is not None:
         tga.lib().tga_set_variant(ctx._h, 10230, args.variant10)
-    if args.precision == "fp16tc":
-        ctx.set_precision(tga.PRECISION_FP16_TC)
     stream = torch.cuda.ExternalStream(tga.lib().tga_stream(ctx._h))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     lib = tga.lib()
     import ctypes
+    prec_id = {"fp32": tga.PRECISION_FP32, "fp16tc": tga.PRECISION_FP16_TC}
 
     def step_device():
         return ctx.acquire_cells(None, FS, mask=tga.ALL, cn0=True, device_bits=d_bits.data_ptr(), n_ant=n_ant,
@@ -220,47 +243,94 @@ def main():
         lib.tga_kernel_times(ctx._h, cap, names, ms, la, fl, ctypes.byref(n))
         return {names[i].decode(): (ms[i], la[i], fl[i]) for i in range(min(n.value, cap))}
 
-    for _ in range(args.warmup):
-        step_device()
-    torch.cuda.synchronize()
+    def measure(precision):
+        """W warm-up and K timed device steps of one arithmetic; every rank
+        takes the same collective steps.  Returns ms/step (max over ranks),
+        cells, per-kernel times, launches and the last step's cells."""
+        ctx.set_precision(prec_id[precision])
+        for _ in range(args.warmup):
+            step_device()
+        torch.cuda.synchronize()
+        lib.tga_set_profiling(ctx._h, 1)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        total_ms, launches, agg, out = 0.0, 0, {}, None
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)  # evict L2 between steps (outside the timed events)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            out = step_device()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            launches += ctx.last_stats()["kernel_launches"]
+            for k, (ms, la, fl) in kernel_times().items():
+                a = agg.setdefault(k, [0.0, 0, 0.0])
+                a[0] += ms
+                a[1] += la
+                a[2] += fl
+        torch.cuda.synchronize()
+        lib.tga_set_profiling(ctx._h, 0)
+        cells = ctx.last_stats()["cells"]
+        ms_step = total_ms / args.steps
+        if world > 1:
+            t = torch.tensor([ms_step], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_step = float(t.item())
+            dist.barrier()
+        return ms_step, cells, agg, launches, out
 
-    lib.tga_set_profiling(ctx._h, 1)
+    def roofline(agg, precision, sm_mhz):
+        """Dominant kernel of a run against its roofline: the tensor-core
+        correlator against the measured sustained dense FP16/BF16 rate (it is
+        timed inside a long step), the FP32 kernels against the FP32 pipe."""
+        dname, (dms, dl, dfl) = max(agg.items(), key=lambda kv: kv[1][0])
+        avg_launch_s = dms / dl / 1e3
+        achieved = dfl / dl / avg_launch_s / 1e12
+        peaks = load_peaks()
+        if precision == "fp16tc" and dname.startswith("correlate_tc"):
+            if peaks and peaks.get("bf16_tflops_sustained"):
+                peak, src = float(peaks["bf16_tflops_sustained"]), "of measured: MEASURED_PEAKS.json bf16_tflops_sustained"
+            else:
+                peak, src = 1400.0, "of fallback: sustained dense bf16 figure of the profiling recipe"
+            bound = "tensor"
+            note = ("algorithmic FLOPs: the three DFT stages as dense real 2R x 2R GEMMs, 8 (31 + R2 + R3) "
+                    "per complex output point")
+        else:
+            peak = fp32_peak_tflops(sm_mhz)
+            src = ("148 SM x 128 FP32 lanes x 2 flop x median SM clock under load (%.0f MHz); "
+                   "MEASURED_PEAKS.json has no FP32 SIMT figure" % sm_mhz)
+            bound = "fp32"
+            note = "algorithmic FLOPs of the prime-factor transform as executed (FMA = 2)"
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tp):
+            traffic = json.load(open(tp)).get(dname.split("[")[0], {}).get("bytes_per_launch")
+        return {"bound": bound, "kernel": dname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": src, "flops": note,
+                "flops_per_launch": dfl / dl, "avg_launch_ms": dms / dl}
+
+    def kernels(agg):
+        tot = sum(x[0] for x in agg.values())
+        return {k: {"ms_per_step": v[0] / args.steps, "share": v[0] / tot, "launches_per_step": v[1] / args.steps}
+                for k, v in agg.items()}
+
     clk = Clocks(local)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
     clk.start()
-    total_ms, launches, agg = 0.0, 0, {}
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)  # evict L2 between steps (outside the timed events)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-        cells_out = step_device()
-        with torch.cuda.stream(stream):
-            e1.record(stream)
-        e1.synchronize()
-        total_ms += e0.elapsed_time(e1)
-        st = ctx.last_stats()
-        launches += st["kernel_launches"]
-        for k, (ms, la, fl) in kernel_times().items():
-            a = agg.setdefault(k, [0.0, 0, 0.0])
-            a[0] += ms
-            a[1] += la
-            a[2] += fl
-    torch.cuda.synchronize()
+    ms_step, cells, agg, launches, out = measure(args.precision)
+    other = None
+    if not args.no_compare:
+        oprec = "fp32" if args.precision == "fp16tc" else "fp16tc"
+        other = (oprec,) + measure(oprec)
     clocks = clk.stop()
-    lib.tga_set_profiling(ctx._h, 0)
-    cells = ctx.last_stats()["cells"]
-    ms_step = total_ms / args.steps
-    if world > 1:
-        t = torch.tensor([ms_step], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
-        dist.barrier()
+    sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
     value = cells * world / (ms_step / 1e3)
 
     # end to end through the C ABI from pinned host memory
+    ctx.set_precision(prec_id[args.precision])
     host = pinned.numpy()
     e2e_times = []
     for i in range(0 if args.no_e2e else args.warmup + args.steps):
@@ -280,35 +350,32 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
 
-    # roofline of the dominant kernel (FP32 SIMT pipe)
-    dom = max(agg.items(), key=lambda kv: kv[1][0])
-    dname, (dms, dl, dfl) = dom
-    avg_launch_s = dms / dl / 1e3
-    achieved = dfl / dl / avg_launch_s / 1e12
-    sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
-    peak = fp32_peak_tflops(sm_mhz)
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(dname.split("[")[0], {}).get("bytes_per_launch")
-
+    dtype = {"fp32": "f32", "fp16tc": "f16-tc+f32"}
     line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f16-tc+f32", "data": "synthetic",
+            "vs_baseline": None, "dtype": dtype[args.precision], "data": "synthetic",
             "config": {"workload": WORKLOAD, "n_ant": n_ant, "cells_per_step_per_gpu": cells,
+                       "arithmetic": ("FP16 tensor-core (tcgen05) transform, FP32 accumulation, selected row "
+                                      "re-evaluated in FP32" if args.precision == "fp16tc"
+                                      else "FP32 CUDA-core transform"),
                        "l2": "256 MB buffer written between timed steps; 3.9 GB intermediate per step",
                        "parallelism": "replicas (weak scaling: one 24-antenna observation per GPU)"},
             "e2e": {"value": cells * world / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": h2d.value,
                     "d2h_bytes_per_step": d2h.value, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": launches,
-            "roofline": {"bound": "fp32", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": "148 SM x 128 FP32 lanes x 2 flop x median SM clock under load "
-                                        "(%.0f MHz); MEASURED_PEAKS.json has no FP32 SIMT figure" % sm_mhz,
-                         "flops_per_launch": dfl / dl, "avg_launch_ms": dms / dl},
-            "kernels": {k: {"ms_per_step": v[0] / args.steps, "share": v[0] / sum(x[0] for x in agg.values()),
-                            "launches_per_step": v[1] / args.steps} for k, v in agg.items()},
+            "roofline": roofline(agg, args.precision, sm_mhz),
+            "kernels": kernels(agg),
             "clocks": clocks}
+    if other is not None:
+        oprec, oms, ocells, oagg, olaunch, oout = other
+        da, ka = detections(out)
+        db, kb = detections(oout)
+        same = bool(np.array_equal(da, db) and np.array_equal(ka[da], kb[db]))
+        ovalue = ocells * world / (oms / 1e3)
+        line["compare"] = {"arithmetic": dtype[oprec], "value": ovalue, "ms_per_step": oms,
+                           "speedup_of_headline": value / ovalue, "same_detections": same,
+                           "detected_cells": int(da.sum()), "cells": int(len(da)),
+                           "roofline": roofline(oagg, oprec, sm_mhz), "gpu_launches": olaunch}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, desc = cpu_sample_baseline(os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": "cells/s", "cores": os.cpu_count(), "kind": "port",
