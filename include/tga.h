@@ -299,6 +299,57 @@ int tga_code_chips(int constellation, int prn, int8_t* out, size_t capacity, siz
 int tga_code_resampled(int constellation, int prn, double samples_per_code,
                        size_t num_samples, float* out);
 
+/* ---- fine acquisition --------------------------------------------------------
+ * Refines a grid estimate (the search's code phase and Doppler bin) of one
+ * satellite by Newton iteration on the coherent multi-antenna power
+ *
+ *   P = | sum_a exp(-i phi_a) R_a(tau, f) |^2,
+ *   R_a = (1/N) sum_n s_a[n] exp(+i 2 pi f (n - n0) / fs) c(n - tau),
+ *
+ * over a window of N samples (n0 its centre), with per-antenna carrier phases
+ * phi_a, continuous code delay tau (samples; the search's best_codephase
+ * convention) and carrier frequency f (Hz, absolute, like the search's
+ * Doppler grid).  c is the code with Gaussian-smoothed (sub)chip edges (a
+ * front-end filter model, edge_sigma_chips), which makes P smooth in tau.
+ * The window must hold no data-bit or secondary-code transition.
+ * Reference counterpart: optimize_fit (junk/acquisition.py:403-445), a scalar
+ * frequency search and a Gaussian fit of three code-phase samples. */
+typedef struct tga_fine_task {
+  int32_t constellation;     /* TGA_GPS ... TGA_QZSS                          */
+  int32_t prn;
+  double code_phase;         /* start delay, samples                          */
+  double frequency;          /* start carrier frequency, Hz                   */
+  int64_t start;             /* window: samples [start, start + length)       */
+  int64_t length;
+} tga_fine_task;
+typedef struct tga_fine_options {
+  double edge_sigma_chips;   /* replica edge smoothing, chips (0 -> 0.1)      */
+  double scan_half_width_hz; /* frequency pre-scan +- this around the start
+                                (0 -> 150 Hz + 1/window; < 0 -> no scan)      */
+  int32_t max_iter;          /* Newton evaluations (0 -> 20)                  */
+  double tol_code_phase;     /* convergence, samples (0 -> 1e-4)              */
+  double tol_frequency;      /* convergence, Hz (0 -> 1e-3)                   */
+} tga_fine_options;
+typedef struct tga_fine_result {
+  double code_phase;         /* refined delay, samples                         */
+  double frequency;          /* refined carrier frequency, Hz                  */
+  double power;              /* P at the solution                              */
+  double power_start;        /* P at the start point with aligned phases       */
+  int32_t iterations;        /* Newton evaluations used                        */
+  int32_t converged;         /* 1 when the last accepted step met the tolerances */
+} tga_fine_result;
+/* Refine n_tasks satellites on host packed bits [n_ant][row_bytes]; phases
+ * (n_tasks * n_ant, may be NULL) receives the fitted carrier phases. */
+int tga_fine_acquire(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, size_t row_bytes, double fs,
+                     const tga_fine_task* tasks, size_t n_tasks, const tga_fine_options* opt,
+                     tga_fine_result* out, double* phases);
+/* P, its gradient and Hessian at one point, in the parameter order
+ * (code_phase, frequency, phi_0 .. phi_{n_ant-1}): grad has 2 + n_ant
+ * entries, hess (2 + n_ant)^2 (row-major); either may be NULL. */
+int tga_fine_eval(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, size_t row_bytes, double fs,
+                  const tga_fine_task* task, const double* phases, double edge_sigma_chips, double* power,
+                  double* grad, double* hess);
+
 #ifdef __cplusplus
 }
 #endif

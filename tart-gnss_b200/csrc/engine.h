@@ -36,6 +36,19 @@ struct SampleSource {
   double pc = 0.0;  // TAU / fs, bits mode phase points pc * n
 };
 
+// One fine-acquisition evaluation: a (sub)chip sequence of seq_len entries,
+// T samples each, at continuous delay tau (samples) and carrier frequency
+// f_over_fs (cycles per sample), over samples [start, start + length) with
+// the carrier phase referred to sample n0; chip edges smoothed by a Gaussian
+// of sigma samples.  Sums land in out[slot][antenna][12].
+struct FineTask {
+  const int8_t* seq;
+  int seq_len;
+  int slot;
+  double T, tau, f_over_fs, two_pi_over_fs, n0, sigma;
+  long long start, length;
+};
+
 struct SearchDims {
   int n_ant = 0, nb = 0, n_prn = 0;
   const double* fc = nullptr;  // device Doppler grid [nb]
@@ -117,6 +130,12 @@ cudaError_t launch_bits_to_signal(const uint8_t* d_bits, size_t row_bytes, int r
 // Selects an alternative launch configuration of the transform kernels for
 // third digit M (tuning; 0 = default).
 void set_pfa_variant(int M, int v);
+
+// fine acquisition: per (task, antenna) the complex sums R, dR/dtau, dR/df,
+// d2R/dtau2, d2R/df2, d2R/dtau df (un-normalised), zeroed and accumulated
+cudaError_t launch_fine_sums(const uint8_t* d_bits, int n_ant, size_t row_bytes, const double* d_mean,
+                             const FineTask* d_tasks, int n_tasks, long long max_length, double* d_out,
+                             cudaStream_t st);
 
 int kernel_launch_count_reset();
 void kernel_launch_add(int n);

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -1000,6 +1001,358 @@ int tga_antenna_xcorr(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant, size_t 
     CK(cudaStreamSynchronize(ctx->stream));
     const double n = (double)(row_bytes * 8);
     *out = (2.0 * (double)cnt[1] - n) / n;
+    return TGA_OK;
+  });
+}
+
+// ---------------------------------------------------------------------------
+// fine acquisition (tga_fine_eval, tga_fine_acquire)
+// ---------------------------------------------------------------------------
+namespace {
+
+using cplx = std::complex<double>;
+
+struct FineOpts {
+  double sigma_chips = 0.1, scan_hw = 0.0, tol_tau = 1e-4, tol_f = 1e-3;
+  int max_iter = 20;
+};
+
+FineOpts fine_opts(const tga_fine_options* o) {
+  FineOpts r;
+  if (!o) return r;
+  if (o->edge_sigma_chips > 0) r.sigma_chips = o->edge_sigma_chips;
+  r.scan_hw = o->scan_half_width_hz;
+  if (o->max_iter > 0) r.max_iter = o->max_iter;
+  if (o->tol_code_phase > 0) r.tol_tau = o->tol_code_phase;
+  if (o->tol_frequency > 0) r.tol_f = o->tol_frequency;
+  return r;
+}
+
+// replica model of one satellite: its (sub)chip sequence on the device, T
+// samples per (sub)chip, edge smoothing sigma in samples
+struct FineJob {
+  tga_fine_task t;
+  const int8_t* d_seq = nullptr;
+  int L = 0;
+  double T = 0, sigma = 0;
+};
+
+FineJob fine_job(tga_ctx* ctx, double fs, const tga_fine_task& t, double sigma_chips, size_t total_samples) {
+  if (t.constellation < 0 || t.constellation >= N_CONST) throw InvalidArg("bad constellation");
+  validate_prn(t.constellation, t.prn);
+  if (t.length <= 0 || t.start < 0 || (size_t)(t.start + t.length) > total_samples)
+    throw InvalidArg("fine-acquisition window outside the recording");
+  if (!std::isfinite(t.code_phase) || !std::isfinite(t.frequency)) throw InvalidArg("non-finite start point");
+  const ConstellationInfo& ci = info(t.constellation);
+  FineJob j;
+  j.t = t;
+  const std::string name = "fine.seq." + std::to_string(t.constellation) + "." + std::to_string(t.prn);
+  const std::vector<int8_t> seq = resample_sequence(t.constellation, t.prn);
+  j.L = (int)seq.size();
+  j.d_seq = (const int8_t*)ctx->buf(name, seq.size());
+  if (!ctx->uploaded.count(name)) {
+    CK(cudaMemcpy((void*)j.d_seq, seq.data(), seq.size(), cudaMemcpyHostToDevice));
+    ctx->uploaded[name] = {};
+  }
+  j.T = fs * ci.code_period_s / (double)j.L;
+  j.sigma = sigma_chips * fs * ci.code_period_s / (double)ci.primary_chips;
+  return j;
+}
+
+FineTask fine_task(const FineJob& j, double fs, double tau, double f, int slot) {
+  FineTask k;
+  k.seq = j.d_seq;
+  k.seq_len = j.L;
+  k.slot = slot;
+  k.T = j.T;
+  k.tau = tau;
+  k.f_over_fs = f / fs;
+  k.two_pi_over_fs = 2.0 * M_PI / fs;
+  k.start = j.t.start;
+  k.length = j.t.length;
+  k.n0 = (double)j.t.start + 0.5 * (double)j.t.length;
+  k.sigma = j.sigma;
+  return k;
+}
+
+// device bits and the antenna means (over the whole row, as the search)
+void fine_upload(tga_ctx* ctx, const uint8_t* h_bits, size_t A, size_t row_bytes, const uint8_t** d_bits,
+                 const double** d_mean) {
+  uint8_t* b = (uint8_t*)ctx->buf("fine.bits", A * row_bytes);
+  CK(cudaMemcpyAsync(b, h_bits, A * row_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->h2d += A * row_bytes;
+  double* m = (double*)ctx->buf("fine.mean", A * sizeof(double));
+  CK(launch_antenna_means(b, (int)A, row_bytes, m, ctx->stream));
+  *d_bits = b;
+  *d_mean = m;
+}
+
+// sums of a batch of evaluations, normalised by the window length:
+// out[task][antenna][R, dR/dtau, dR/df, d2R/dtau2, d2R/df2, d2R/dtau df]
+void fine_sums(tga_ctx* ctx, const uint8_t* d_bits, size_t A, size_t row_bytes, const double* d_mean,
+               const std::vector<FineTask>& tasks, std::vector<cplx>& out) {
+  const size_t n = tasks.size();
+  FineTask* d_tasks = (FineTask*)ctx->buf("fine.tasks", n * sizeof(FineTask));
+  double* d_out = (double*)ctx->buf("fine.sums", n * A * 12 * sizeof(double));
+  CK(cudaMemcpyAsync(d_tasks, tasks.data(), n * sizeof(FineTask), cudaMemcpyHostToDevice, ctx->stream));
+  long long max_len = 0;
+  for (const FineTask& t : tasks) max_len = std::max(max_len, t.length);
+  CK(launch_fine_sums(d_bits, (int)A, row_bytes, d_mean, d_tasks, (int)n, max_len, d_out, ctx->stream));
+  std::vector<double> h(n * A * 12);
+  CK(cudaMemcpyAsync(h.data(), d_out, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  out.resize(n * A * 6);
+  for (size_t i = 0; i < n; ++i) {
+    const double inv = 1.0 / (double)tasks[i].length;
+    for (size_t k = 0; k < A * 6; ++k)
+      out[i * A * 6 + k] = cplx(h[i * A * 12 + 2 * k], h[i * A * 12 + 2 * k + 1]) * inv;
+  }
+}
+
+// P = |sum_a exp(-i phi_a) R_a|^2 with its gradient and Hessian in the order
+// (tau, f, phi_0 .. phi_{A-1}); g and H may be null
+void fine_assemble(const cplx* R, int A, const double* phi, double* P, double* g, double* H) {
+  cplx S, St, Sf, Stt, Sff, Stf;
+  std::vector<cplx> u(A);
+  for (int a = 0; a < A; ++a) {
+    u[a] = std::polar(1.0, -phi[a]);
+    const cplx* r = R + (size_t)a * 6;
+    S += u[a] * r[0];
+    St += u[a] * r[1];
+    Sf += u[a] * r[2];
+    Stt += u[a] * r[3];
+    Sff += u[a] * r[4];
+    Stf += u[a] * r[5];
+  }
+  const cplx cS = std::conj(S);
+  *P = std::norm(S);
+  const int D = 2 + A;
+  const cplx mi(0.0, -1.0);
+  if (g) {
+    g[0] = 2.0 * (cS * St).real();
+    g[1] = 2.0 * (cS * Sf).real();
+    for (int a = 0; a < A; ++a) g[2 + a] = 2.0 * (cS * (mi * u[a] * R[(size_t)a * 6])).real();
+  }
+  if (H) {
+    H[0] = 2.0 * (std::conj(St) * St + cS * Stt).real();
+    H[D + 1] = 2.0 * (std::conj(Sf) * Sf + cS * Sff).real();
+    H[1] = H[D] = 2.0 * (std::conj(St) * Sf + cS * Stf).real();
+    for (int a = 0; a < A; ++a) {
+      const cplx* r = R + (size_t)a * 6;
+      const cplx Q = mi * u[a] * r[0], Qt = mi * u[a] * r[1], Qf = mi * u[a] * r[2];
+      H[2 + a] = H[(size_t)(2 + a) * D] = 2.0 * (std::conj(St) * Q + cS * Qt).real();
+      H[D + 2 + a] = H[(size_t)(2 + a) * D + 1] = 2.0 * (std::conj(Sf) * Q + cS * Qf).real();
+      for (int b = 0; b < A; ++b) {
+        const cplx Qb = mi * u[b] * R[(size_t)b * 6];
+        double v = 2.0 * (std::conj(Q) * Qb).real();
+        if (a == b) v += 2.0 * (cS * (-u[a] * r[0])).real();
+        H[(size_t)(2 + a) * D + 2 + b] = v;
+      }
+    }
+  }
+}
+
+// solves M x = b for symmetric positive definite M (n x n, overwritten);
+// false when M is not positive definite
+bool cholesky_solve(std::vector<double>& M, std::vector<double>& b, int n) {
+  for (int j = 0; j < n; ++j) {
+    double d = M[(size_t)j * n + j];
+    for (int k = 0; k < j; ++k) d -= M[(size_t)j * n + k] * M[(size_t)j * n + k];
+    if (!(d > 0.0)) return false;
+    d = std::sqrt(d);
+    M[(size_t)j * n + j] = d;
+    for (int i = j + 1; i < n; ++i) {
+      double v = M[(size_t)i * n + j];
+      for (int k = 0; k < j; ++k) v -= M[(size_t)i * n + k] * M[(size_t)j * n + k];
+      M[(size_t)i * n + j] = v / d;
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    double v = b[i];
+    for (int k = 0; k < i; ++k) v -= M[(size_t)i * n + k] * b[k];
+    b[i] = v / M[(size_t)i * n + i];
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double v = b[i];
+    for (int k = i + 1; k < n; ++k) v -= M[(size_t)k * n + i] * b[k];
+    b[i] = v / M[(size_t)i * n + i];
+  }
+  return true;
+}
+
+}  // namespace
+
+int tga_fine_eval(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant, size_t row_bytes, double fs,
+                  const tga_fine_task* task, const double* phases, double edge_sigma_chips, double* power,
+                  double* grad, double* hess) {
+  return guarded(ctx, [&] {
+    if (!h_bits || !task || !power || n_ant == 0 || row_bytes == 0 || !(fs > 0)) throw InvalidArg("bad arguments");
+    const FineJob j = fine_job(ctx, fs, *task, edge_sigma_chips > 0 ? edge_sigma_chips : 0.1, row_bytes * 8);
+    const uint8_t* d_bits;
+    const double* d_mean;
+    fine_upload(ctx, h_bits, n_ant, row_bytes, &d_bits, &d_mean);
+    std::vector<cplx> R;
+    fine_sums(ctx, d_bits, n_ant, row_bytes, d_mean, {fine_task(j, fs, task->code_phase, task->frequency, 0)}, R);
+    std::vector<double> phi(n_ant);
+    for (size_t a = 0; a < n_ant; ++a) phi[a] = phases ? phases[a] : std::arg(R[a * 6]);
+    fine_assemble(R.data(), (int)n_ant, phi.data(), power, grad, hess);
+    return TGA_OK;
+  });
+}
+
+int tga_fine_acquire(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant, size_t row_bytes, double fs,
+                     const tga_fine_task* tasks, size_t n_tasks, const tga_fine_options* opt,
+                     tga_fine_result* out, double* phases) {
+  return guarded(ctx, [&] {
+    if (!h_bits || (!tasks && n_tasks) || (!out && n_tasks) || n_ant == 0 || row_bytes == 0 || !(fs > 0))
+      throw InvalidArg("bad arguments");
+    if (n_tasks == 0) return TGA_OK;
+    const FineOpts o = fine_opts(opt);
+    const int A = (int)n_ant;
+    std::vector<FineJob> jobs;
+    for (size_t i = 0; i < n_tasks; ++i) jobs.push_back(fine_job(ctx, fs, tasks[i], o.sigma_chips, row_bytes * 8));
+    const uint8_t* d_bits;
+    const double* d_mean;
+    fine_upload(ctx, h_bits, n_ant, row_bytes, &d_bits, &d_mean);
+
+    struct St {
+      double tau, f, P = 0, lambda = 0;
+      std::vector<double> phi;
+      std::vector<cplx> R;  // sums at (tau, f)
+      bool done = false, conv = false;
+      int iters = 0;
+    };
+    std::vector<St> st(n_tasks);
+    std::vector<cplx> R;
+    auto aligned = [&](const cplx* r, std::vector<double>& phi) {
+      double s = 0;
+      phi.resize(A);
+      for (int a = 0; a < A; ++a) {
+        phi[a] = std::arg(r[(size_t)a * 6]);
+        s += std::abs(r[(size_t)a * 6]);
+      }
+      return s * s;  // P with every antenna phase-aligned
+    };
+
+    // 1. frequency pre-scan: the grid's Doppler bins are coarser than the
+    //    main lobe of a long window, so the start may sit on a side lobe
+    std::vector<int> nscan(n_tasks, 0);
+    std::vector<FineTask> batch;
+    for (size_t i = 0; i < n_tasks; ++i) {
+      const double win = (double)tasks[i].length / fs;
+      const double df = 0.25 / win;
+      const double hw = o.scan_hw == 0.0 ? 150.0 + 1.0 / win : o.scan_hw;
+      const int K = hw < 0 ? 0 : (int)std::ceil(hw / df);
+      nscan[i] = K;
+      for (int k = -K; k <= K; ++k)
+        batch.push_back(fine_task(jobs[i], fs, tasks[i].code_phase, tasks[i].frequency + k * df, (int)batch.size()));
+    }
+    fine_sums(ctx, d_bits, n_ant, row_bytes, d_mean, batch, R);
+    size_t pos = 0;
+    for (size_t i = 0; i < n_tasks; ++i) {
+      const double df = 0.25 * fs / (double)tasks[i].length;
+      const int K = nscan[i];
+      double best = -1;
+      int kb = 0;
+      std::vector<double> tmp;
+      for (int k = -K; k <= K; ++k, ++pos) {
+        const double p = aligned(&R[pos * n_ant * 6], tmp);
+        if (k == 0) out[i].power_start = p;
+        if (p > best) {
+          best = p;
+          kb = k;
+        }
+      }
+      st[i].tau = tasks[i].code_phase;
+      st[i].f = tasks[i].frequency + kb * df;
+    }
+    // 2. phase-aligned start at the scan maximum
+    batch.clear();
+    for (size_t i = 0; i < n_tasks; ++i) batch.push_back(fine_task(jobs[i], fs, st[i].tau, st[i].f, (int)i));
+    fine_sums(ctx, d_bits, n_ant, row_bytes, d_mean, batch, R);
+    for (size_t i = 0; i < n_tasks; ++i) {
+      st[i].R.assign(R.begin() + i * n_ant * 6, R.begin() + (i + 1) * n_ant * 6);
+      st[i].P = aligned(st[i].R.data(), st[i].phi);
+    }
+
+    // 3. damped Newton (Levenberg-Marquardt) on (tau, f, phi_1 .. phi_{A-1});
+    //    phi_0 stays fixed because P does not change with a common phase
+    const int D = 2 + A, Dr = 1 + A;
+    std::vector<double> g(D), H((size_t)D * D), M((size_t)Dr * Dr), b(Dr);
+    for (int it = 0; it < o.max_iter; ++it) {
+      batch.clear();
+      std::vector<int> who;
+      std::vector<std::vector<double>> trial_phi;
+      std::vector<double> trial_dtau, trial_df;
+      for (size_t i = 0; i < n_tasks; ++i) {
+        St& s = st[i];
+        if (s.done) continue;
+        double P;
+        fine_assemble(s.R.data(), A, s.phi.data(), &P, g.data(), H.data());
+        // reduced system (drop phi_0 = index 2)
+        auto red = [&](int r) { return r < 2 ? r : r + 1; };
+        double dmax = 0;
+        for (int r = 0; r < Dr; ++r) dmax = std::max(dmax, std::abs(H[(size_t)red(r) * D + red(r)]));
+        bool ok = false;
+        for (int tries = 0; tries < 12 && !ok; ++tries) {
+          for (int r = 0; r < Dr; ++r) {
+            b[r] = g[red(r)];
+            for (int c = 0; c < Dr; ++c) M[(size_t)r * Dr + c] = -H[(size_t)red(r) * D + red(c)];
+            M[(size_t)r * Dr + r] += s.lambda * std::max(std::abs(H[(size_t)red(r) * D + red(r)]), 1e-12 * dmax);
+          }
+          ok = cholesky_solve(M, b, Dr);
+          if (!ok) s.lambda = s.lambda == 0 ? 1e-3 : s.lambda * 10;
+        }
+        if (!ok) {
+          s.done = true;
+          continue;
+        }
+        // stay inside the smooth peak: at most 2 samples and half a main lobe per step
+        const double win = (double)tasks[i].length / fs;
+        double scale = 1.0;
+        if (std::abs(b[0]) > 2.0) scale = 2.0 / std::abs(b[0]);
+        if (std::abs(b[1]) > 0.5 / win) scale = std::min(scale, 0.5 / win / std::abs(b[1]));
+        std::vector<double> phi = s.phi;
+        for (int a = 1; a < A; ++a) phi[a] += scale * b[1 + a];
+        who.push_back((int)i);
+        trial_phi.push_back(phi);
+        trial_dtau.push_back(scale * b[0]);
+        trial_df.push_back(scale * b[1]);
+        batch.push_back(fine_task(jobs[i], fs, s.tau + scale * b[0], s.f + scale * b[1], (int)batch.size()));
+      }
+      if (batch.empty()) break;
+      fine_sums(ctx, d_bits, n_ant, row_bytes, d_mean, batch, R);
+      for (size_t k = 0; k < who.size(); ++k) {
+        St& s = st[who[k]];
+        ++s.iters;
+        double Pn;
+        fine_assemble(&R[k * n_ant * 6], A, trial_phi[k].data(), &Pn, nullptr, nullptr);
+        if (Pn >= s.P) {
+          s.tau += trial_dtau[k];
+          s.f += trial_df[k];
+          s.phi = trial_phi[k];
+          s.R.assign(R.begin() + k * n_ant * 6, R.begin() + (k + 1) * n_ant * 6);
+          s.P = Pn;
+          s.lambda = s.lambda < 1e-6 ? 0.0 : s.lambda * 0.1;
+          if (std::abs(trial_dtau[k]) < o.tol_tau && std::abs(trial_df[k]) < o.tol_f) {
+            s.conv = true;
+            s.done = true;
+          }
+        } else {
+          s.lambda = s.lambda == 0 ? 1e-3 : s.lambda * 10;
+          if (s.lambda > 1e12) s.done = true;
+        }
+      }
+    }
+    for (size_t i = 0; i < n_tasks; ++i) {
+      out[i].code_phase = st[i].tau;
+      out[i].frequency = st[i].f;
+      out[i].power = st[i].P;
+      out[i].iterations = st[i].iters;
+      out[i].converged = st[i].conv ? 1 : 0;
+      if (phases)
+        for (int a = 0; a < A; ++a) phases[i * n_ant + a] = st[i].phi[a];
+    }
     return TGA_OK;
   });
 }

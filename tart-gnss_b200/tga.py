@@ -73,6 +73,22 @@ CELL_DTYPE = np.dtype([("constellation", "<i4"), ("prn", "<i4"), ("antenna", "<i
 assert CELL_DTYPE.itemsize == ctypes.sizeof(Cell)
 
 _lib = None
+class FineTask(ctypes.Structure):
+    """tga_fine_task: start point and window of one satellite's refinement."""
+    _fields_ = [("constellation", ctypes.c_int32), ("prn", ctypes.c_int32), ("code_phase", ctypes.c_double),
+                ("frequency", ctypes.c_double), ("start", ctypes.c_int64), ("length", ctypes.c_int64)]
+
+
+class FineOptions(ctypes.Structure):
+    _fields_ = [("edge_sigma_chips", ctypes.c_double), ("scan_half_width_hz", ctypes.c_double),
+                ("max_iter", ctypes.c_int32), ("tol_code_phase", ctypes.c_double), ("tol_frequency", ctypes.c_double)]
+
+
+class FineResult(ctypes.Structure):
+    _fields_ = [("code_phase", ctypes.c_double), ("frequency", ctypes.c_double), ("power", ctypes.c_double),
+                ("power_start", ctypes.c_double), ("iterations", ctypes.c_int32), ("converged", ctypes.c_int32)]
+
+
 _P = ctypes.c_void_p
 
 
@@ -109,6 +125,8 @@ def lib():
     L.tga_set_profiling.argtypes = [_P, i32]
     L.tga_set_variant.argtypes = [_P, i32, i32]
     L.tga_set_precision.argtypes = [_P, i32]
+    L.tga_fine_eval.argtypes = [_P, _P, sz, sz, dbl, _P, _P, dbl, _P, _P, _P]
+    L.tga_fine_acquire.argtypes = [_P, _P, sz, sz, dbl, _P, sz, _P, _P, _P]
     L.tga_acquire_single_static.argtypes = [i32, _P, _P, sz, dbl, dbl, dbl, i32, sz, _P, _P]
     L.tga_last_transfer_bytes.argtypes = [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.tga_kernel_times.argtypes = [_P, i32, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_int)]
@@ -331,6 +349,39 @@ class Context:
         self._check(lib().tga_antenna_xcorr(self._h, _ptr(bits), bits.shape[0], bits.shape[1], i, j,
                                             ctypes.byref(out)))
         return out.value
+
+    def fine_eval(self, packed_bits, sampling_freq, constellation, prn, code_phase, frequency, start, length,
+                  phases=None, edge_sigma_chips=0.1):
+        """Coherent power P, gradient and Hessian at one point, parameter order
+        (code_phase, frequency, phi_0 .. phi_{A-1}); phases None = aligned."""
+        bits = np.ascontiguousarray(packed_bits, dtype=np.uint8)
+        A = bits.shape[0]
+        t = FineTask(constellation, prn, float(code_phase), float(frequency), int(start), int(length))
+        ph = None if phases is None else np.ascontiguousarray(phases, dtype=np.float64)
+        P = ctypes.c_double()
+        g = np.zeros(2 + A)
+        H = np.zeros((2 + A, 2 + A))
+        self._check(lib().tga_fine_eval(self._h, _ptr(bits), A, bits.shape[1], float(sampling_freq), ctypes.byref(t),
+                                        None if ph is None else _ptr(ph), float(edge_sigma_chips), ctypes.byref(P),
+                                        _ptr(g), _ptr(H)))
+        return P.value, g, H
+
+    def fine_acquire(self, packed_bits, sampling_freq, tasks, edge_sigma_chips=0.1, scan_half_width_hz=0.0,
+                     max_iter=0):
+        """Newton refinement of (code_phase, frequency) per task, tasks being
+        (constellation, prn, code_phase, frequency, start, length) tuples.
+        Returns (list of dicts, phases [n_tasks, n_ant])."""
+        bits = np.ascontiguousarray(packed_bits, dtype=np.uint8)
+        A = bits.shape[0]
+        arr = (FineTask * len(tasks))(*[FineTask(int(c), int(p), float(cp), float(f), int(s0), int(n))
+                                        for c, p, cp, f, s0, n in tasks])
+        out = (FineResult * len(tasks))()
+        phases = np.zeros((len(tasks), A))
+        opt = FineOptions(float(edge_sigma_chips), float(scan_half_width_hz), int(max_iter), 0.0, 0.0)
+        self._check(lib().tga_fine_acquire(self._h, _ptr(bits), A, bits.shape[1], float(sampling_freq), arr,
+                                           len(tasks), ctypes.byref(opt), out, _ptr(phases)))
+        res = [{k: getattr(r, k) for k, _ in FineResult._fields_} for r in out]
+        return res, phases
 
     def correlation_matrix(self, packed_bits):
         bits = np.ascontiguousarray(packed_bits, dtype=np.uint8)

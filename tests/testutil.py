@@ -132,3 +132,36 @@ def make_observation(n_ant, n_samples, fs, sats, seed, noise_sigma=1.0):
         bits[a] = (v >= 0.0).astype(np.uint8)
     packed = np.packbits(bits, axis=1)
     return packed, bits
+
+
+# code period (s) and primary chips per constellation (GPS, Galileo, BeiDou,
+# SBAS, L1C, QZSS), for the band-limited fine-acquisition front end
+CODE_PERIOD_S = {0: 1e-3, 1: 4e-3, 2: 10e-3, 3: 1e-3, 4: 10e-3, 5: 1e-3}
+PRIMARY_CHIPS = {0: 1023, 1: 4092, 2: 10230, 3: 1023, 4: 10230, 5: 1023}
+
+
+def synth_fine(sats, n_ant, n_samples, fs, sigma_chips, seed, if_hz=4.092e6):
+    """Band-limited 1-bit recording for fine acquisition: every satellite
+    (dict c, prn, tau (continuous delay, samples), dop (Hz), cn0 (dB-Hz))
+    reaches every antenna with the same delay and Doppler and its own random
+    carrier phase; its code edges are smoothed by the same Gaussian front end
+    the fine-acquisition replica models (sigma_chips).  Unit Gaussian noise,
+    sign-quantised, packed MSB-first.  Returns (bits, per-satellite phases)."""
+    import fine_oracle as FO
+    import tga
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((n_ant, n_samples))
+    n = np.arange(n_samples, dtype=np.float64)
+    phases = []
+    for s in sats:
+        seq = tga.code_chips(s["c"], s["prn"]).astype(np.float64)
+        T, sigma = FO.model_geometry(len(seq), CODE_PERIOD_S[s["c"]], PRIMARY_CHIPS[s["c"]], fs, sigma_chips)
+        code = FO.band_limited_signal(seq, T, sigma, n, s["tau"])
+        amp = 2.0 * math.sqrt(10.0 ** (s["cn0"] / 10.0) / fs)
+        th = rng.uniform(0, 2 * np.pi, size=n_ant)
+        phases.append(th)
+        cyc = np.mod((if_hz + s["dop"]) / fs * n, 1.0)
+        for a in range(n_ant):
+            x[a] += amp * code * np.cos(2 * np.pi * cyc + th[a])
+    bits = np.packbits(x >= 0.0, axis=1)
+    return bits, phases
