@@ -7,7 +7,8 @@
 //
 //  * odd prime R (3, 5, 11, 31): symmetric split into s_n = x_n + x_{R-n} and
 //    d_n = x_n - x_{R-n}; each output pair (k, R-k) costs (R-1) real FMAs per
-//    component: 4*((R-1)/2)^2 + O(R) instructions per R points.
+//    component, issued as packed FP32 pairs (re, im): 2*((R-1)/2)^2 + O(R)
+//    instructions per R points.
 //  * 33 = 3 x 11 and 10 = 2 x 5 as Good-Thomas prime-factor maps (no twiddles):
 //    input digit map n = (N2*n1 + N1*n2) mod N, output map by the Chinese
 //    remainder theorem.
@@ -19,8 +20,11 @@
 
 namespace tga {
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex adds use the packed FP32 instructions of sm_100 (one instruction
+// for the real and imaginary parts; per component the same rounding as the
+// scalar operation, so results are bit-identical to the scalar forms).
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
@@ -35,6 +39,17 @@ template <> __device__ __forceinline__ float kcos<11>(int m) { return kCos11[m];
 template <> __device__ __forceinline__ float ksin<11>(int m) { return kSin11[m]; }
 template <> __device__ __forceinline__ float kcos<31>(int m) { return kCos31[m]; }
 template <> __device__ __forceinline__ float ksin<31>(int m) { return kSin31[m]; }
+// the same constants as (v, v) pairs
+template <int R> __device__ __forceinline__ float2 kcos2(int m);
+template <int R> __device__ __forceinline__ float2 ksin2(int m);
+template <> __device__ __forceinline__ float2 kcos2<3>(int m) { return kCos3x2[m]; }
+template <> __device__ __forceinline__ float2 ksin2<3>(int m) { return kSin3x2[m]; }
+template <> __device__ __forceinline__ float2 kcos2<5>(int m) { return kCos5x2[m]; }
+template <> __device__ __forceinline__ float2 ksin2<5>(int m) { return kSin5x2[m]; }
+template <> __device__ __forceinline__ float2 kcos2<11>(int m) { return kCos11x2[m]; }
+template <> __device__ __forceinline__ float2 ksin2<11>(int m) { return kSin11x2[m]; }
+template <> __device__ __forceinline__ float2 kcos2<31>(int m) { return kCos31x2[m]; }
+template <> __device__ __forceinline__ float2 ksin2<31>(int m) { return kSin31x2[m]; }
 
 // DFT of odd prime length R; input x[0..R-1] (read only), outputs via st.
 template <int R, bool INV, class St>
