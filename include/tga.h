@@ -299,6 +299,31 @@ int tga_code_chips(int constellation, int prn, int8_t* out, size_t capacity, siz
 int tga_code_resampled(int constellation, int prn, double samples_per_code,
                        size_t num_samples, float* out);
 
+/* ---- narrowband RFI scan (--rfi) ----------------------------------------------
+ * rfi::analyze_channel (rfi.rs:145-168) for every antenna row: spectral lines
+ * at least 15 dB above the median bin power of the whole record (f64 FFT),
+ * clustered within 10 kHz, strongest first, at most 3 (rfi.rs:91-140); the
+ * implied period fs / f of the strongest; the autocorrelation at lags 1, 3,
+ * 16 (rfi.rs:84-87).  Dead channels (variance < 1e-9) carry NaN fields and no
+ * lines.  NaN stands for the reference's None. */
+typedef struct tga_rfi_line {
+  double frequency;          /* Hz */
+  double excess_db;          /* dB above the median bin power */
+} tga_rfi_line;
+typedef struct tga_rfi_channel {
+  int32_t antenna;
+  int32_t dead;
+  double acf_lag1, acf_lag3, acf_lag16;
+  double period_samples;
+  int32_t n_lines;
+  tga_rfi_line lines[3];
+} tga_rfi_channel;
+int tga_rfi_scan(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, size_t row_bytes, double fs,
+                 tga_rfi_channel* out);
+/* RfiReport as serde_json::to_string_pretty writes it (main.rs:439-478);
+ * *json is malloc'd, release with tga_free. */
+int tga_rfi_json(const tga_rfi_channel* channels, size_t n, char** json);
+
 /* ---- fine acquisition --------------------------------------------------------
  * Refines a grid estimate (the search's code phase and Doppler bin) of one
  * satellite by Newton iteration on the coherent multi-antenna power

@@ -4,9 +4,9 @@
 // main.rs:61-167), implications (apply_mode_implications main.rs:172-210),
 // acquisition mode (main.rs:696-904, JSON CombinedOutput on stdout or
 // --output), correlation mode --i/--j (main.rs:907-928) and --benchmark
-// (main.rs:482-694).  Modes outside the acquisition search (--simulate,
-// --rfi, --test-antennas) are reported as unsupported.  Errors exit with
-// status 1 like the reference.
+// (main.rs:482-694) and the RFI report --rfi (main.rs:439-478, rfi.rs).
+// Modes outside these (--simulate, --test-antennas) are reported as
+// unsupported.  Errors exit with status 1 like the reference.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -157,7 +157,6 @@ int main(int argc, char** argv) {
     return 0;
   }
   if (a.simulate) die("--simulate is not part of this engine (acquisition search only)", argv[0], false);
-  if (a.rfi) die("--rfi is not part of this engine (acquisition search only)", argv[0], false);
 
   tga_observation obs;
   std::memset(&obs, 0, sizeof obs);
@@ -188,6 +187,23 @@ int main(int argc, char** argv) {
   if (rc != TGA_OK) {
     std::fprintf(stderr, "no usable B200 (sm_100) GPU: status %d\n", rc);
     return 1;
+  }
+
+  if (a.rfi) {
+    // main.rs:439-478: the RFI report of every antenna, then exit
+    std::vector<tga_rfi_channel> ch(n_ant);
+    rc = tga_rfi_scan(ctx, obs.data, n_ant, obs.row_bytes, fs, ch.data());
+    if (rc != TGA_OK) {
+      std::fprintf(stderr, "RFI scan failed: %s\n", tga_last_error(ctx));
+      return 1;
+    }
+    char* json = nullptr;
+    if (tga_rfi_json(ch.data(), ch.size(), &json) != TGA_OK) return 1;
+    write_out(json, a.output, "RFI JSON");
+    tga_free(json);
+    tga_destroy(ctx);
+    tga_observation_free(&obs);
+    return 0;
   }
 
   if (a.benchmark) {

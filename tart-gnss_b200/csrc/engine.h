@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
 #include <vector>
 
 namespace tga {
@@ -136,6 +137,14 @@ void set_pfa_variant(int M, int v);
 cudaError_t launch_fine_sums(const uint8_t* d_bits, int n_ant, size_t row_bytes, const double* d_mean,
                              const FineTask* d_tasks, int n_tasks, long long max_length, double* d_out,
                              cudaStream_t st);
+
+// narrowband RFI scan of every antenna row (rfi.rs:91-168): f64 spectrum,
+// exact median bin power, local maxima above 15 dB (up to cap per antenna,
+// d_count counts all), exact autocorrelation popcounts at lags 1, 3, 16
+cudaError_t rfi_scan_device(const uint8_t* d_bits, int n_ant, size_t row_bytes, const double* d_mean, double* d_z,
+                            void* d_X, double* d_p, unsigned* d_hist, unsigned long long* d_prefix,
+                            unsigned long long* d_rank, int cap, unsigned* d_count, long long* d_bins,
+                            double* d_excess, unsigned long long* d_acf, cudaStream_t st, std::string* why);
 
 int kernel_launch_count_reset();
 void kernel_launch_add(int n);

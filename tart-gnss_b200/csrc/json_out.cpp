@@ -240,6 +240,51 @@ extern "C" int tga_results_json(const tga_cell* cells, size_t n_cells, const int
   }
 }
 
+// RfiReport (rfi.rs:76-81) in serde_json's pretty layout: Option::None is
+// written as null, empty line lists as [].
+extern "C" int tga_rfi_json(const tga_rfi_channel* ch, size_t n, char** json) {
+  if (!json || (!ch && n)) return TGA_ERR_INVALID_ARG;
+  auto opt = [](double v) { return std::isnan(v) ? std::string("null") : fmt_f64(v); };
+  std::string s = "{\n  \"antenna_numbers\": [";
+  if (n == 0) {
+    s += "]";
+  } else {
+    for (size_t i = 0; i < n; ++i) s += (i ? ",\n    " : "\n    ") + std::to_string(ch[i].antenna);
+    s += "\n  ]";
+  }
+  s += ",\n  \"channels\": [";
+  if (n == 0) s += "]";
+  for (size_t i = 0; i < n; ++i) {
+    const tga_rfi_channel& c = ch[i];
+    s += i ? ",\n    {\n" : "\n    {\n";
+    s += "      \"antenna\": " + std::to_string(c.antenna) + ",\n";
+    s += std::string("      \"dead\": ") + (c.dead ? "true" : "false") + ",\n";
+    s += "      \"acf_lag1\": " + opt(c.acf_lag1) + ",\n";
+    s += "      \"acf_lag3\": " + opt(c.acf_lag3) + ",\n";
+    s += "      \"acf_lag16\": " + opt(c.acf_lag16) + ",\n";
+    s += "      \"period_samples\": " + opt(c.period_samples) + ",\n";
+    s += "      \"lines\": [";
+    if (c.n_lines == 0) {
+      s += "]";
+    } else {
+      for (int k = 0; k < c.n_lines; ++k) {
+        s += k ? ",\n        {\n" : "\n        {\n";
+        s += "          \"frequency\": " + fmt_f64(c.lines[k].frequency) + ",\n";
+        s += "          \"excess_db\": " + fmt_f64(c.lines[k].excess_db) + "\n        }";
+      }
+      s += "\n      ]";
+    }
+    s += "\n    }";
+    if (i + 1 == n) s += "\n  ]";
+  }
+  s += "\n}";
+  char* out = (char*)std::malloc(s.size() + 1);
+  if (!out) return TGA_ERR_OUT_OF_MEMORY;
+  std::memcpy(out, s.c_str(), s.size() + 1);
+  *json = out;
+  return TGA_OK;
+}
+
 extern "C" int tga_format_f64(double v, char* out, size_t cap) {
   const std::string s = fmt_f64(v);
   if (!out || cap < s.size() + 1) return TGA_ERR_CAPACITY;

@@ -1357,6 +1357,102 @@ int tga_fine_acquire(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant, size_t r
   });
 }
 
+// ---------------------------------------------------------------------------
+// narrowband RFI scan (tga_rfi_scan), rfi.rs:91-168
+// ---------------------------------------------------------------------------
+int tga_rfi_scan(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant, size_t row_bytes, double fs,
+                 tga_rfi_channel* out) {
+  return guarded(ctx, [&] {
+    if (!h_bits || !out || n_ant == 0 || row_bytes == 0 || !(fs > 0)) throw InvalidArg("bad arguments");
+    const size_t A = n_ant;
+    const long long n = (long long)row_bytes * 8, half = n / 2;
+    if (n > 0x7fffffffLL) throw InvalidArg("record longer than 2^31 samples");
+    constexpr int kCap = 1 << 16;  // candidate lines per antenna
+    cudaStream_t st = ctx->stream;
+    uint8_t* d_bits = (uint8_t*)ctx->buf("rfi.bits", A * row_bytes);
+    CK(cudaMemcpyAsync(d_bits, h_bits, A * row_bytes, cudaMemcpyHostToDevice, st));
+    ctx->h2d += A * row_bytes;
+    double* d_mean = (double*)ctx->buf("rfi.mean", A * sizeof(double));
+    CK(launch_antenna_means(d_bits, (int)A, row_bytes, d_mean, st));
+    double* d_z = (double*)ctx->buf("rfi.z", A * (size_t)n * sizeof(double));
+    void* d_X = ctx->buf("rfi.X", A * (size_t)(n / 2 + 1) * 16);
+    double* d_p = (double*)ctx->buf("rfi.p", A * (size_t)half * sizeof(double));
+    unsigned* d_hist = (unsigned*)ctx->buf("rfi.hist", A * 256 * sizeof(unsigned));
+    unsigned long long* d_prefix = (unsigned long long*)ctx->buf("rfi.prefix", A * 8);
+    unsigned long long* d_rank = (unsigned long long*)ctx->buf("rfi.rank", A * 8);
+    unsigned* d_count = (unsigned*)ctx->buf("rfi.count", A * sizeof(unsigned));
+    long long* d_bins = (long long*)ctx->buf("rfi.bins", A * kCap * sizeof(long long));
+    double* d_excess = (double*)ctx->buf("rfi.excess", A * kCap * sizeof(double));
+    unsigned long long* d_acf = (unsigned long long*)ctx->buf("rfi.acf", A * 9 * 8);
+    std::string why;
+    const cudaError_t e = rfi_scan_device(d_bits, (int)A, row_bytes, d_mean, d_z, d_X, d_p, d_hist, d_prefix, d_rank,
+                                          kCap, d_count, d_bins, d_excess, d_acf, st, &why);
+    if (!why.empty()) throw std::runtime_error(why);
+    CK(e);
+    std::vector<double> mean(A);
+    std::vector<unsigned> count(A);
+    std::vector<unsigned long long> acf(A * 9);
+    CK(cudaMemcpyAsync(mean.data(), d_mean, A * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(count.data(), d_count, A * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(acf.data(), d_acf, A * 9 * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (size_t a = 0; a < A; ++a)
+      if (count[a] > (unsigned)kCap) throw std::runtime_error("more than 65536 candidate RFI lines on one antenna");
+    const int lags[3] = {1, 3, 16};
+    for (size_t a = 0; a < A; ++a) {
+      tga_rfi_channel& ch = out[a];
+      std::memset(&ch, 0, sizeof ch);
+      ch.antenna = (int32_t)a;
+      const double m = mean[a];
+      // variance of z = s - m over the row (rfi.rs:148): ones (1-m)^2 + zeros (1+m)^2
+      const double ones = 0.5 * (m + 1.0) * (double)n;
+      const double var = (ones * (1.0 - m) * (1.0 - m) + ((double)n - ones) * (1.0 + m) * (1.0 + m)) / (double)n;
+      const double nan = std::nan("");
+      ch.acf_lag1 = ch.acf_lag3 = ch.acf_lag16 = ch.period_samples = nan;
+      if (var < 1e-9 || n < 8) {
+        ch.dead = var < 1e-9 ? 1 : 0;
+        continue;
+      }
+      double* acfs[3] = {&ch.acf_lag1, &ch.acf_lag3, &ch.acf_lag16};
+      for (int l = 0; l < 3; ++l) {
+        const double cnt = (double)(n - lags[l]);
+        const double diff = (double)acf[a * 9 + 3 * l], oh = (double)acf[a * 9 + 3 * l + 1],
+                     ot = (double)acf[a * 9 + 3 * l + 2];
+        const double sss = cnt - 2.0 * diff, sh = 2.0 * oh - cnt, stl = 2.0 * ot - cnt;
+        *acfs[l] = (sss - m * (sh + stl) + cnt * m * m) / cnt;
+      }
+      // candidate lines: strongest first, ties in bin order (a stable sort of
+      // the bin-ordered list, rfi.rs:126), then 10 kHz clustering
+      const unsigned c = count[a];
+      std::vector<long long> bins(c);
+      std::vector<double> ex(c);
+      if (c) {
+        CK(cudaMemcpy(bins.data(), d_bins + a * kCap, c * sizeof(long long), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(ex.data(), d_excess + a * kCap, c * sizeof(double), cudaMemcpyDeviceToHost));
+      }
+      std::vector<size_t> idx(c);
+      for (size_t i = 0; i < c; ++i) idx[i] = i;
+      std::sort(idx.begin(), idx.end(), [&](size_t x, size_t y) {
+        if (ex[x] != ex[y]) return ex[x] > ex[y];
+        return bins[x] < bins[y];
+      });
+      const double bin_hz = fs / (double)n;
+      for (size_t i : idx) {
+        const double f = (double)bins[i] * bin_hz;
+        bool far = true;
+        for (int k = 0; k < ch.n_lines; ++k)
+          if (!(std::abs(ch.lines[k].frequency - f) > 10000.0)) far = false;
+        if (!far) continue;
+        ch.lines[ch.n_lines].frequency = f;
+        ch.lines[ch.n_lines].excess_db = ex[i];
+        if (++ch.n_lines == 3) break;
+      }
+      if (ch.n_lines) ch.period_samples = fs / ch.lines[0].frequency;
+    }
+    return TGA_OK;
+  });
+}
+
 int tga_code_chips(int constellation, int prn, int8_t* out, size_t capacity, size_t* n) {
   try {
     std::vector<int8_t> s = resample_sequence(constellation, prn);

@@ -89,6 +89,17 @@ class FineResult(ctypes.Structure):
                 ("power_start", ctypes.c_double), ("iterations", ctypes.c_int32), ("converged", ctypes.c_int32)]
 
 
+class RfiLine(ctypes.Structure):
+    _fields_ = [("frequency", ctypes.c_double), ("excess_db", ctypes.c_double)]
+
+
+class RfiChannel(ctypes.Structure):
+    """tga_rfi_channel: RfiChannel of rfi.rs (NaN for None)."""
+    _fields_ = [("antenna", ctypes.c_int32), ("dead", ctypes.c_int32), ("acf_lag1", ctypes.c_double),
+                ("acf_lag3", ctypes.c_double), ("acf_lag16", ctypes.c_double), ("period_samples", ctypes.c_double),
+                ("n_lines", ctypes.c_int32), ("lines", RfiLine * 3)]
+
+
 _P = ctypes.c_void_p
 
 
@@ -125,6 +136,8 @@ def lib():
     L.tga_set_profiling.argtypes = [_P, i32]
     L.tga_set_variant.argtypes = [_P, i32, i32]
     L.tga_set_precision.argtypes = [_P, i32]
+    L.tga_rfi_scan.argtypes = [_P, _P, sz, sz, dbl, _P]
+    L.tga_rfi_json.argtypes = [_P, sz, _P]
     L.tga_fine_eval.argtypes = [_P, _P, sz, sz, dbl, _P, _P, dbl, _P, _P, _P]
     L.tga_fine_acquire.argtypes = [_P, _P, sz, sz, dbl, _P, sz, _P, _P, _P]
     L.tga_acquire_single_static.argtypes = [i32, _P, _P, sz, dbl, dbl, dbl, i32, sz, _P, _P]
@@ -382,6 +395,24 @@ class Context:
                                            len(tasks), ctypes.byref(opt), out, _ptr(phases)))
         res = [{k: getattr(r, k) for k, _ in FineResult._fields_} for r in out]
         return res, phases
+
+    def rfi_scan(self, packed_bits, sampling_freq, as_json=False):
+        """rfi::run on packed rows: list of dicts shaped like rfi.rs's RfiChannel
+        (None where the reference has None), or the --rfi JSON text."""
+        bits = np.ascontiguousarray(packed_bits, dtype=np.uint8)
+        out = (RfiChannel * bits.shape[0])()
+        self._check(lib().tga_rfi_scan(self._h, _ptr(bits), bits.shape[0], bits.shape[1], float(sampling_freq), out))
+        if as_json:
+            p = ctypes.c_char_p()
+            self._check(lib().tga_rfi_json(out, len(out), ctypes.byref(p)))
+            text = ctypes.string_at(p).decode()
+            lib().tga_free(p)
+            return text
+        opt = lambda v: None if np.isnan(v) else float(v)
+        return [dict(antenna=c.antenna, dead=bool(c.dead), acf_lag1=opt(c.acf_lag1), acf_lag3=opt(c.acf_lag3),
+                     acf_lag16=opt(c.acf_lag16), period_samples=opt(c.period_samples),
+                     lines=[dict(frequency=c.lines[k].frequency, excess_db=c.lines[k].excess_db)
+                            for k in range(c.n_lines)]) for c in out]
 
     def correlation_matrix(self, packed_bits):
         bits = np.ascontiguousarray(packed_bits, dtype=np.uint8)
