@@ -299,6 +299,17 @@ int tga_code_chips(int constellation, int prn, int8_t* out, size_t capacity, siz
 int tga_code_resampled(int constellation, int prn, double samples_per_code,
                        size_t num_samples, float* out);
 
+/* ---- ACR table Monte Carlo (examples/gen_acr_tables.rs) ---------------------------
+ * Regenerates a C/N0 lookup table for one constellation: for every C/N0 from
+ * cn0_lo to cn0_hi in cn0_step, `trials` two-code-period signals of `prn` at
+ * fs on a 100 kHz carrier (random code delay and carrier phase, unit noise,
+ * the reference generator's xorshift64 streams and seeds), one-bit
+ * quantised on the GPU and searched with the batched acquisition (one bin at
+ * 100 kHz); r_A = sum peak^2 / sum second^2, forced strictly increasing like
+ * the reference.  out receives (r_A, C/N0) pairs; cap counts pairs. */
+int tga_acr_table(tga_ctx* ctx, int constellation, int prn, double fs, double cn0_lo, double cn0_hi,
+                  double cn0_step, int trials, double* out, size_t cap, size_t* n_out);
+
 /* ---- narrowband RFI scan (--rfi) ----------------------------------------------
  * rfi::analyze_channel (rfi.rs:145-168) for every antenna row: spectral lines
  * at least 15 dB above the median bin power of the whole record (f64 FFT),

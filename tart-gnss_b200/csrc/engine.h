@@ -146,6 +146,11 @@ cudaError_t rfi_scan_device(const uint8_t* d_bits, int n_ant, size_t row_bytes, 
                             unsigned long long* d_rank, int cap, unsigned* d_count, long long* d_bins,
                             double* d_excess, unsigned long long* d_acf, cudaStream_t st, std::string* why);
 
+// ACR Monte Carlo synthesizer (examples/gen_acr_tables.rs): n_points x
+// n_trials rows of 2 * period one-bit samples, packed MSB-first
+cudaError_t launch_acr_synth(const int8_t* d_code, int period, int n_trials, double cn0_lo, double cn0_step,
+                             int n_points, double fs, double f_carrier, uint8_t* d_bits, cudaStream_t st);
+
 int kernel_launch_count_reset();
 void kernel_launch_add(int n);
 int kernel_launch_count();

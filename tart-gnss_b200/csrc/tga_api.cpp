@@ -1453,6 +1453,59 @@ int tga_rfi_scan(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant, size_t row_b
   });
 }
 
+// ---------------------------------------------------------------------------
+// ACR table Monte Carlo (tga_acr_table), examples/gen_acr_tables.rs:134-173
+// ---------------------------------------------------------------------------
+int tga_acr_table(tga_ctx* ctx, int constellation, int prn, double fs, double cn0_lo, double cn0_hi,
+                  double cn0_step, int trials, double* out, size_t cap, size_t* n_out) {
+  return guarded(ctx, [&] {
+    if (constellation < 0 || constellation >= N_CONST) throw InvalidArg("bad constellation");
+    validate_prn(constellation, prn);
+    if (trials < 1 || !(cn0_step > 0) || !(cn0_hi >= cn0_lo) || !(fs > 0) || !n_out)
+      throw InvalidArg("bad arguments");
+    const int points = (int)std::floor((cn0_hi - cn0_lo) / cn0_step + 1e-9) + 1;
+    *n_out = (size_t)points;
+    if (!out) return TGA_OK;
+    if (cap < (size_t)points) return TGA_ERR_CAPACITY;
+    const size_t period = period_samples(constellation, fs);
+    if ((2 * period) % 8) throw InvalidArg("two code periods are not a whole number of bytes");
+    const size_t row_bytes = 2 * period / 8;
+    const std::vector<int8_t> code = resampled_code(constellation, prn, (double)period, 2 * period);
+    int8_t* d_code = (int8_t*)ctx->buf("acr.code", code.size());
+    CK(cudaMemcpyAsync(d_code, code.data(), code.size(), cudaMemcpyHostToDevice, ctx->stream));
+    uint8_t* d_bits = (uint8_t*)ctx->buf("acr.bits", (size_t)points * trials * row_bytes);
+    CK(launch_acr_synth(d_code, (int)period, trials, cn0_lo, cn0_step, points, fs, 100e3, d_bits, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));  // code is a host temporary
+    int32_t prns[1] = {prn};
+    tga_all_options o;
+    std::memset(&o, 0, sizeof o);
+    o.constellation_mask = 1u << constellation;
+    o.prn_filter = prns;
+    o.n_prn_filter = 1;
+    o.center_freq = 100e3;  // gen_acr_tables.rs:38 F_CARRIER, search band 0: one bin
+    o.search_band = 0.0;
+    std::vector<tga_cell> cells((size_t)trials);
+    double prev = 0.0;
+    for (int j = 0; j < points; ++j) {
+      size_t nc = 0;
+      const int rc = tga_acquire_all_device(ctx, d_bits + (size_t)j * trials * row_bytes, (size_t)trials, row_bytes,
+                                            fs, &o, cells.data(), cells.size(), &nc);
+      if (rc != TGA_OK) return rc;
+      double p2 = 0, s2 = 0;
+      for (size_t k = 0; k < nc; ++k) {
+        p2 += cells[k].signal_strength * cells[k].signal_strength;
+        s2 += cells[k].second_peak * cells[k].second_peak;
+      }
+      double r_a = p2 / s2;
+      if (r_a <= prev) r_a = prev + 0.001;  // strictly increasing (gen_acr_tables.rs:148-152)
+      prev = r_a;
+      out[2 * j] = r_a;
+      out[2 * j + 1] = cn0_lo + (double)j * cn0_step;
+    }
+    return TGA_OK;
+  });
+}
+
 int tga_code_chips(int constellation, int prn, int8_t* out, size_t capacity, size_t* n) {
   try {
     std::vector<int8_t> s = resample_sequence(constellation, prn);

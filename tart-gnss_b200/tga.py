@@ -137,6 +137,7 @@ def lib():
     L.tga_set_variant.argtypes = [_P, i32, i32]
     L.tga_set_precision.argtypes = [_P, i32]
     L.tga_rfi_scan.argtypes = [_P, _P, sz, sz, dbl, _P]
+    L.tga_acr_table.argtypes = [_P, i32, i32, dbl, dbl, dbl, dbl, i32, _P, sz, _P]
     L.tga_rfi_json.argtypes = [_P, sz, _P]
     L.tga_fine_eval.argtypes = [_P, _P, sz, sz, dbl, _P, _P, dbl, _P, _P, _P]
     L.tga_fine_acquire.argtypes = [_P, _P, sz, sz, dbl, _P, sz, _P, _P, _P]
@@ -395,6 +396,18 @@ class Context:
                                            len(tasks), ctypes.byref(opt), out, _ptr(phases)))
         res = [{k: getattr(r, k) for k, _ in FineResult._fields_} for r in out]
         return res, phases
+
+    def acr_table(self, constellation, prn=1, sampling_freq=16.368e6, cn0_lo=33.0, cn0_hi=62.0, cn0_step=0.5,
+                  trials=100):
+        """gen_acr_tables Monte Carlo on the GPU: [n, 2] array of (r_A, C/N0)."""
+        n = ctypes.c_size_t()
+        self._check(lib().tga_acr_table(self._h, constellation, prn, float(sampling_freq), float(cn0_lo),
+                                        float(cn0_hi), float(cn0_step), int(trials), None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, 2))
+        self._check(lib().tga_acr_table(self._h, constellation, prn, float(sampling_freq), float(cn0_lo),
+                                        float(cn0_hi), float(cn0_step), int(trials), _ptr(out), n.value,
+                                        ctypes.byref(n)))
+        return out
 
     def rfi_scan(self, packed_bits, sampling_freq, as_json=False):
         """rfi::run on packed rows: list of dicts shaped like rfi.rs's RfiChannel
