@@ -299,6 +299,44 @@ int tga_code_chips(int constellation, int prn, int8_t* out, size_t capacity, siz
 int tga_code_resampled(int constellation, int prn, double samples_per_code,
                        size_t num_samples, float* out);
 
+/* ---- non-coherent search (weak-signal mode) ------------------------------------
+ * An extension of the drop-in search (no reference counterpart; the crate
+ * searches one two-period window): `blocks` consecutive coherent blocks of
+ * `coherent_periods` code periods starting at sample `start`; each block is
+ * wiped off with the reference's phase convention (correlate.rs:110-115),
+ * folded into one period and correlated cyclically with the code; |y|^2 is
+ * summed over the blocks before the peak search.  Doppler bins are centred:
+ * center_freq + (i - (n_bins - 1) / 2) * bin_step_hz.  Ties: the later lag
+ * within a bin, the later bin across bins; second peak at a circular
+ * distance of more than ceil(fs / 1.023 MHz) samples from the peak.  Needs an
+ * integer number of samples per chip (TGA_ERR_UNSUPPORTED otherwise). */
+typedef struct tga_nc_options {
+  int32_t constellation;
+  const int32_t* prn_filter;   /* NULL = every PRN of the constellation     */
+  size_t n_prn_filter;
+  const int32_t* ant_filter;   /* NULL = every antenna                      */
+  size_t n_ant_filter;
+  double center_freq;          /* Hz                                        */
+  double bin_step_hz;
+  int32_t n_bins;
+  int32_t coherent_periods;
+  int32_t blocks;
+  int64_t start;               /* first sample                              */
+} tga_nc_options;
+typedef struct tga_nc_cell {
+  int32_t prn;
+  int32_t antenna;
+  int32_t best_freq_idx;
+  int32_t reserved;
+  int64_t best_codephase;      /* samples, [0, period)                     */
+  double power;                /* sum over blocks of (|r| sqrt(N))^2, N = samples per block */
+  double second_power;
+  double frequency;            /* bin frequency - center_freq (Hz)          */
+} tga_nc_cell;
+/* Cells in (PRN, antenna) order; cap counts cells. */
+int tga_search_noncoherent(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, size_t row_bytes, double fs,
+                           const tga_nc_options* opt, tga_nc_cell* out, size_t cap, size_t* n_out);
+
 /* ---- ACR table Monte Carlo (examples/gen_acr_tables.rs) ---------------------------
  * Regenerates a C/N0 lookup table for one constellation: for every C/N0 from
  * cn0_lo to cn0_hi in cn0_step, `trials` two-code-period signals of `prn` at

@@ -445,6 +445,16 @@ cudaError_t launch_forward_z(const PolyClass& pc, int n_ab, float2* d_z, int num
   return dispatch_pfa<FWD_Z>(pc.M, p, p.n_seq, num_sms, st);
 }
 
+cudaError_t launch_forward_seqs(const PolyClass& pc, long long n_seq, float2* d_z, int num_sms, cudaStream_t st) {
+  if (n_seq > 0x7fffffffLL) return cudaErrorInvalidValue;
+  PfaParams p = {};
+  p.z = d_z;
+  p.n_seq = (int)n_seq;
+  p.S = pc.S;
+  p.P = pc.P;
+  return dispatch_pfa<FWD_Z>(pc.M, p, p.n_seq, num_sms, st);
+}
+
 cudaError_t launch_code_spectra(const PolyClass& pc, const int8_t* d_chips, int n_prn, float2* d_D,
                                 int num_sms, cudaStream_t st) {
   PfaParams p = {};

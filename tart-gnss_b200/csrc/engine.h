@@ -76,6 +76,8 @@ cudaError_t launch_antenna_means(const uint8_t* d_bits, int n_rows, size_t row_b
 cudaError_t launch_frontend(const SampleSource& src, const SearchDims& dims, const PolyClass& pc,
                             float2* d_z, cudaStream_t st);
 cudaError_t launch_forward_z(const PolyClass& pc, int n_ab, float2* d_z, int num_sms, cudaStream_t st);
+// forward transform of n_seq Lc-point sequences in place (any count)
+cudaError_t launch_forward_seqs(const PolyClass& pc, long long n_seq, float2* d_z, int num_sms, cudaStream_t st);
 cudaError_t launch_code_spectra(const PolyClass& pc, const int8_t* d_chips, int n_prn, float2* d_D,
                                 int num_sms, cudaStream_t st);
 cudaError_t launch_correlate(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
@@ -150,6 +152,16 @@ cudaError_t rfi_scan_device(const uint8_t* d_bits, int n_ant, size_t row_bytes, 
 // n_trials rows of 2 * period one-bit samples, packed MSB-first
 cudaError_t launch_acr_synth(const int8_t* d_code, int period, int n_trials, double cn0_lo, double cn0_step,
                              int n_points, double fs, double f_carrier, uint8_t* d_bits, cudaStream_t st);
+
+// non-coherent search: K-period cyclic blocks, |y|^2 summed over B blocks
+cudaError_t launch_nc_frontend(const SampleSource& src, const SearchDims& dims, const PolyClass& pc, int K, int B,
+                               long long start, float2* d_z, cudaStream_t st);
+cudaError_t launch_nc_correlate(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
+                                const float2* d_D, unsigned long long* d_keys, int num_sms, cudaStream_t st);
+cudaError_t launch_nc_reduce(const SearchDims& dims, const unsigned long long* d_keys, BestRow* d_best,
+                             cudaStream_t st);
+cudaError_t launch_nc_second(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
+                             const float2* d_D, BestRow* d_best, int chip_width, int num_sms, cudaStream_t st);
 
 int kernel_launch_count_reset();
 void kernel_launch_add(int n);

@@ -1,0 +1,352 @@
+// Non-coherent search: coherent blocks of K code periods, |y|^2 summed over
+// B blocks before the peak search (the weak-signal mode of the engine).
+//
+// The drop-in search (correlate.rs:91-183) correlates one two-period window.
+// This mode extends it the usual way for weak signals: block b covers
+// samples [start + b K P, start + (b+1) K P); its K periods are wiped off with
+// the reference's phase convention ((p * f) as f32, correlate.rs:110-115),
+// folded into one period (a cyclic correlation with the periodic code), split
+// into the S polyphase residues and transformed like the drop-in Z; the
+// correlator multiplies by the code spectrum, inverts, and adds |y|^2 of
+// every block into a shared-memory accumulator before it takes the maximum
+// (last maximum in lag order) or, for the selected bin, the second peak at a
+// circular distance of more than one chip.  Doppler bins are a centred grid
+// center + (i - (nb - 1) / 2) step; the last maximum over bins wins.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "dft.cuh"
+#include "engine.h"
+#include "pfa_common.cuh"
+
+namespace tga {
+
+namespace {
+
+struct NcFrontParams {
+  SampleSource src;
+  const double* fc;
+  int nb, P, S, Lc, K, B;
+  long long start;
+  float pulse[kMaxPulse];
+  float2* z;
+};
+
+constexpr int kNcJ = 64;  // chips per CTA
+
+__device__ __forceinline__ float2 wipe_bits(const NcFrontParams& p, int row, long long n, double f) {
+  const uint8_t byte = __ldg(p.src.bits + (size_t)row * p.src.row_bytes + (n >> 3));
+  const double v = ((byte >> (7 - (int)(n & 7))) & 1) ? 1.0 : -1.0;
+  const float s = (float)(v - __ldg(p.src.mean + row));
+  const float ph = __double2float_rn((p.src.pc * (double)n) * f);
+  float sn, cs;
+  sincosf(ph, &sn, &cs);
+  return make_float2(cs * s, sn * s);
+}
+
+__global__ void __launch_bounds__(256) nc_frontend_kernel(NcFrontParams p) {
+  extern __shared__ float2 fsm[];
+  const int S = p.S, P = p.P, Lc = p.Lc;
+  const int ab = blockIdx.y / p.B, blk = blockIdx.y - ab * p.B;
+  const int ant_slot = ab / p.nb, bin = ab - ant_slot * p.nb;
+  const int row = p.src.ant[ant_slot];
+  const double f = p.fc[bin];
+  const long long n0 = p.start + (long long)blk * p.K * P;
+  const int j0 = blockIdx.x * kNcJ;
+  const int nj = min(kNcJ, Lc - j0);
+  const int cnt = nj * S + S - 1;
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+    int m = S * j0 + i;
+    if (m >= P) m -= P;  // the folded block is P-periodic
+    float2 x = make_float2(0.f, 0.f);
+    for (int k = 0; k < p.K; ++k) x = cadd(x, wipe_bits(p, row, n0 + (long long)k * P + m, f));
+    fsm[i + i / S] = x;
+  }
+  __syncthreads();
+  const size_t seq0 = ((size_t)ab * p.B + blk) * S;
+  for (int o = threadIdx.x; o < S * nj; o += blockDim.x) {
+    const int rho = o / nj, jj = o - rho * nj;
+    float2 z = make_float2(0.f, 0.f);
+    const int base = jj * S + rho;
+    for (int s = 0; s < S; ++s) {
+      const int i = base + s;
+      const float w = p.pulse[s];
+      z.x = fmaf(w, fsm[i + i / S].x, z.x);
+      z.y = fmaf(w, fsm[i + i / S].y, z.y);
+    }
+    p.z[(seq0 + rho) * Lc + j0 + jj] = z;
+  }
+}
+
+enum NcMode { NC_PEAK = 0, NC_SECOND = 1 };
+
+struct NcParams {
+  const float2* z;  // [n_ab][B][S][Lc], digit layout
+  const float2* D;  // [n_prn][2][Lc]; the cyclic spectrum (index 0) is used
+  int n_items, n_prn, S, P, B, chip_width;
+  unsigned long long* keys;  // NC_PEAK: [n_ab][n_prn]
+  BestRow* best;             // NC_SECOND: [n_ant][n_prn]
+};
+
+template <int M, int BC, int NT, int MODE>
+__global__ void __launch_bounds__(NT, 1) nc_correlate_kernel(NcParams p) {
+  using G = Geo<M>;
+  constexpr int COLS = G::COLS, LC = G::LC, NC = G::NC;
+  extern __shared__ float2 buf[];
+  float* acc = reinterpret_cast<float*>(buf + BC * LC);
+  __shared__ unsigned long long s_key;
+  __shared__ unsigned int s_p2;
+  const int tid = threadIdx.x, S = p.S;
+  const int groups = (S + BC - 1) / BC;
+  for (int w = blockIdx.x; w < p.n_items; w += gridDim.x) {
+    int ab, prn, tau_star = 0;
+    if (MODE == NC_PEAK) {
+      ab = w / p.n_prn;
+      prn = w - ab * p.n_prn;
+    } else {
+      const BestRow b = p.best[w];
+      ab = b.ab;
+      prn = w % p.n_prn;
+      tau_star = b.tau;
+    }
+    if (tid == 0) {
+      s_key = 0ull;
+      s_p2 = 0u;
+    }
+    unsigned long long kbest = 0ull;
+    float pbest = 0.f;
+    for (int g = 0; g < groups; ++g) {
+      auto seq_of = [&](int s) -> int {
+        const int rho = g * BC + s;
+        return rho < S ? rho : -1;
+      };
+      for (int i = tid; i < BC * LC; i += NT) acc[i] = 0.f;
+      __syncthreads();
+      auto accumulate = [&](int s, int a, int b, int c, float2 v) {
+        acc[s * LC + G::offset(a, b, c)] += fmaf(v.x, v.x, v.y * v.y);
+      };
+      for (int blk = 0; blk < p.B; ++blk) {
+        // stage 1: products and DFT-31 over digit a
+        for (int u = tid; u < BC * COLS; u += NT) {
+          const int s = u / COLS, col = u - s * COLS;
+          const int q = seq_of(s);
+          if (q < 0) continue;
+          const float2* zs = p.z + (((size_t)ab * p.B + blk) * S + q) * LC + col;
+          const float2* ds = p.D + (size_t)prn * 2 * LC + col;
+          float2 x[31];
+#pragma unroll
+          for (int a = 0; a < 31; ++a) x[a] = cmul(__ldcg(zs + a * COLS), __ldg(ds + a * COLS));
+          float2* dst = buf + s * LC + col;
+          dft_odd<31, true>(x, [&](int ta, float2 v) { dst[ta * COLS] = v; });
+        }
+        __syncthreads();
+        // stage 2: DFT-33 over digit b
+        for (int u = tid; u < BC * 31 * NC; u += NT) {
+          const int s = u / (31 * NC), r = u - s * 31 * NC;
+          const int a = r / NC, c = r - a * NC;
+          if (seq_of(s) < 0) continue;
+          float2* base = buf + s * LC + a * COLS + c * 33;
+          float2 x[33];
+#pragma unroll
+          for (int b = 0; b < 33; ++b) x[b] = base[b];
+          if constexpr (NC == 1) {
+            dft33<true>(x, [&](int tb, float2 v) { accumulate(s, a, tb, 0, v); });
+          } else {
+            dft33<true>(x, [&](int tb, float2 v) { base[tb] = v; });
+          }
+        }
+        // stage 3: DFT-M over digit c
+        if constexpr (NC > 1) {
+          __syncthreads();
+          for (int u = tid; u < BC * 1023; u += NT) {
+            const int s = u / 1023, gi = u - s * 1023;
+            const int a = gi / 33, b = gi - a * 33;
+            if (seq_of(s) < 0) continue;
+            const float2* base = buf + s * LC + a * COLS + b;
+            float2 x[NC];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) x[c] = base[c * 33];
+            dft_small<NC, true>(x, [&](int tc, float2 v) { accumulate(s, a, b, tc, v); });
+          }
+        }
+        __syncthreads();
+      }
+      // the accumulated powers of this group's residues
+      for (int i = tid; i < BC * LC; i += NT) {
+        const int s = i / LC, off = i - s * LC;
+        const int q = seq_of(s);
+        if (q < 0) continue;
+        const int a = off / COLS, rem = off - a * COLS;
+        const int c = rem / 33, b = rem - c * 33;
+        const int lag = q + S * G::natural(a, b, c);
+        const float pw = acc[i];
+        if (MODE == NC_PEAK) {
+          const unsigned long long k = ((unsigned long long)__float_as_uint(pw) << 32) | (unsigned)lag;
+          kbest = k > kbest ? k : kbest;  // ties: the later lag (Iterator::max_by)
+        } else {
+          int d = lag - tau_star;
+          d = d < 0 ? -d : d;
+          if (min(d, p.P - d) > p.chip_width) pbest = fmaxf(pbest, pw);
+        }
+      }
+      __syncthreads();
+    }
+    if (MODE == NC_PEAK) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, kbest, o);
+        kbest = other > kbest ? other : kbest;
+      }
+      if ((tid & 31) == 0) atomicMax(&s_key, kbest);
+      __syncthreads();
+      if (tid == 0) p.keys[w] = s_key;
+    } else {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) pbest = fmaxf(pbest, __shfl_xor_sync(0xffffffffu, pbest, o));
+      if ((tid & 31) == 0) atomicMax(&s_p2, __float_as_uint(pbest));
+      __syncthreads();
+      if (tid == 0) p.best[w].p2 = __uint_as_float(s_p2);
+    }
+    __syncthreads();
+  }
+}
+
+template <int M>
+struct NcCfg;
+template <>
+struct NcCfg<1> {
+  static constexpr int BC = 8, NT = 288;
+};
+template <>
+struct NcCfg<4> {
+  static constexpr int BC = 2, NT = 288;
+};
+template <>
+struct NcCfg<10> {
+  static constexpr int BC = 1, NT = 352;
+};
+
+template <int M, int MODE>
+cudaError_t run_nc(const NcParams& p, int num_sms, cudaStream_t st) {
+  using C = NcCfg<M>;
+  constexpr int LC = Geo<M>::LC;
+  const size_t smem = (size_t)C::BC * LC * (sizeof(float2) + sizeof(float));
+  auto kern = nc_correlate_kernel<M, C::BC, C::NT, MODE>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, smem);
+  if (per_sm < 1) per_sm = 1;
+  int grid = num_sms * per_sm;
+  if (grid > p.n_items) grid = p.n_items;
+  if (grid < 1) return cudaSuccess;
+  kern<<<grid, C::NT, smem, st>>>(p);
+  kernel_launch_add(1);
+  return cudaGetLastError();
+}
+
+template <int MODE>
+cudaError_t dispatch_nc(int M, const NcParams& p, int num_sms, cudaStream_t st) {
+  switch (M) {
+    case 1: return run_nc<1, MODE>(p, num_sms, st);
+    case 4: return run_nc<4, MODE>(p, num_sms, st);
+    case 10: return run_nc<10, MODE>(p, num_sms, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// per (antenna, PRN): the last bin with the largest accumulated peak
+__global__ void nc_reduce_kernel(int n_ant, int nb, int n_prn, const unsigned long long* __restrict__ keys,
+                                 BestRow* __restrict__ best) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_ant * n_prn) return;
+  const int ant = i / n_prn, prn = i - ant * n_prn;
+  float pb = -1.f;
+  unsigned long long kb = 0ull;
+  int bb = 0;
+  for (int bin = 0; bin < nb; ++bin) {
+    const unsigned long long k = keys[((size_t)ant * nb + bin) * n_prn + prn];
+    const float pr = __uint_as_float((unsigned)(k >> 32));
+    if (bin == 0 || pr >= pb) {
+      pb = pr;
+      kb = k;
+      bb = bin;
+    }
+  }
+  BestRow r;
+  r.ab = ant * nb + bb;
+  r.hyp = 0;
+  r.tau = (int)(unsigned)(kb & 0xffffffffull);
+  r.p = pb;
+  r.p2 = 0.f;
+  best[i] = r;
+}
+
+}  // namespace
+
+cudaError_t launch_nc_frontend(const SampleSource& src, const SearchDims& dims, const PolyClass& pc, int K, int B,
+                               long long start, float2* d_z, cudaStream_t st) {
+  NcFrontParams p;
+  p.src = src;
+  p.fc = dims.fc;
+  p.nb = dims.nb;
+  p.P = pc.P;
+  p.S = pc.S;
+  p.Lc = pc.Lc;
+  p.K = K;
+  p.B = B;
+  p.start = start;
+  for (int i = 0; i < kMaxPulse; ++i) p.pulse[i] = pc.pulse[i];
+  p.z = d_z;
+  const int span = kNcJ * pc.S + pc.S;
+  const size_t smem = (size_t)(span + span / pc.S + 1) * sizeof(float2);
+  const long long gy = (long long)dims.n_ant * dims.nb * B;
+  if (gy > 65535) return cudaErrorInvalidValue;
+  dim3 grid((pc.Lc + kNcJ - 1) / kNcJ, (unsigned)gy);
+  cudaError_t e = cudaFuncSetAttribute(nc_frontend_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  nc_frontend_kernel<<<grid, 256, smem, st>>>(p);
+  kernel_launch_add(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_nc_correlate(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
+                                const float2* d_D, unsigned long long* d_keys, int num_sms, cudaStream_t st) {
+  NcParams p = {};
+  p.z = d_z;
+  p.D = d_D;
+  p.keys = d_keys;
+  p.n_prn = dims.n_prn;
+  p.S = pc.S;
+  p.P = pc.P;
+  p.B = B;
+  p.n_items = dims.n_ant * dims.nb * dims.n_prn;
+  return dispatch_nc<NC_PEAK>(pc.M, p, num_sms, st);
+}
+
+cudaError_t launch_nc_reduce(const SearchDims& dims, const unsigned long long* d_keys, BestRow* d_best,
+                             cudaStream_t st) {
+  const int n = dims.n_ant * dims.n_prn;
+  if (n <= 0) return cudaSuccess;
+  nc_reduce_kernel<<<(n + 127) / 128, 128, 0, st>>>(dims.n_ant, dims.nb, dims.n_prn, d_keys, d_best);
+  kernel_launch_add(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_nc_second(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
+                             const float2* d_D, BestRow* d_best, int chip_width, int num_sms, cudaStream_t st) {
+  NcParams p = {};
+  p.z = d_z;
+  p.D = d_D;
+  p.best = d_best;
+  p.n_prn = dims.n_prn;
+  p.S = pc.S;
+  p.P = pc.P;
+  p.B = B;
+  p.chip_width = chip_width;
+  p.n_items = dims.n_ant * dims.n_prn;
+  return dispatch_nc<NC_SECOND>(pc.M, p, num_sms, st);
+}
+
+}  // namespace tga

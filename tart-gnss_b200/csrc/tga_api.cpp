@@ -1454,6 +1454,127 @@ int tga_rfi_scan(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant, size_t row_b
 }
 
 // ---------------------------------------------------------------------------
+// non-coherent search (tga_search_noncoherent)
+// ---------------------------------------------------------------------------
+int tga_search_noncoherent(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant_total, size_t row_bytes, double fs,
+                           const tga_nc_options* opt, tga_nc_cell* out, size_t cap, size_t* n_out) {
+  return guarded(ctx, [&] {
+    if (!h_bits || !opt || !n_out || n_ant_total == 0 || row_bytes == 0 || !(fs > 0)) throw InvalidArg("bad arguments");
+    const int c = opt->constellation;
+    if (c < 0 || c >= N_CONST) throw InvalidArg("bad constellation");
+    if (opt->n_bins < 1 || opt->coherent_periods < 1 || opt->blocks < 1 || opt->start < 0 ||
+        !(opt->bin_step_hz >= 0))
+      throw InvalidArg("bad search geometry");
+    std::vector<int32_t> ants, prn_list;
+    if (opt->ant_filter) {
+      for (size_t i = 0; i < opt->n_ant_filter; ++i) {
+        if (opt->ant_filter[i] < 0 || (size_t)opt->ant_filter[i] >= n_ant_total)
+          throw InvalidArg("antenna index out of range");
+        ants.push_back(opt->ant_filter[i]);
+      }
+    } else {
+      for (size_t i = 0; i < n_ant_total; ++i) ants.push_back((int32_t)i);
+    }
+    const ConstellationInfo& ci = info(c);
+    if (opt->prn_filter) {
+      for (size_t i = 0; i < opt->n_prn_filter; ++i) {
+        validate_prn(c, opt->prn_filter[i]);
+        prn_list.push_back(opt->prn_filter[i]);
+      }
+    } else {
+      for (int q = ci.prn_first; q <= ci.prn_last; ++q) prn_list.push_back(q);
+    }
+    const size_t n_cells = ants.size() * prn_list.size();
+    *n_out = n_cells;
+    if (!out) return TGA_OK;
+    if (cap < n_cells) return TGA_ERR_CAPACITY;
+    const size_t P = period_samples(c, fs);
+    const long long need = opt->start + (long long)opt->blocks * opt->coherent_periods * (long long)P;
+    if (need > (long long)row_bytes * 8) throw InvalidArg("the blocks run past the end of the recording");
+    PolyClass pc;
+    std::vector<int> prns_i(prn_list.begin(), prn_list.end());
+    if (!poly_class_for(ctx, c, (double)P, P, 2 * P, prns_i, &pc)) {
+      ctx->err = "non-coherent search needs an integer number of samples per chip";
+      return TGA_ERR_UNSUPPORTED;
+    }
+    begin_call(ctx);
+    const int n_ant = (int)ants.size(), n_prn = (int)prn_list.size(), nb = opt->n_bins, B = opt->blocks;
+    cudaStream_t st = ctx->stream;
+    uint8_t* d_bits = (uint8_t*)ctx->buf("nc.bits", n_ant_total * row_bytes);
+    CK(cudaMemcpyAsync(d_bits, h_bits, n_ant_total * row_bytes, cudaMemcpyHostToDevice, st));
+    ctx->h2d += n_ant_total * row_bytes;
+    double* d_mean = (double*)ctx->buf("nc.mean", n_ant_total * sizeof(double));
+    CK(launch_antenna_means(d_bits, (int)n_ant_total, row_bytes, d_mean, st));
+    int32_t* d_ant = (int32_t*)ctx->buf("nc.ant", ants.size() * sizeof(int32_t));
+    CK(cudaMemcpyAsync(d_ant, ants.data(), ants.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    std::vector<double> fc(nb);
+    for (int i = 0; i < nb; ++i) fc[i] = opt->center_freq + (double)(i - (nb - 1) / 2) * opt->bin_step_hz;
+    double* d_fc = (double*)ctx->buf("nc.fc", fc.size() * sizeof(double));
+    CK(cudaMemcpyAsync(d_fc, fc.data(), fc.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    std::vector<int8_t> chips((size_t)n_prn * pc.Lc);
+    for (int i = 0; i < n_prn; ++i) {
+      const std::vector<int8_t>& ch = cached_chips(ctx, c, prn_list[i]);
+      std::memcpy(&chips[(size_t)i * pc.Lc], ch.data(), (size_t)pc.Lc);
+    }
+    int8_t* d_chips = (int8_t*)ctx->buf("nc.chips", chips.size());
+    CK(cudaMemcpyAsync(d_chips, chips.data(), chips.size(), cudaMemcpyHostToDevice, st));
+    SampleSource src;
+    src.bits = d_bits;
+    src.row_bytes = row_bytes;
+    src.mean = d_mean;
+    src.ant = d_ant;
+    src.n_ant = n_ant;
+    src.pc = 6.283185307179586 / fs;
+    SearchDims dims;
+    dims.n_ant = n_ant;
+    dims.nb = nb;
+    dims.n_prn = n_prn;
+    dims.fc = d_fc;
+    const long long n_seq = (long long)n_ant * nb * B * pc.S;
+    float2* d_z = (float2*)ctx->buf("nc.z", (size_t)n_seq * pc.Lc * sizeof(float2));
+    float2* d_D = (float2*)ctx->buf("nc.D", (size_t)n_prn * 2 * pc.Lc * sizeof(float2));
+    unsigned long long* d_keys =
+        (unsigned long long*)ctx->buf("nc.keys", (size_t)n_ant * nb * n_prn * sizeof(unsigned long long));
+    BestRow* d_best = (BestRow*)ctx->buf("nc.best", (size_t)n_ant * n_prn * sizeof(BestRow));
+    const double tf = transform_flops_per_point(pc.M);
+    timed(ctx, "nc_code_spectra", (double)n_prn * 2 * pc.Lc * tf,
+          [&] { return launch_code_spectra(pc, d_chips, n_prn, d_D, ctx->num_sms, st); });
+    timed(ctx, "nc_frontend", 0.0,
+          [&] { return launch_nc_frontend(src, dims, pc, opt->coherent_periods, B, opt->start, d_z, st); });
+    timed(ctx, "nc_forward_z", (double)n_seq * pc.Lc * tf,
+          [&] { return launch_forward_seqs(pc, n_seq, d_z, ctx->num_sms, st); });
+    timed(ctx, "nc_correlate", (double)n_ant * nb * n_prn * B * pc.P * (tf + 9.0),
+          [&] { return launch_nc_correlate(pc, dims, B, d_z, d_D, d_keys, ctx->num_sms, st); });
+    timed(ctx, "nc_reduce", 0.0, [&] { return launch_nc_reduce(dims, d_keys, d_best, st); });
+    timed(ctx, "nc_second", (double)n_ant * n_prn * B * pc.P * (tf + 9.0), [&] {
+      return launch_nc_second(pc, dims, B, d_z, d_D, d_best, chip_width_of(fs), ctx->num_sms, st);
+    });
+    std::vector<BestRow> best((size_t)n_ant * n_prn);
+    CK(cudaMemcpyAsync(best.data(), d_best, best.size() * sizeof(BestRow), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    collect_times(ctx);
+    ctx->last_cells = (double)n_ant * nb * n_prn * (double)P * B;
+    // |y| of the polyphase correlator is Lc |r|; report (|r| sqrt(N))^2 per block
+    const double scale = (double)opt->coherent_periods * (double)P / ((double)pc.Lc * (double)pc.Lc);
+    size_t k = 0;
+    for (int q = 0; q < n_prn; ++q)
+      for (int a = 0; a < n_ant; ++a, ++k) {
+        const BestRow& r = best[(size_t)a * n_prn + q];
+        tga_nc_cell& o = out[k];
+        std::memset(&o, 0, sizeof o);
+        o.prn = prn_list[q];
+        o.antenna = ants[a];
+        o.best_freq_idx = r.ab - a * nb;
+        o.best_codephase = r.tau;
+        o.power = (double)r.p * scale;
+        o.second_power = (double)r.p2 * scale;
+        o.frequency = fc[o.best_freq_idx] - opt->center_freq;
+      }
+    return TGA_OK;
+  });
+}
+
+// ---------------------------------------------------------------------------
 // ACR table Monte Carlo (tga_acr_table), examples/gen_acr_tables.rs:134-173
 // ---------------------------------------------------------------------------
 int tga_acr_table(tga_ctx* ctx, int constellation, int prn, double fs, double cn0_lo, double cn0_hi,

@@ -100,6 +100,19 @@ class RfiChannel(ctypes.Structure):
                 ("n_lines", ctypes.c_int32), ("lines", RfiLine * 3)]
 
 
+class NcOptions(ctypes.Structure):
+    _fields_ = [("constellation", ctypes.c_int32), ("prn_filter", ctypes.POINTER(ctypes.c_int32)),
+                ("n_prn_filter", ctypes.c_size_t), ("ant_filter", ctypes.POINTER(ctypes.c_int32)),
+                ("n_ant_filter", ctypes.c_size_t), ("center_freq", ctypes.c_double), ("bin_step_hz", ctypes.c_double),
+                ("n_bins", ctypes.c_int32), ("coherent_periods", ctypes.c_int32), ("blocks", ctypes.c_int32),
+                ("start", ctypes.c_int64)]
+
+
+NC_CELL_DTYPE = np.dtype([("prn", np.int32), ("antenna", np.int32), ("best_freq_idx", np.int32),
+                          ("reserved", np.int32), ("best_codephase", np.int64), ("power", np.float64),
+                          ("second_power", np.float64), ("frequency", np.float64)])
+
+
 _P = ctypes.c_void_p
 
 
@@ -137,6 +150,7 @@ def lib():
     L.tga_set_variant.argtypes = [_P, i32, i32]
     L.tga_set_precision.argtypes = [_P, i32]
     L.tga_rfi_scan.argtypes = [_P, _P, sz, sz, dbl, _P]
+    L.tga_search_noncoherent.argtypes = [_P, _P, sz, sz, dbl, _P, _P, sz, _P]
     L.tga_acr_table.argtypes = [_P, i32, i32, dbl, dbl, dbl, dbl, i32, _P, sz, _P]
     L.tga_rfi_json.argtypes = [_P, sz, _P]
     L.tga_fine_eval.argtypes = [_P, _P, sz, sz, dbl, _P, _P, dbl, _P, _P, _P]
@@ -396,6 +410,26 @@ class Context:
                                            len(tasks), ctypes.byref(opt), out, _ptr(phases)))
         res = [{k: getattr(r, k) for k, _ in FineResult._fields_} for r in out]
         return res, phases
+
+    def search_noncoherent(self, packed_bits, sampling_freq, constellation, prns=None, ants=None,
+                           center_freq=GPS_IF, bin_step_hz=500.0, n_bins=21, coherent_periods=1, blocks=10, start=0):
+        """Non-coherent search: record array of NC_CELL_DTYPE in (PRN, antenna) order."""
+        bits = np.ascontiguousarray(packed_bits, dtype=np.uint8)
+        pr = None if prns is None else np.ascontiguousarray(prns, dtype=np.int32)
+        an = None if ants is None else np.ascontiguousarray(ants, dtype=np.int32)
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        o = NcOptions(int(constellation), None if pr is None else pr.ctypes.data_as(i32p), 0 if pr is None else len(pr),
+                      None if an is None else an.ctypes.data_as(i32p), 0 if an is None else len(an),
+                      float(center_freq), float(bin_step_hz), int(n_bins), int(coherent_periods), int(blocks),
+                      int(start))
+        n = ctypes.c_size_t()
+        self._check(lib().tga_search_noncoherent(self._h, _ptr(bits), bits.shape[0], bits.shape[1],
+                                                 float(sampling_freq), ctypes.byref(o), None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, dtype=NC_CELL_DTYPE)
+        self._check(lib().tga_search_noncoherent(self._h, _ptr(bits), bits.shape[0], bits.shape[1],
+                                                 float(sampling_freq), ctypes.byref(o), _ptr(out), len(out),
+                                                 ctypes.byref(n)))
+        return out
 
     def acr_table(self, constellation, prn=1, sampling_freq=16.368e6, cn0_lo=33.0, cn0_hi=62.0, cn0_step=0.5,
                   trials=100):
