@@ -195,6 +195,8 @@ def main():
                          "(default), or FP32 CUDA cores")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the second arithmetic (the FP32 fused search beside the tensor-core one)")
+    ap.add_argument("--no-weak", action="store_true",
+                    help="skip the weak-signal non-coherent search (10 ms coherent x 10, 201 x 50 Hz bins)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -325,6 +327,36 @@ def main():
     if not args.no_compare:
         oprec = "fp32" if args.precision == "fp16tc" else "fp16tc"
         other = (oprec,) + measure(oprec)
+    weak = None
+    if not args.no_weak:
+        # weak-signal search on the same recording: GPS C/A PRNs 1-32, 10 ms
+        # coherent blocks x 10 (100 ms), 201 bins of 50 Hz; cells count
+        # (antenna, PRN, bin, code phase, block)
+        host = pinned.numpy()
+        kw = dict(prns=list(range(1, 33)), bin_step_hz=50.0, n_bins=201, coherent_periods=10, blocks=10)
+        for _ in range(args.warmup):
+            ctx.search_noncoherent(host, FS, tga.GPS, **kw)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        wt = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.search_noncoherent(host, FS, tga.GPS, **kw)
+            wt.append(time.perf_counter() - t0)
+        w_s = statistics.mean(wt)
+        if world > 1:
+            t = torch.tensor([w_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            w_s = float(t.item())
+        wcells = n_ant * 32 * 201 * 16368.0 * 10
+        weak = {"workload": "GPS C/A PRNs 1-32 x %d ant, 10 ms coherent x 10 blocks (100 ms), 201 x 50 Hz bins, "
+                            "FP32 non-coherent search through tga_search_noncoherent (host bits, end to end)" % n_ant,
+                "value": wcells * world / w_s, "unit": "cell-blocks/s", "ms_per_step": w_s * 1e3,
+                "cells_per_step_per_gpu": wcells}
     clocks = clk.stop()
     sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
     value = cells * world / (ms_step / 1e3)
@@ -376,6 +408,8 @@ def main():
                            "speedup_of_headline": value / ovalue, "same_detections": same,
                            "detected_cells": int(da.sum()), "cells": int(len(da)),
                            "roofline": roofline(oagg, oprec, sm_mhz), "gpu_launches": olaunch}
+    if weak is not None:
+        line["weak_signal"] = weak
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, desc = cpu_sample_baseline(os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": "cells/s", "cores": os.cpu_count(), "kind": "port",
