@@ -113,6 +113,13 @@ NC_CELL_DTYPE = np.dtype([("prn", np.int32), ("antenna", np.int32), ("best_freq_
                           ("second_power", np.float64), ("frequency", np.float64)])
 
 
+class Observation(ctypes.Structure):
+    """tga_observation (Observation::from_hdf5, observation.rs:48-92)."""
+    _fields_ = [("num_antenna", ctypes.c_uint32), ("sampling_frequency", ctypes.c_double),
+                ("row_bytes", ctypes.c_size_t), ("timestamp", ctypes.c_char * 64),
+                ("config_json", ctypes.c_void_p), ("data", ctypes.c_void_p), ("error", ctypes.c_char * 256)]
+
+
 _P = ctypes.c_void_p
 
 
@@ -151,6 +158,9 @@ def lib():
     L.tga_set_precision.argtypes = [_P, i32]
     L.tga_rfi_scan.argtypes = [_P, _P, sz, sz, dbl, _P]
     L.tga_search_noncoherent.argtypes = [_P, _P, sz, sz, dbl, _P, _P, sz, _P]
+    L.tga_results_json.argtypes = [_P, sz, _P, sz, ctypes.c_uint32, i32, dbl, dbl, _P, _P]
+    L.tga_observation_read_hdf5.argtypes = [ctypes.c_char_p, _P]
+    L.tga_observation_free.argtypes = [_P]
     L.tga_acr_table.argtypes = [_P, i32, i32, dbl, dbl, dbl, dbl, i32, _P, sz, _P]
     L.tga_rfi_json.argtypes = [_P, sz, _P]
     L.tga_fine_eval.argtypes = [_P, _P, sz, sz, dbl, _P, _P, dbl, _P, _P, _P]
@@ -160,6 +170,24 @@ def lib():
     L.tga_kernel_times.argtypes = [_P, i32, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_int)]
     _lib = L
     return L
+
+
+def read_hdf5(path):
+    """TART HDF5 observation: dict(num_antenna, sampling_frequency, row_bytes,
+    timestamp, config (str), data [num_antenna, row_bytes] packed bits)."""
+    obs = Observation()
+    rc = lib().tga_observation_read_hdf5(str(path).encode(), ctypes.byref(obs))
+    if rc:
+        raise TgaError(rc, obs.error.decode(errors="replace"))
+    try:
+        n = obs.num_antenna * obs.row_bytes
+        data = np.ctypeslib.as_array(ctypes.cast(obs.data, ctypes.POINTER(ctypes.c_uint8)), shape=(n,)).copy()
+        out = dict(num_antenna=obs.num_antenna, sampling_frequency=obs.sampling_frequency, row_bytes=obs.row_bytes,
+                   timestamp=obs.timestamp.decode(), config=ctypes.string_at(obs.config_json).decode(),
+                   data=data.reshape(obs.num_antenna, obs.row_bytes))
+    finally:
+        lib().tga_observation_free(ctypes.byref(obs))
+    return out
 
 
 def _ptr(a):
@@ -377,6 +405,23 @@ class Context:
         self._check(lib().tga_antenna_xcorr(self._h, _ptr(bits), bits.shape[0], bits.shape[1], i, j,
                                             ctypes.byref(out)))
         return out.value
+
+    def acquire_json(self, packed_bits, sampling_freq, mask=ALL, cn0=False, filter_phase_mad=float("nan"),
+                     filter_freq_mad=float("nan")):
+        """The CLI's acquisition JSON (CombinedOutput, main.rs:893) for every
+        antenna: the cells of acquire_cells through tga_results_json; a MAD
+        filter of NaN is off (--filter-phase-mad / --filter-freq-mad)."""
+        cells = self.acquire_cells(packed_bits, sampling_freq, mask=mask, cn0=cn0)
+        n_ant = np.asarray(packed_bits).shape[0]
+        ants = np.arange(n_ant, dtype=np.int32)
+        p = ctypes.c_char_p()
+        nf = ctypes.c_size_t()
+        self._check(lib().tga_results_json(_ptr(cells), len(cells), _ptr(ants), n_ant, mask, int(cn0),
+                                           float(filter_phase_mad), float(filter_freq_mad), ctypes.byref(p),
+                                           ctypes.byref(nf)))
+        text = ctypes.string_at(p).decode()
+        lib().tga_free(p)
+        return text
 
     def fine_eval(self, packed_bits, sampling_freq, constellation, prn, code_phase, frequency, start, length,
                   phases=None, edge_sigma_chips=0.1):

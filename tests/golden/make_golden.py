@@ -19,6 +19,11 @@ Outputs (committed; the GPU box never reads the reference):
   longest search window), plus the sampling rate from the file's config.
   The HDF5 `data` dataset is stored contiguous and uncompressed at the end
   of the file; its offset is checked against the JSON config.
+* tart_head4096.hdf -- the same HDF5 file cut down to the first 4096 bytes
+  of every antenna row: the file's own metadata (its first 6176 bytes)
+  with the `data` dataspace (current and maximum dims) and the contiguous
+  layout size patched to 24 x 4096, followed by the 24 row heads.  It is a
+  valid HDF5 file of the reference's layout for the reader and CLI tests.
 """
 import json
 import os
@@ -70,7 +75,30 @@ def main(ref):
                         ones=ones, row_bytes=np.int64(row_bytes),
                         sampling_frequency=np.float64(cfg["sampling_frequency"]),
                         timestamp=np.bytes_(b"2026-03-09T04:25:10.145497+00:00"))
-    print("wrote kats.json and tart_head.npz", ones[:4], off)
+    write_hdf5_fixture(raw, block, n_ant, row_bytes, off)
+    print("wrote kats.json, tart_head.npz and tart_head4096.hdf", ones[:4], off)
+
+
+# byte offsets, inside the first 6176 bytes of the reference file, of the
+# `data` dataset's dataspace dims (row length, current and maximum) and of
+# its contiguous layout size
+DIM_OFFSETS = (1712, 1728)
+LAYOUT_SIZE_OFFSET = 1794
+HEAD_ROW = 4096
+
+
+def write_hdf5_fixture(raw, block, n_ant, row_bytes, off):
+    import struct
+    meta = bytearray(raw[:off])
+    for o in DIM_OFFSETS:
+        assert struct.unpack_from("<Q", meta, o)[0] == row_bytes
+        assert struct.unpack_from("<Q", meta, o - 8)[0] == n_ant
+        struct.pack_into("<Q", meta, o, HEAD_ROW)
+    assert struct.unpack_from("<Q", meta, LAYOUT_SIZE_OFFSET)[0] == n_ant * row_bytes
+    assert struct.unpack_from("<Q", meta, LAYOUT_SIZE_OFFSET - 8)[0] == off
+    struct.pack_into("<Q", meta, LAYOUT_SIZE_OFFSET, n_ant * HEAD_ROW)
+    with open(os.path.join(HERE, "tart_head4096.hdf"), "wb") as f:
+        f.write(bytes(meta) + block[:, :HEAD_ROW].tobytes())
 
 
 if __name__ == "__main__":
