@@ -227,6 +227,12 @@ int tga_set_profiling(tga_ctx* ctx, int enable);
  *    every (antenna, PRN) is then re-evaluated in FP32, so reported peak, lag
  *    and second peak are FP32 values; only the choice of Doppler bin and
  *    hypothesis among near-equal candidates can differ from the FP32 mode. */
+/* Test hooks (0 in normal use).  TGA_TEST_TC_SKIP_COMMIT: the tensor-core
+ * correlator issues no MMA for its first batch, so its bounded wait (1 s)
+ * expires with nothing in flight; the call then fails with TGA_ERR_TIMEOUT
+ * and the context stays usable.  It exists to test that failure path. */
+#define TGA_TEST_TC_SKIP_COMMIT 1
+int tga_set_test_flags(tga_ctx* ctx, int flags);
 #define TGA_PRECISION_FP32 0
 #define TGA_PRECISION_FP16_TC 1
 int tga_set_precision(tga_ctx* ctx, int precision);

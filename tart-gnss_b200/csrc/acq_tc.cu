@@ -30,8 +30,8 @@
 //
 // One CTA per (row, group of BC code-phase residues); two CTAs per SM share
 // the SM's 512 TMEM columns and overlap one CTA's tensor-core work with the
-// other's SIMT work.  Waits on the tensor cores are bounded: on expiry the
-// kernel sets *err, drains (again bounded), frees its TMEM and returns.
+// other's SIMT work.  Waits on the tensor cores are bounded (1 s): on expiry
+// the kernel sets *err, drains (again bounded), frees its TMEM and returns.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -161,6 +161,24 @@ constexpr int cmax3(int a, int b, int c) { return a > b ? (a > c ? a : c) : (b >
 constexpr int kTcThreads = 384;  // 12 warps: a multiple of the 4 TMEM lane quadrants
 constexpr int kTcTmemCols = 256;
 constexpr long long kWaitPolls = 1LL << 22;
+constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per wait on the tensor cores
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// polls the mbarrier phase until it completes, at most kWaitPolls times and
+// kWaitNs nanoseconds (a suspended try_wait has no fixed duration)
+__device__ __forceinline__ uint32_t bounded_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t done = 0;
+  const unsigned long long t0 = globaltimer_ns();
+  for (long long k = 0; k < kWaitPolls && !done; ++k) {
+    done = mbar_try_wait(bar, phase);
+    if (!done && (k & 63) == 63 && globaltimer_ns() - t0 > kWaitNs) break;
+  }
+  return done;
+}
 
 // factorisation Lc = 31 * R2 * R3 and the number of code-phase residues
 // (transforms) a CTA runs together
@@ -312,6 +330,7 @@ struct Tc3Params {
   int n_items;  // n_ab * 2 * groups
   int groups;   // ceil(S / BC)
   int n_prn, S;
+  int skip_commit;  // test hook: see TGA_TEST_TC_SKIP_COMMIT
 };
 
 // Code of an output of the inverse transform -> its lag.  The code packs
@@ -395,10 +414,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) pfa_tc3_kernel(Tc3Params p) {
   // and issue nothing, which leaves the SM to the co-resident CTA.
   auto wait_mma = [&]() -> bool {
     uint32_t done = 1;
-    if (warp == 0) {
-      done = 0;
-      for (long long k = 0; k < kWaitPolls && !done; ++k) done = mbar_try_wait(&s_bar, phase);
-    }
+    if (warp == 0) done = bounded_wait(&s_bar, phase);
     if (__syncthreads_or(!done)) return false;
     phase ^= 1u;
     tc_fence_after();
@@ -485,14 +501,19 @@ __global__ void __launch_bounds__(kTcThreads, 2) pfa_tc3_kernel(Tc3Params p) {
           s_key[(it + 1) & 1] = 0ull;
         }
         tc_fence_after();
+        // test hook (TGA_TEST_TC_SKIP_COMMIT): issue nothing, so the wait
+        // below runs out and the failure path is exercised with no
+        // tensor-core work in flight
+        if (!p.skip_commit) {
 #pragma unroll 1
-        for (int t = 0; t < T::TILES1; ++t)
+          for (int t = 0; t < T::TILES1; ++t)
 #pragma unroll 1
-          for (int ks = 0; ks < T::K1 / 16; ++ks)
-            mma_f16(tmem_base + (uint32_t)(t * T::N1),
-                    desc_kchunks(a_addr + t * 2048, T::LBO1) + (uint64_t)(2 * ks * (T::LBO1 >> 4)), db1 + 2 * ks,
-                    idesc_f16(T::N1), ks > 0 ? 1u : 0u);
-        mma_commit(&s_bar);
+            for (int ks = 0; ks < T::K1 / 16; ++ks)
+              mma_f16(tmem_base + (uint32_t)(t * T::N1),
+                      desc_kchunks(a_addr + t * 2048, T::LBO1) + (uint64_t)(2 * ks * (T::LBO1 >> 4)), db1 + 2 * ks,
+                      idesc_f16(T::N1), ks > 0 ? 1u : 0u);
+          mma_commit(&s_bar);
+        }
         pend = (long long)ab_h * p.n_prn + prn;
       }
       if (!wait_mma()) {
@@ -624,8 +645,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) pfa_tc3_kernel(Tc3Params p) {
     // the tensor cores did not answer in time: flag it, give the in-flight
     // MMAs a second bounded window to finish, then release TMEM
     if (tid == 0) atomicExch(p.err, 1);
-    uint32_t done = 0;
-    for (long long k = 0; k < kWaitPolls && !done; ++k) done = mbar_try_wait(&s_bar, phase);
+    bounded_wait(&s_bar, phase);
     __syncthreads();
   } else {
     __syncthreads();
@@ -639,9 +659,11 @@ __global__ void __launch_bounds__(kTcThreads, 2) pfa_tc3_kernel(Tc3Params p) {
 
 template <int M>
 cudaError_t run_tc3(const PolyClass& pc, const SearchDims& dims, const void* d_bmat, const void* d_z16,
-                    const void* d_d16, unsigned long long* d_keys, int* d_err, int num_sms, cudaStream_t st) {
+                    const void* d_d16, unsigned long long* d_keys, int* d_err, int test_flags, int num_sms,
+                    cudaStream_t st) {
   using T = T3<M>;
   Tc3Params p = {};
+  p.skip_commit = test_flags & 1;
   p.bmat = static_cast<const uint4*>(d_bmat);
   p.z16 = static_cast<const uint4*>(d_z16);
   p.d16 = static_cast<const uint4*>(d_d16);
@@ -738,12 +760,12 @@ cudaError_t launch_tc_pack(const PolyClass& pc, const float2* d_src, long long n
 }
 
 cudaError_t launch_correlate_tc(const PolyClass& pc, const SearchDims& dims, const void* d_bmat, const void* d_z16,
-                                const void* d_d16, unsigned long long* d_keys, int* d_err, int num_sms,
-                                cudaStream_t st) {
+                                const void* d_d16, unsigned long long* d_keys, int* d_err, int test_flags,
+                                int num_sms, cudaStream_t st) {
   switch (pc.M) {
-    case 1: return run_tc3<1>(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, num_sms, st);
-    case 4: return run_tc3<4>(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, num_sms, st);
-    case 10: return run_tc3<10>(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, num_sms, st);
+    case 1: return run_tc3<1>(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
+    case 4: return run_tc3<4>(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
+    case 10: return run_tc3<10>(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -98,9 +98,11 @@ double tc_gemm_flops_per_point(int M);
 std::vector<unsigned char> tc_dft_matrices(int M);
 cudaError_t launch_tc_pack(const PolyClass& pc, const float2* d_src, long long n_seq, bool code, void* d_dst,
                            int num_sms, cudaStream_t st);
+// test_flags bit 0: skip the first MMA batch and its commit (test hook for
+// the bounded-wait failure path; 0 in normal use)
 cudaError_t launch_correlate_tc(const PolyClass& pc, const SearchDims& dims, const void* d_bmat, const void* d_z16,
-                                const void* d_d16, unsigned long long* d_keys, int* d_err, int num_sms,
-                                cudaStream_t st);
+                                const void* d_d16, unsigned long long* d_keys, int* d_err, int test_flags,
+                                int num_sms, cudaStream_t st);
 cudaError_t launch_reduce_bins(const SearchDims& dims, const unsigned long long* d_keys,
                                BestRow* d_best, cudaStream_t st);
 cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,

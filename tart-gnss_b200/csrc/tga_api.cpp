@@ -69,6 +69,7 @@ struct tga_ctx {
   };
   std::vector<std::pair<std::string, KTime>> ktimes;
   int* tc_err_pending = nullptr;  // device flag of the last tensor-core launch
+  int test_flags = 0;             // TGA_TEST_* hooks (tga_set_test_flags)
   // planning caches: verified polyphase classes, host chips, uploaded chips
   struct ClassCache {
     bool structure_ok = false;
@@ -401,7 +402,10 @@ void run_group(tga_ctx* ctx, const ClassGroup& grp, const SampleSource& src, con
     CK(cudaMemsetAsync(d_keys, 0, (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long), st));
     // tensor-core FLOPs of the three DFT stages as dense real GEMMs
     timed(ctx, ("correlate_tc" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * tc_gemm_flops_per_point(pc.M),
-          [&] { return launch_correlate_tc(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, ctx->num_sms, st); });
+          [&] {
+            return launch_correlate_tc(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, ctx->test_flags, ctx->num_sms,
+                                       st);
+          });
     ctx->tc_err_pending = d_err;
   } else {
     timed(ctx, ("correlate" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * (tf + 9.0),
@@ -918,6 +922,12 @@ int tga_last_transfer_bytes(const tga_ctx* ctx, uint64_t* h2d, uint64_t* d2h) {
 }
 
 void* tga_stream(tga_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int tga_set_test_flags(tga_ctx* ctx, int flags) {
+  if (!ctx || (flags & ~TGA_TEST_TC_SKIP_COMMIT)) return TGA_ERR_INVALID_ARG;
+  ctx->test_flags = flags;
+  return TGA_OK;
+}
 
 int tga_set_precision(tga_ctx* ctx, int precision) {
   if (!ctx || (precision != TGA_PRECISION_FP32 && precision != TGA_PRECISION_FP16_TC)) return TGA_ERR_INVALID_ARG;

@@ -33,6 +33,7 @@ GPS_IF = 4.092e6
 GPS_SEARCH_BAND = 6000.0
 ACR_TABLE = {GPS: 0, SBAS: 0, QZSS: 0, GALILEO: 1, BEIDOU: 2, L1C: 3}
 PRECISION_FP32, PRECISION_FP16_TC = 0, 1
+TEST_TC_SKIP_COMMIT = 1
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no sm_100 device", 4: "out of memory",
           5: "unsupported", 6: "timeout", 7: "capacity"}
@@ -156,6 +157,7 @@ def lib():
     L.tga_set_profiling.argtypes = [_P, i32]
     L.tga_set_variant.argtypes = [_P, i32, i32]
     L.tga_set_precision.argtypes = [_P, i32]
+    L.tga_set_test_flags.argtypes = [_P, i32]
     L.tga_rfi_scan.argtypes = [_P, _P, sz, sz, dbl, _P]
     L.tga_search_noncoherent.argtypes = [_P, _P, sz, sz, dbl, _P, _P, sz, _P]
     L.tga_results_json.argtypes = [_P, sz, _P, sz, ctypes.c_uint32, i32, dbl, dbl, _P, _P]
@@ -381,6 +383,10 @@ class Context:
             results.sort(key=lambda r: r["sv"])
             out[NAMES[c]] = {"antenna_numbers": ants, "results": results}
         return out
+
+    def set_test_flags(self, flags):
+        """Test hooks (TGA_TEST_*); 0 in normal use."""
+        self._check(lib().tga_set_test_flags(self._h, int(flags)))
 
     def set_precision(self, precision):
         """0 = FP32 (default), 1 = FP16 tensor-core search with FP32 refinement."""

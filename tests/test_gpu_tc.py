@@ -85,3 +85,22 @@ def test_tc_real_recording_same_detections(ctxs):
                       <= REL_TOL * a["signal_strength"][same_row])
         # over all cells the selected row agrees almost everywhere
         assert same_row.mean() > 0.9
+
+
+def test_tc_wait_expiry_reports_timeout_and_context_survives():
+    """Failure detection without a fault: with the test hook the correlator
+    issues no MMA for its first batch, its bounded wait (1 s) expires, the
+    kernel flags it, drains, frees TMEM and returns; the call fails with
+    TGA_ERR_TIMEOUT and the same context then searches normally."""
+    sig, pp, period, fs = _sig(tga.GPS, 7, 47.0, False, 0x7E57)
+    with tga.Context(0) as c:
+        c.set_precision(tga.PRECISION_FP16_TC)
+        c.set_test_flags(tga.TEST_TC_SKIP_COMMIT)
+        with pytest.raises(tga.TgaError) as ei:
+            c.acquire_single(tga.GPS, sig, pp, fs, 4.092e6, 6000.0, 7, period)
+        assert ei.value.code == 6  # TGA_ERR_TIMEOUT
+        c.set_test_flags(0)
+        r = c.acquire_single(tga.GPS, sig, pp, fs, 4.092e6, 6000.0, 7, period)
+        c.set_precision(tga.PRECISION_FP32)
+        f = c.acquire_single(tga.GPS, sig, pp, fs, 4.092e6, 6000.0, 7, period)
+    assert (r.best_codephase, r.best_freq_idx) == (f.best_codephase, f.best_freq_idx)
