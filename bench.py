@@ -77,6 +77,41 @@ def synth_observation(seed, n_ant=N_ANT, n_samples=SAMPLES, chunk=163680):
     return bits, sats
 
 
+def synth_fine_observation(seed, n_ant=24, n=163680, sigma_chips=0.1):
+    """Band-limited 1-bit recording for the fine-acquisition measurement: 6
+    GPS C/A and 6 Galileo E1-C satellites at 45 dB-Hz, continuous delays and
+    Dopplers, chip edges smoothed by a Gaussian of sigma_chips (the front-end
+    model of the refinement), per-antenna carrier phases, unit noise.
+    Returns (bits, satellites)."""
+    import tga
+    from scipy.special import ndtr
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((n_ant, n))
+    t_all = np.arange(n, dtype=np.float64)
+    sats = []
+    for c, hi, per_s, chips in ((0, 32, 1e-3, 1023), (1, 36, 4e-3, 4092)):
+        for prn in rng.choice(np.arange(1, hi + 1), size=6, replace=False):
+            P0 = int(FS * per_s)
+            s = dict(c=c, prn=int(prn), P=P0, tau=float(rng.uniform(0, P0)), dop=float(rng.uniform(-4000, 4000)))
+            seq = tga.code_chips(c, int(prn)).astype(np.float64)
+            L = len(seq)
+            T, sig = FS * per_s / L, sigma_chips * FS * per_s / chips
+            t = t_all - s["tau"]
+            k = np.floor(t / T).astype(np.int64)
+            code = seq[np.mod(k, L)].copy()
+            for dm in (-1, 0, 1, 2):
+                m = k + dm
+                d = seq[np.mod(m, L)] - seq[np.mod(m - 1, L)]
+                u = (t - m * T) / sig
+                code += d * (ndtr(u) - (u >= 0))
+            amp = 2.0 * math.sqrt(10.0 ** 4.5 / FS)
+            cyc = np.mod((4.092e6 + s["dop"]) / FS * t_all, 1.0)
+            for a in range(n_ant):
+                x[a] += amp * code * np.cos(2 * np.pi * cyc + rng.uniform(0, 2 * np.pi))
+            sats.append(s)
+    return np.packbits(x >= 0.0, axis=1), sats
+
+
 class Clocks:
     """nvidia-smi sampler running during the timed region."""
 
@@ -197,6 +232,7 @@ def main():
                     help="skip the second arithmetic (the FP32 fused search beside the tensor-core one)")
     ap.add_argument("--no-weak", action="store_true",
                     help="skip the weak-signal non-coherent search (10 ms coherent x 10, 201 x 50 Hz bins)")
+    ap.add_argument("--no-fine", action="store_true", help="skip the fine-acquisition measurement")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -410,6 +446,42 @@ def main():
                            "roofline": roofline(oagg, oprec, sm_mhz), "gpu_launches": olaunch}
     if weak is not None:
         line["weak_signal"] = weak
+    if not args.no_fine:
+        # fine acquisition: grid estimates of the search, then the joint
+        # multi-antenna Newton refinement, timed end to end through the C ABI
+        fbits, fsats = synth_fine_observation(SEED + 7 + rank, n_ant=n_ant)
+        IF = 4.092e6
+        tasks, gt, gf = [], [], []
+        for sv in fsats:
+            cells = ctx.acquire_cells(fbits, FS, mask=1 << sv["c"], prn_filter=[sv["prn"]])
+            tau_g = cells["best_codephase"] % sv["P"]
+            f_g = cells["frequency"] + IF
+            et = (tau_g - sv["tau"] + 0.5 * sv["P"]) % sv["P"] - 0.5 * sv["P"]
+            ef = f_g - (IF + sv["dop"])
+            hit = (np.abs(et) <= 2.0) & (np.abs(ef) <= 300.0)
+            gt.append(et[hit])
+            gf.append(ef[hit])
+            b = int(np.argmax(cells["signal_strength"]))
+            tasks.append((sv["c"], sv["prn"], float(tau_g[b]), float(f_g[b]), 0, fbits.shape[1] * 8))
+        ft = []
+        for i in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res, _ = ctx.fine_acquire(fbits, FS, tasks)
+            if i >= args.warmup:
+                ft.append(time.perf_counter() - t0)
+        rt = np.array([(r["code_phase"] - sv["tau"] + 0.5 * sv["P"]) % sv["P"] - 0.5 * sv["P"]
+                       for r, sv in zip(res, fsats)])
+        rf = np.array([r["frequency"] - (IF + sv["dop"]) for r, sv in zip(res, fsats)])
+        rms = lambda v: float(np.sqrt(np.mean(np.square(v))))
+        gt, gf = np.concatenate(gt), np.concatenate(gf)
+        line["fine_acquisition"] = {
+            "workload": "%d antennas x 12 satellites (6 GPS C/A, 6 Galileo E1-C), 10 ms window, 45 dB-Hz, band-limited "
+                        "synthetic, joint Newton refinement of delay, Doppler and per-antenna phase" % n_ant,
+            "ms_per_call": 1e3 * statistics.mean(ft),
+            "delay_rms_samples": {"grid": rms(gt), "refined": rms(rt)},
+            "doppler_rms_hz": {"grid": rms(gf), "refined": rms(rf)},
+            "converged": int(sum(r["converged"] for r in res))}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, desc = cpu_sample_baseline(os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": "cells/s", "cores": os.cpu_count(), "kind": "port",
