@@ -24,14 +24,16 @@
 // kz + kd = k and 4 S Lc^2 2^-k <= 32768.  Then |Z 2^-kz| <= 4 S Lc 2^-kz and
 // |C 2^-kd| <= Lc 2^-kd stay inside FP16, every product is below 32768 and so
 // is every correlation value; stage outputs are rounded with satfinite.
-// Keys carry |y|^2 2^-2k and are only compared; the selected row of every
-// (antenna, PRN) is re-evaluated in FP32 afterwards (launch_refine), so the
-// reported peak, lag and second peak are FP32 values.
+// Keys carry the row maximum of |y|^2 2^-2k (the lag bits are zero) and are
+// only compared; the selected row of every (antenna, PRN) is re-evaluated in
+// FP32 afterwards (launch_refine), so the reported peak, lag and second peak
+// are FP32 values.
 //
-// One CTA per (row, group of BC code-phase residues); two CTAs per SM share
-// the SM's 512 TMEM columns and overlap one CTA's tensor-core work with the
-// other's SIMT work.  Waits on the tensor cores are bounded (1 s): on expiry
-// the kernel sets *err, drains (again bounded), frees its TMEM and returns.
+// One CTA per SM (all 512 TMEM columns) runs two PRN chains over the Z of a
+// (row, group of BC code-phase residues) work item, so that the tensor cores
+// work on one chain while the warps transpose the other; a dedicated warp
+// issues the MMAs.  Every wait is bounded (1 s): on expiry the kernel sets
+// *err, drains (again bounded), frees its TMEM and returns.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -91,6 +93,19 @@ __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t d
 }
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// bulk copy global -> this CTA's shared memory, completing `bytes` of the
+// barrier's transaction count (both addresses 16-byte aligned, bytes % 16 == 0)
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
                : "memory");
 }
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
@@ -158,8 +173,10 @@ constexpr uint32_t idesc_f16(int n) { return (1u << 4) | ((uint32_t)(n >> 3) << 
 constexpr int pad16(int x) { return (x + 15) / 16 * 16; }
 constexpr int cmax3(int a, int b, int c) { return a > b ? (a > c ? a : c) : (b > c ? b : c); }
 
-constexpr int kTcThreads = 384;  // 12 warps: a multiple of the 4 TMEM lane quadrants
-constexpr int kTcTmemCols = 256;
+constexpr int kSimtWarps = 12;  // a multiple of the 4 TMEM lane quadrants
+constexpr int kSimtThreads = 32 * kSimtWarps;
+constexpr int kTcThreads = kSimtThreads + 32;  // and the warp that issues the tensor-core work
+constexpr int kTcTmemCols = 512;
 constexpr long long kWaitPolls = 1LL << 22;
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per wait on the tensor cores
 
@@ -171,7 +188,8 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 // polls the mbarrier phase until it completes, at most kWaitPolls times and
 // kWaitNs nanoseconds (a suspended try_wait has no fixed duration)
 __device__ __forceinline__ uint32_t bounded_wait(uint64_t* bar, uint32_t phase) {
-  uint32_t done = 0;
+  uint32_t done = mbar_try_wait(bar, phase);
+  if (done) return done;  // the common case reads no timer
   const unsigned long long t0 = globaltimer_ns();
   for (long long k = 0; k < kWaitPolls && !done; ++k) {
     done = mbar_try_wait(bar, phase);
@@ -202,29 +220,44 @@ struct T3 {
   static constexpr int R2 = Tc3Cfg<M>::R2, R3 = Tc3Cfg<M>::R3, BC = Tc3Cfg<M>::BC;
   static constexpr int LC = 1023 * M, OCOLS = 33 * M;
   static_assert(31 * R2 * R3 == LC, "factorisation");
-  static_assert(R3 == 11, "the epilogue reads 22 TMEM columns");
+  static_assert(R3 == 11, "the epilogue reads 22 TMEM columns per transform");
+  // With R2 even the stage-3 transforms (t1, 2j) and (t1, 2j + 1) share one
+  // operand row: K entries [0, 2 R3) and [P3OFF, P3OFF + 2 R3), against a
+  // block-diagonal DFT-R3 matrix whose outputs land in accumulator columns
+  // [0, 2 R3) and [P3OFF, P3OFF + 2 R3).
+  static constexpr bool PAIR3 = R2 % 2 == 0;
+  static constexpr int P3OFF = 24;
+  static_assert(2 * R3 <= P3OFF, "paired stage-3 halves");
   // rows (transform columns) of each stage for one residue
   static constexpr int ROWS1 = R2 * R3, ROWS2 = 31 * R3, ROWS3 = 31 * R2;
-  static constexpr int NR1 = BC * ROWS1, NR2 = BC * ROWS2, NR3 = BC * ROWS3;
+  static constexpr int ROWS3P = PAIR3 ? ROWS3 / 2 : ROWS3;  // stage-3 operand rows
+  static constexpr int NR1 = BC * ROWS1, NR2 = BC * ROWS2, NR3 = BC * ROWS3P;
   static constexpr int TILES1 = (NR1 + 127) / 128, TILES2 = (NR2 + 127) / 128, TILES3 = (NR3 + 127) / 128;
-  static constexpr int K1 = 64, K2 = pad16(2 * R2), K3 = pad16(2 * R3);
+  static constexpr int K1 = 64, K2 = pad16(2 * R2), K3 = PAIR3 ? 2 * P3OFF : pad16(2 * R3);
   static_assert(K2 <= 64 && K3 <= 64, "one swizzle atom per matrix row");
   static constexpr int N1 = K1, N2 = K2, N3 = K3;
-  static constexpr int KB1 = 128, KB2 = K2 == 64 ? 128 : 64, KB3 = K3 == 64 ? 128 : 64;
-  static_assert(TILES1 * N1 <= kTcTmemCols && TILES2 * N2 <= kTcTmemCols && TILES3 * N3 <= kTcTmemCols, "TMEM");
+  static constexpr int KB1 = 128, KB2 = K2 > 32 ? 128 : 64, KB3 = K3 > 32 ? 128 : 64;
+  // TMEM columns of one chain (its largest stage); two chains per CTA
+  static constexpr int CHAIN_COLS = cmax3(TILES1 * N1, TILES2 * N2, TILES3 * N3);
+  static_assert(CHAIN_COLS <= kTcTmemCols / 2, "two chains in the CTA's TMEM");
   // data operand regions: rows padded to whole tiles, K chunks lbo apart
   static constexpr int LBO1 = TILES1 * 128 * 16 + 16, LBO2 = TILES2 * 128 * 16 + 16, LBO3 = TILES3 * 128 * 16 + 16;
   static constexpr int A_RAW = cmax3(K1 / 8 * LBO1, K2 / 8 * LBO2, K3 / 8 * LBO3);
   static constexpr int A_BYTES = (A_RAW + 1023) / 1024 * 1024;
   static constexpr int B1_BYTES = N1 * KB1, B2_BYTES = N2 * KB2, B3_BYTES = N3 * KB3;
   static_assert(B1_BYTES % 1024 == 0 && B2_BYTES % 1024 == 0 && B3_BYTES % 1024 == 0, "1024-byte aligned regions");
-  // product units: (row, 16-byte chunk of 4 complex inputs); U per thread
+  // one (PRN, hypothesis) block of code units: 8 ROWS1 x 16 bytes
+  static constexpr int CODE_BYTES = 8 * ROWS1 * 16;
+  static constexpr int CODE_REGION = (CODE_BYTES + 1023) / 1024 * 1024;
+  // product units: (row, 16-byte chunk of 4 complex inputs); U per SIMT thread
   static constexpr int UNITS = NR1 * 8;
-  static constexpr int U = (UNITS + kTcThreads - 1) / kTcThreads;
+  static constexpr int U = (UNITS + kSimtThreads - 1) / kSimtThreads;
   static_assert(8 * ROWS1 < 65536 && 8 * LBO1 < 65536, "packed unit offsets");
-  static constexpr int SMEM_RAW = A_BYTES + B1_BYTES + B2_BYTES + B3_BYTES + 1024;
-  // at least 80 KB so that no more than two CTAs (2 x 256 TMEM columns) share an SM
-  static constexpr int SMEM = SMEM_RAW > 81920 ? SMEM_RAW : 81920;
+  static constexpr int SMEM_RAW = 2 * A_BYTES + B1_BYTES + B2_BYTES + B3_BYTES + 2 * CODE_REGION + 1024;
+  // more than half of the SM's shared memory: one CTA, and so one 512-column
+  // TMEM allocation, per SM
+  static constexpr int SMEM = SMEM_RAW > 120 * 1024 ? SMEM_RAW : 120 * 1024;
+  static_assert(SMEM <= 227 * 1024, "shared memory");
   // CRT output map of the (31, R2, R3) transform: lag digits -> natural index
   static constexpr int E1 = (LC / 31) * modinv_c((LC / 31) % 31, 31);
   static constexpr int E2 = (LC / R2) * modinv_c((LC / R2) % R2, R2);
@@ -249,26 +282,36 @@ __device__ __forceinline__ uint32_t pack_h2_sat(float lo, float hi) {
   asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
   return d;
 }
-// z * c for FP16 complex z = (zr, zi), c = (cr, ci), crot = (-ci, cr)
-__device__ __forceinline__ uint32_t cmul_h2(uint32_t z, uint32_t c, uint32_t crot) {
-  const __half2 zz = bits_h2(z);
-  const __half2 t = __hmul2(__low2half2(zz), bits_h2(c));
-  return h2_bits(__hfma2(__high2half2(zz), bits_h2(crot), t));
+// c * z for FP16 complex c = (cr, ci), z = (zr, zi):
+// cr (zr, zi) + ci (-zi, zr), with (-zi, zr) from swapping the halves of z
+// and flipping the sign bit of the low one
+__device__ __forceinline__ uint32_t cmul_h2(uint32_t z, uint32_t c) {
+  const __half2 cc = bits_h2(c);
+  const uint32_t zs = __byte_perm(z, 0u, 0x1032u) ^ 0x00008000u;
+  const __half2 t = __hmul2(__low2half2(cc), bits_h2(z));
+  return h2_bits(__hfma2(__high2half2(cc), bits_h2(zs), t));
 }
 __device__ __forceinline__ void st_shared_u32(unsigned char* p, uint32_t v) { *reinterpret_cast<uint32_t*>(p) = v; }
 
 // inverse DFT-R as a real N x K matrix in layout KB, built on the host in
 // double precision and rounded once to FP16: row n = 2 t + (0 re | 1 im),
 // column k = 2 d + (0 re | 1 im), entries of exp(+2 pi i t d / R); zero
-// outside 2R x 2R
-template <int R, int N, int KB>
-void host_idft_matrix(unsigned char* dst) {
+// outside 2R x 2R.  PAIR repeats the block at row and column offset `off`.
+template <int R, int N, int KB, bool PAIR>
+void host_idft_matrix(unsigned char* dst, int off) {
   const double kPi = 3.14159265358979323846;
   for (int n = 0; n < N; ++n)
     for (int k = 0; k < KB / 2; ++k) {
+      int nn = n, kk = k;
+      bool in = nn < 2 * R && kk < 2 * R;
+      if (!in && PAIR && nn >= off && nn < off + 2 * R && kk >= off && kk < off + 2 * R) {
+        nn -= off;
+        kk -= off;
+        in = true;
+      }
       double val = 0.0;
-      if (n < 2 * R && k < 2 * R) {
-        const int t = n >> 1, u = n & 1, d = k >> 1, v = k & 1;
+      if (in) {
+        const int t = nn >> 1, u = nn & 1, d = kk >> 1, v = kk & 1;
         const double ang = 2.0 * kPi * (double)((t * d) % R) / (double)R;
         const double c = std::cos(ang), sn = std::sin(ang);
         val = (u == 0) ? (v == 0 ? c : -sn) : (v == 0 ? sn : c);
@@ -280,10 +323,10 @@ void host_idft_matrix(unsigned char* dst) {
 
 // ---------------------------------------------------------------------------
 // FP16 operands in the (31, R2, R3) frequency layout.  Unit (seq, j, u) with
-// u = d3 R2 + d2 holds inputs d1 = 4j .. 4j+3 of stage-1 row u: 4 half2 for Z
-// (16 bytes), 4 x (c, c rotated by i) for the code spectra (32 bytes).
+// u = d3 R2 + d2 holds inputs d1 = 4j .. 4j+3 of stage-1 row u as 4 half2
+// (16 bytes), for Z and for the code spectra alike.
 // ---------------------------------------------------------------------------
-template <int M, bool CODE>
+template <int M>
 __global__ void __launch_bounds__(256) tc_pack_kernel(const float2* __restrict__ src, uint4* __restrict__ dst,
                                                       long long n_units, float scale) {
   using T = T3<M>;
@@ -296,7 +339,7 @@ __global__ void __launch_bounds__(256) tc_pack_kernel(const float2* __restrict__
     const int d3 = u / T::R2, d2 = u - d3 * T::R2;
     const int kpart = T::freq_part(d2, T::R2, T::E2) + T::freq_part(d3, T::R3, T::E3);
     const float2* s = src + seq * T::LC;
-    uint32_t h[4], hr[4];
+    uint32_t h[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int d1 = 4 * j + i;
@@ -310,347 +353,445 @@ __global__ void __launch_bounds__(256) tc_pack_kernel(const float2* __restrict__
         v.y *= scale;
       }
       h[i] = pack_h2(v.x, v.y);
-      hr[i] = pack_h2(-v.y, v.x);
     }
-    if (CODE) {
-      dst[2 * e] = make_uint4(h[0], hr[0], h[1], hr[1]);
-      dst[2 * e + 1] = make_uint4(h[2], hr[2], h[3], hr[3]);
-    } else {
-      dst[e] = make_uint4(h[0], h[1], h[2], h[3]);
-    }
+    dst[e] = make_uint4(h[0], h[1], h[2], h[3]);
   }
 }
 
 struct Tc3Params {
   const uint4* bmat;  // the three DFT matrices in their shared-memory layouts
   const uint4* z16;   // [n_ab*2][S] sequences of 8*ROWS1 units
-  const uint4* d16;   // [n_prn][2] spectra of 8*ROWS1 double units
+  const uint4* d16;   // [n_prn][2] sequences of 8*ROWS1 units
   unsigned long long* keys;
   int* err;
-  int n_items;  // n_ab * 2 * groups
+  int n_items;  // n_ab * 2 * groups: (row, residue group) work items
   int groups;   // ceil(S / BC)
   int n_prn, S;
   int skip_commit;  // test hook: see TGA_TEST_TC_SKIP_COMMIT
 };
 
-// Code of an output of the inverse transform -> its lag.  The code packs
-// (residue slot s, t1, t2, t3) as ((s * 31 + t1) * R2 + t2) * R3 + t3; the lag
-// is rho + S * natural(t1, t2, t3) with rho = rho0 + s.  Out of line: it runs
-// once per PRN and thread, and on exact ties.
-template <int M>
-__device__ __noinline__ int tc_lag_of(int code, int rho0, int S) {
-  using T = T3<M>;
-  const int t3 = code % T::R3;
-  int q = code / T::R3;
-  const int t2 = q % T::R2;
-  q /= T::R2;
-  const int t1 = q % 31, s = q / 31;
-  return rho0 + s + S * T::natural(t1, t2, t3);
+// Reads the 22 accumulator columns of stage-3 transform `half` of this warp's
+// lane quadrant at column taddr into v[0..21] (v[22], v[23] are padding).
+template <bool PAIR3>
+__device__ __forceinline__ void tmem_ld_stage3(uint32_t taddr, int half, uint32_t (&v)[24]) {
+  uint32_t(&lo)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[0]);
+  uint32_t(&lo8)[8] = *reinterpret_cast<uint32_t(*)[8]>(&v[0]);
+  uint32_t(&hi8)[8] = *reinterpret_cast<uint32_t(*)[8]>(&v[16]);
+  uint32_t(&hi16)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[8]);
+  if (!PAIR3 || half == 0) {
+    tmem_ld16(taddr, lo);
+    tmem_ld8(taddr + 16, hi8);
+  } else {
+    tmem_ld8(taddr + 24, lo8);
+    tmem_ld16(taddr + 32, hi16);
+  }
 }
 
+// One CTA per SM.  A work item is one (antenna, bin, hypothesis) row and one
+// group of BC code-phase residues; its Z stays in registers while the CTA
+// runs two chains through the PRNs in pairs: chain x takes PRN 2 i + x (the
+// last PRN twice when their number is odd; the key update is idempotent).
+// Each chain has its own code block in shared memory, fetched for its next
+// PRN with one bulk copy as soon as the chain's products are formed.  Per
+// PRN pair:
+//   SIMT warps:  P1(a) P1(b) P2(a) P2(b) P3(a) P3(b) P4(a) P4(b)
+//   MMA warp:          M1(a) M1(b) M2(a) M2(b) M3(a) M3(b)
+// where Mi(x) runs while the SIMT warps work on the other chain.  Hand-offs:
+// s_ready[x] (arrivals of the 12 SIMT warps: chain x's operands are in
+// shared memory and its accumulator has been read), s_done[x]
+// (tcgen05.commit) and s_code[x] (bulk copy).  A tcgen05.mma holds its
+// thread until the tensor cores take it, so the issuing has a warp of its
+// own.  Every wait is bounded.
 template <int M>
-__global__ void __launch_bounds__(kTcThreads, 2) pfa_tc3_kernel(Tc3Params p) {
+__global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   using T = T3<M>;
-  constexpr int NT = kTcThreads, NW = NT / 32, R2 = T::R2, R3 = T::R3, BC = T::BC, U = T::U;
+  constexpr int NW = kSimtWarps, NTS = kSimtThreads, R2 = T::R2, R3 = T::R3, BC = T::BC, U = T::U;
   static_assert(NW % 4 == 0, "a warp task keeps its TMEM lane quadrant");
   // TMEM columns read by one warp task in the transposition phases
   constexpr int CS1 = T::N1 / 32, CS2 = T::N2 >= 32 ? T::N2 / 32 : 1;
   constexpr int W2 = T::N2 >= 32 ? 32 : T::N2;
+  constexpr int HALVES3 = T::PAIR3 ? 2 : 1;
+  constexpr int NT2 = T::TILES1 * 4 * CS1, NT3 = T::TILES2 * 4 * CS2, NT4 = T::TILES3 * 4 * HALVES3;
+  constexpr int TPW2 = (NT2 + NW - 1) / NW, TPW3 = (NT3 + NW - 1) / NW, TPW4 = (NT4 + NW - 1) / NW;
+  // P4 reads TMEM in batches of LB4 tasks: all loads of a batch in flight,
+  // one wait
+  constexpr int LB4 = TPW4 < 2 ? TPW4 : 2;
   constexpr int kBatch = (U + 1) / 2;
   extern __shared__ unsigned char smem_raw[];
-  __shared__ uint64_t s_bar;
+  __shared__ uint64_t s_ready[2], s_done[2], s_code[2];
   __shared__ uint32_t s_tmem;
-  __shared__ unsigned long long s_key[2];
   const uint32_t raw = smem_addr(smem_raw);
-  unsigned char* A = smem_raw + ((1024 - (raw & 1023)) & 1023);
-  unsigned char* B1 = A + T::A_BYTES;
+  unsigned char* A0 = smem_raw + ((1024 - (raw & 1023)) & 1023);
+  unsigned char* B1 = A0 + 2 * T::A_BYTES;
   unsigned char* B2 = B1 + T::B1_BYTES;
   unsigned char* B3 = B2 + T::B2_BYTES;
+  unsigned char* CODE0 = B3 + T::B3_BYTES;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quad = warp & 3;
-  const int S = p.S;
+  const int S = p.S, n_rounds = (p.n_prn + 1) / 2;
 
   if (warp == 0) {
     tmem_alloc(&s_tmem, kTcTmemCols);
     tmem_relinquish();
   }
   if (tid == 0) {
-    mbar_init(&s_bar, 1);
-    s_key[0] = s_key[1] = 0ull;
+    for (int x = 0; x < 2; ++x) {
+      mbar_init(&s_ready[x], NW);
+      mbar_init(&s_done[x], 1);
+      mbar_init(&s_code[x], 1);
+    }
   }
   // operand rows and K entries that no stage writes (padding) must hold
   // finite values: they meet zeros of the DFT matrices
-  for (int i = tid; i < T::A_BYTES / 16; i += NT) reinterpret_cast<uint4*>(A)[i] = make_uint4(0u, 0u, 0u, 0u);
+  for (int i = tid; i < 2 * T::A_BYTES / 16; i += kTcThreads) reinterpret_cast<uint4*>(A0)[i] = make_uint4(0u, 0u, 0u, 0u);
   constexpr int B_CHUNKS = (T::B1_BYTES + T::B2_BYTES + T::B3_BYTES) / 16;
-  for (int i = tid; i < B_CHUNKS; i += NT) reinterpret_cast<uint4*>(B1)[i] = __ldg(p.bmat + i);
+  for (int i = tid; i < B_CHUNKS; i += kTcThreads) reinterpret_cast<uint4*>(B1)[i] = __ldg(p.bmat + i);
   fence_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = s_tmem;
-  const uint32_t a_addr = smem_addr(A);
-  const uint64_t db1 = Lay<T::KB1>::desc(smem_addr(B1));
-  const uint64_t db2 = Lay<T::KB2>::desc(smem_addr(B2));
-  const uint64_t db3 = Lay<T::KB3>::desc(smem_addr(B3));
-  const uint32_t lane_off = (uint32_t)(quad * 32) << 16;
+  // PRN of chain x in round r
+  auto prn_of = [&](int r, int x) -> int { return 2 * r + x < p.n_prn ? 2 * r + x : p.n_prn - 1; };
 
-  // product units of this thread: unit e = tid + k NT is (row r, chunk j);
-  // packed (code-spectrum unit index << 16) | shared-memory byte offset
-  uint32_t uoff[U];
+  if (warp == NW) {
+    // ---------------- MMA warp: one thread issues the tensor-core work ----------------
+    if (lane == 0) {
+      const uint32_t a_addr = smem_addr(A0);
+      const uint64_t db1 = Lay<T::KB1>::desc(smem_addr(B1));
+      const uint64_t db2 = Lay<T::KB2>::desc(smem_addr(B2));
+      const uint64_t db3 = Lay<T::KB3>::desc(smem_addr(B3));
+      uint32_t ph_ready[2] = {0u, 0u};
+      int commits[2] = {0, 0}, fetches[2] = {0, 0};
+      bool ok = true;
+      // code block of chain x for round r of work item w
+      auto fetch = [&](int x, int w, int r) {
+        const int hyp = (w / p.groups) & 1;
+        const uint4* src = p.d16 + ((size_t)prn_of(r, x) * 2 + hyp) * 8 * T::ROWS1;
+        mbar_arrive_expect_tx(&s_code[x], (uint32_t)T::CODE_BYTES);
+        bulk_g2s(smem_addr(CODE0 + x * T::CODE_REGION), src, (uint32_t)T::CODE_BYTES, &s_code[x]);
+        ++fetches[x];
+      };
+      if ((int)blockIdx.x < p.n_items && n_rounds > 0) {
+        fetch(0, blockIdx.x, 0);
+        fetch(1, blockIdx.x, 0);
+      }
+      for (int w = blockIdx.x; w < p.n_items && ok; w += gridDim.x) {
+        for (int r = 0; r < n_rounds && ok; ++r) {
+#pragma unroll 1
+          for (int st = 0; st < 3 && ok; ++st) {
+#pragma unroll 1
+            for (int x = 0; x < 2; ++x) {
+              if (!bounded_wait(&s_ready[x], ph_ready[x])) {
+                ok = false;
+                break;
+              }
+              ph_ready[x] ^= 1u;
+              tc_fence_after();
+              const uint32_t tm = tmem_base + (uint32_t)(x * (kTcTmemCols / 2));
+              const uint32_t ax = a_addr + (uint32_t)(x * T::A_BYTES);
+              // test hook (TGA_TEST_TC_SKIP_COMMIT): issue nothing, so the
+              // SIMT warps' first wait runs out with no tensor-core work in
+              // flight
+              if (!p.skip_commit) {
+                // fully unrolled: descriptors are the stage's base plus
+                // constants (start-address field in 16-byte units; a tile of
+                // 128 rows is 2048 bytes, a K step two chunks)
+                if (st == 0) {
+                  const uint64_t da = desc_kchunks(ax, T::LBO1);
 #pragma unroll
-  for (int k = 0; k < U; ++k) {
-    const int e = tid + k * NT;
-    const int j = e / T::NR1, r = e - j * T::NR1;
-    const int u = r - (r / T::ROWS1) * T::ROWS1;
-    uoff[k] = e < T::UNITS ? ((uint32_t)(j * T::ROWS1 + u) << 16) | (uint32_t)(r * 16 + j * T::LBO1) : 0u;
-  }
-
-  uint32_t phase = 0;
-  bool failed = false;
-  unsigned it = 0;      // PRN iterations of this CTA (key slot parity)
-  long long pend = -1;  // thread 0: key index awaiting its flush
-
-  // bounded wait for the last commit; false when the tensor cores did not
-  // answer.  One warp polls the mbarrier; the others wait at the CTA barrier
-  // and issue nothing, which leaves the SM to the co-resident CTA.
-  auto wait_mma = [&]() -> bool {
-    uint32_t done = 1;
-    if (warp == 0) done = bounded_wait(&s_bar, phase);
-    if (__syncthreads_or(!done)) return false;
-    phase ^= 1u;
-    tc_fence_after();
-    return true;
-  };
-  auto issue_sync = [&]() {
-    fence_async_smem();
-    tc_fence_before();
-    __syncthreads();
-  };
-
-  for (int w = blockIdx.x; w < p.n_items && !failed; w += gridDim.x) {
-    const int ab_h = w / p.groups, g = w - ab_h * p.groups, hyp = ab_h & 1;
-    // this CTA's Z units, kept in registers for every PRN
-    uint4 zr[U];
+                  for (int t = 0; t < T::TILES1; ++t)
+#pragma unroll
+                    for (int ks = 0; ks < T::K1 / 16; ++ks)
+                      mma_f16(tm + (uint32_t)(t * T::N1), da + (uint64_t)(t * 128 + 2 * ks * (T::LBO1 >> 4)),
+                              db1 + 2 * ks, idesc_f16(T::N1), ks > 0 ? 1u : 0u);
+                } else if (st == 1) {
+                  const uint64_t da = desc_kchunks(ax, T::LBO2);
+#pragma unroll
+                  for (int t = 0; t < T::TILES2; ++t)
+#pragma unroll
+                    for (int ks = 0; ks < T::K2 / 16; ++ks)
+                      mma_f16(tm + (uint32_t)(t * T::N2), da + (uint64_t)(t * 128 + 2 * ks * (T::LBO2 >> 4)),
+                              db2 + 2 * ks, idesc_f16(T::N2), ks > 0 ? 1u : 0u);
+                } else {
+                  const uint64_t da = desc_kchunks(ax, T::LBO3);
+#pragma unroll
+                  for (int t = 0; t < T::TILES3; ++t)
+#pragma unroll
+                    for (int ks = 0; ks < T::K3 / 16; ++ks)
+                      mma_f16(tm + (uint32_t)(t * T::N3), da + (uint64_t)(t * 128 + 2 * ks * (T::LBO3 >> 4)),
+                              db3 + 2 * ks, idesc_f16(T::N3), ks > 0 ? 1u : 0u);
+                }
+                mma_commit(&s_done[x]);
+                ++commits[x];
+              }
+              // chain x has read its code block: fetch its next one
+              if (st == 0) {
+                if (r + 1 < n_rounds)
+                  fetch(x, w, r + 1);
+                else if (w + (int)gridDim.x < p.n_items)
+                  fetch(x, w + gridDim.x, 0);
+              }
+            }
+          }
+        }
+      }
+      // drain: the last commit and the last bulk copy of each chain (after a
+      // timeout they may still be in flight)
+      for (int x = 0; x < 2; ++x) {
+        if (commits[x] > 0) bounded_wait(&s_done[x], (uint32_t)((commits[x] - 1) & 1));
+        if (fetches[x] > 0) bounded_wait(&s_code[x], (uint32_t)((fetches[x] - 1) & 1));
+      }
+      if (!ok) atomicExch(p.err, 1);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- SIMT warps ----------------
+    const uint32_t lane_off = (uint32_t)(quad * 32) << 16;
+    // product units of this thread: unit e = tid + k NTS is (row r, chunk j);
+    // packed (code unit index << 16) | operand byte offset
+    uint32_t uoff[U];
 #pragma unroll
     for (int k = 0; k < U; ++k) {
-      const int e = tid + k * NT;
-      zr[k] = make_uint4(0u, 0u, 0u, 0u);
-      if (e < T::UNITS) {
-        const int j = e / T::NR1, r = e - j * T::NR1;
-        const int s = r / T::ROWS1, u = r - s * T::ROWS1;
-        const int rho = g * BC + s;
-        if (rho < S) zr[k] = __ldcs(p.z16 + (((size_t)ab_h * S + rho) * 8 + j) * T::ROWS1 + u);
-      }
+      const int e = tid + k * NTS;
+      const int j = e / T::NR1, r = e - j * T::NR1;
+      const int u = r - (r / T::ROWS1) * T::ROWS1;
+      uoff[k] = e < T::UNITS ? ((uint32_t)(j * T::ROWS1 + u) << 16) | (uint32_t)(r * 16 + j * T::LBO1) : 0u;
     }
-    // |y|^2 of the 11 outputs of stage-3 row task (warp-collective TMEM
-    // read); returns the code of t3 = 0, or -1 when the row is padding
-    auto p4_row = [&](int task, float(&pw)[11]) -> int {
-      const int t = task >> 2;
-      const int r = t * 128 + quad * 32 + lane;
-      const int s = r / T::ROWS3, q = r - s * T::ROWS3;
-      const int t1 = q / R2, t2 = q - t1 * R2;
-      const uint32_t taddr = tmem_base + lane_off + (uint32_t)(t * T::N3);
-      uint32_t v[16], v2[8];
-      tmem_ld16(taddr, v);
-      tmem_ld8(taddr + 16, v2);
-      tmem_wait_ld();
-#pragma unroll
-      for (int h = 0; h < 8; ++h)
-        pw[h] = fmaf(__uint_as_float(v[2 * h]), __uint_as_float(v[2 * h]),
-                     __uint_as_float(v[2 * h + 1]) * __uint_as_float(v[2 * h + 1]));
-#pragma unroll
-      for (int h = 0; h < 3; ++h)
-        pw[8 + h] = fmaf(__uint_as_float(v2[2 * h]), __uint_as_float(v2[2 * h]),
-                         __uint_as_float(v2[2 * h + 1]) * __uint_as_float(v2[2 * h + 1]));
-      const bool valid = r < T::NR3 && g * BC + s < S;
-      return valid ? ((s * 31 + t1) * R2 + t2) * R3 : -1;
-    };
+    uint32_t ph_done[2] = {0u, 0u}, ph_code[2] = {0u, 0u};
+    bool failed = false;
 
-    for (int prn = 0; prn < p.n_prn; ++prn, ++it) {
-      // ---- P1: FP16 products -> stage-1 operand rows ----
-      const uint4* dsrc = p.d16 + (size_t)2 * (((size_t)prn * 2 + hyp) * 8) * T::ROWS1;
-      // two batches of units: all code-spectrum loads of a batch are in
-      // flight before its products are formed
+    // bounded wait of the whole warp: lane 0 polls, every lane then acquires
+    // the completed phase itself
+    auto warp_wait = [&](uint64_t* bar, uint32_t ph) -> bool {
+      uint32_t ok = 1u;
+      if (lane == 0) ok = bounded_wait(bar, ph);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (ok) (void)mbar_try_wait(bar, ph);
+      return ok != 0u;
+    };
+    // chain x's operands are written and its accumulator read: hand over
+    auto signal = [&](int x) {
+      fence_async_smem();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&s_ready[x]);
+    };
+    // ---- P1: FP16 products Z conj(C) -> stage-1 operand rows of chain x ----
+    auto p1 = [&](const uint4(&zr)[U], unsigned char* A, const unsigned char* code) {
+      const uint4* cp = reinterpret_cast<const uint4*>(code);
 #pragma unroll
       for (int k0 = 0; k0 < U; k0 += kBatch) {
-        uint4 c[2 * kBatch];
+        uint4 c[kBatch];
 #pragma unroll
         for (int i = 0; i < kBatch; ++i) {
           const int k = k0 + i;
-          if (k < U && (k < U - 1 || tid + k * NT < T::UNITS)) {
-            const uint4* src = dsrc + 2 * (uoff[k] >> 16);
-            c[2 * i] = __ldcg(src);
-            c[2 * i + 1] = __ldcg(src + 1);
-          }
+          if (k < U && (k < U - 1 || tid + k * NTS < T::UNITS)) c[i] = cp[uoff[k] >> 16];
         }
 #pragma unroll
         for (int i = 0; i < kBatch; ++i) {
           const int k = k0 + i;
-          if (k < U && (k < U - 1 || tid + k * NT < T::UNITS)) {
-            const uint4 c0 = c[2 * i], c1 = c[2 * i + 1], z = zr[k];
+          if (k < U && (k < U - 1 || tid + k * NTS < T::UNITS)) {
+            const uint4 cc = c[i], z = zr[k];
             *reinterpret_cast<uint4*>(A + (uoff[k] & 0xFFFFu)) =
-                make_uint4(cmul_h2(z.x, c0.x, c0.y), cmul_h2(z.y, c0.z, c0.w), cmul_h2(z.z, c1.x, c1.y),
-                           cmul_h2(z.w, c1.z, c1.w));
+                make_uint4(cmul_h2(z.x, cc.x), cmul_h2(z.y, cc.y), cmul_h2(z.z, cc.z), cmul_h2(z.w, cc.w));
           }
         }
       }
-      issue_sync();
-      if (tid == 0) {
-        if (pend >= 0) {
-          // every warp of the previous PRN has folded its key into the other slot
-          atomicMax(p.keys + pend, s_key[(it + 1) & 1]);
-          s_key[(it + 1) & 1] = 0ull;
-        }
-        tc_fence_after();
-        // test hook (TGA_TEST_TC_SKIP_COMMIT): issue nothing, so the wait
-        // below runs out and the failure path is exercised with no
-        // tensor-core work in flight
-        if (!p.skip_commit) {
-#pragma unroll 1
-          for (int t = 0; t < T::TILES1; ++t)
-#pragma unroll 1
-            for (int ks = 0; ks < T::K1 / 16; ++ks)
-              mma_f16(tmem_base + (uint32_t)(t * T::N1),
-                      desc_kchunks(a_addr + t * 2048, T::LBO1) + (uint64_t)(2 * ks * (T::LBO1 >> 4)), db1 + 2 * ks,
-                      idesc_f16(T::N1), ks > 0 ? 1u : 0u);
-          mma_commit(&s_bar);
-        }
-        pend = (long long)ab_h * p.n_prn + prn;
-      }
-      if (!wait_mma()) {
-        failed = true;
-        break;
-      }
-
-      // ---- P2: stage-1 accumulators -> stage-2 rows (t1, d3), K = d2 ----
-      for (int task = warp; task < T::TILES1 * 4 * CS1; task += NW) {
-        const int t = task / (4 * CS1), half = (task >> 2) % CS1;
-        const int r = t * 128 + quad * 32 + lane;
-        const bool valid = r < T::NR1;
-        const int s = r / T::ROWS1, u = r - s * T::ROWS1;
-        const int d3 = u / R2, d2 = u - d3 * R2;
-        // stage-2 row (t1, d3) = s ROWS2 + t1 R3 + d3, K entry d2
-        unsigned char* dst = A + (s * T::ROWS2 + d3) * 16 + (d2 >> 2) * T::LBO2 + (d2 & 3) * 4;
-        uint32_t v[32];
-        tmem_ld_cols<2>(tmem_base + lane_off + (uint32_t)(t * T::N1 + 32 * half), v);
+    };
+    // ---- P2: stage-1 accumulators -> stage-2 rows (t1, d3), K = d2 ----
+    auto p2 = [&](int x) {
+      unsigned char* A = A0 + x * T::A_BYTES;
+      const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
+      uint32_t v[TPW2][32];
 #pragma unroll
-        for (int h = 0; h < 16; ++h) {
-          const int t1 = 16 * half + h;
-          if (valid && t1 < 31)
-            st_shared_u32(dst + t1 * R3 * 16, pack_h2_sat(__uint_as_float(v[2 * h]), __uint_as_float(v[2 * h + 1])));
+      for (int i = 0; i < TPW2; ++i) {
+        const int task = warp + i * NW;
+        if (task < NT2) {
+          const int t = task / (4 * CS1), half = (task >> 2) % CS1;
+          uint32_t(&a)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[i][0]);
+          uint32_t(&b)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[i][16]);
+          tmem_ld16(tb + (uint32_t)(t * T::N1 + 32 * half), a);
+          tmem_ld16(tb + (uint32_t)(t * T::N1 + 32 * half + 16), b);
         }
       }
-      issue_sync();
-      if (tid == 0) {
-        tc_fence_after();
-#pragma unroll 1
-        for (int t = 0; t < T::TILES2; ++t)
-#pragma unroll 1
-          for (int ks = 0; ks < T::K2 / 16; ++ks)
-            mma_f16(tmem_base + (uint32_t)(t * T::N2),
-                    desc_kchunks(a_addr + t * 2048, T::LBO2) + (uint64_t)(2 * ks * (T::LBO2 >> 4)), db2 + 2 * ks,
-                    idesc_f16(T::N2), ks > 0 ? 1u : 0u);
-        mma_commit(&s_bar);
-      }
-      if (!wait_mma()) {
-        failed = true;
-        break;
-      }
-
-      // ---- P3: stage-2 accumulators -> stage-3 rows (t1, t2), K = d3 ----
-      for (int task = warp; task < T::TILES2 * 4 * CS2; task += NW) {
-        const int t = task / (4 * CS2), half = (task >> 2) % CS2;
-        const int r = t * 128 + quad * 32 + lane;
-        const bool valid = r < T::NR2;
-        const int s = r / T::ROWS2, q = r - s * T::ROWS2;
-        const int t1 = q / R3, d3 = q - t1 * R3;
-        // stage-3 row (t1, t2) = s ROWS3 + t1 R2 + t2, K entry d3
-        unsigned char* dst = A + (s * T::ROWS3 + t1 * R2) * 16 + (d3 >> 2) * T::LBO3 + (d3 & 3) * 4;
-        uint32_t v[W2];
-        tmem_ld_cols<W2 / 16>(tmem_base + lane_off + (uint32_t)(t * T::N2 + W2 * half), v);
+      tmem_wait_ld();
 #pragma unroll
-        for (int h = 0; h < W2 / 2; ++h) {
-          const int t2 = (W2 / 2) * half + h;
-          if (valid && t2 < R2)
-            st_shared_u32(dst + t2 * 16, pack_h2_sat(__uint_as_float(v[2 * h]), __uint_as_float(v[2 * h + 1])));
-        }
-      }
-      issue_sync();
-      if (tid == 0) {
-        tc_fence_after();
-#pragma unroll 1
-        for (int t = 0; t < T::TILES3; ++t)
-#pragma unroll 1
-          for (int ks = 0; ks < T::K3 / 16; ++ks)
-            mma_f16(tmem_base + (uint32_t)(t * T::N3),
-                    desc_kchunks(a_addr + t * 2048, T::LBO3) + (uint64_t)(2 * ks * (T::LBO3 >> 4)), db3 + 2 * ks,
-                    idesc_f16(T::N3), ks > 0 ? 1u : 0u);
-        mma_commit(&s_bar);
-      }
-      if (!wait_mma()) {
-        failed = true;
-        break;
-      }
-
-      // ---- P4: |y|^2 maximum over stage-3 rows (t1, t2), t3 ----
-      // Branch-free per row: the row maximum, the mask of its positions and
-      // the last of them.  The reference keeps the later lag on exact ties
-      // (Iterator::max_by); a thread whose maximum is reached more than once
-      // resolves it exactly in a second pass, which almost never runs.
-      float best = -1.f;
-      int bcode = 0;
-      bool tie = false;
-      for (int task = warp; task < T::TILES3 * 4; task += NW) {
-        float pw[11];
-        const int code0 = p4_row(task, pw);
-        if (code0 >= 0) {
-          float m = pw[0];
+      for (int i = 0; i < TPW2; ++i) {
+        const int task = warp + i * NW;
+        if (task < NT2) {
+          const int t = task / (4 * CS1), half = (task >> 2) % CS1;
+          const int r = t * 128 + quad * 32 + lane;
+          const bool valid = r < T::NR1;
+          const int s = r / T::ROWS1, u = r - s * T::ROWS1;
+          const int d3 = u / R2, d2 = u - d3 * R2;
+          // stage-2 row (t1, d3) = s ROWS2 + t1 R3 + d3, K entry d2
+          unsigned char* dst = A + (s * T::ROWS2 + d3) * 16 + (d2 >> 2) * T::LBO2 + (d2 & 3) * 4;
 #pragma unroll
-          for (int h = 1; h < 11; ++h) m = fmaxf(m, pw[h]);
-          unsigned mask = 0u;
-#pragma unroll
-          for (int h = 0; h < 11; ++h) mask |= (pw[h] == m ? 1u : 0u) << h;
-          if (m > best) {
-            best = m;
-            bcode = code0 + (31 - __clz(mask));
-            tie = __popc(mask) > 1;
-          } else if (m == best) {
-            tie = true;
+          for (int h = 0; h < 16; ++h) {
+            const int t1 = 16 * half + h;
+            if (valid && t1 < 31)
+              st_shared_u32(dst + t1 * R3 * 16,
+                            pack_h2_sat(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h + 1])));
           }
         }
       }
-      int blag = best < 0.f ? 0 : tc_lag_of<M>(bcode, g * BC, S);
-      if (__any_sync(0xffffffffu, tie)) {
-        for (int task = warp; task < T::TILES3 * 4; task += NW) {
-          float pw[11];
-          const int code0 = p4_row(task, pw);
-          if (tie && code0 >= 0) {
+    };
+    // ---- P3: stage-2 accumulators -> stage-3 rows (t1, t2), K = d3 ----
+    auto p3 = [&](int x) {
+      unsigned char* A = A0 + x * T::A_BYTES;
+      const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
+      uint32_t v[TPW3][W2];
 #pragma unroll
-            for (int h = 0; h < 11; ++h)
-              if (pw[h] == best) blag = max(blag, tc_lag_of<M>(code0 + h, g * BC, S));
+      for (int i = 0; i < TPW3; ++i) {
+        const int task = warp + i * NW;
+        if (task < NT3) {
+          const int t = task / (4 * CS2), half = (task >> 2) % CS2;
+#pragma unroll
+          for (int c = 0; c < W2 / 16; ++c) {
+            uint32_t(&a)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[i][16 * c]);
+            tmem_ld16(tb + (uint32_t)(t * T::N2 + W2 * half + 16 * c), a);
           }
         }
       }
-      unsigned long long kbest =
-          best < 0.f ? 0ull : (((unsigned long long)__float_as_uint(best) << 32) | (unsigned)blag);
+      tmem_wait_ld();
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long other = __shfl_xor_sync(0xffffffffu, kbest, o);
-        kbest = other > kbest ? other : kbest;
+      for (int i = 0; i < TPW3; ++i) {
+        const int task = warp + i * NW;
+        if (task < NT3) {
+          const int t = task / (4 * CS2), half = (task >> 2) % CS2;
+          const int r = t * 128 + quad * 32 + lane;
+          const bool valid = r < T::NR2;
+          const int s = r / T::ROWS2, q = r - s * T::ROWS2;
+          const int t1 = q / R3, d3 = q - t1 * R3;
+          if (T::PAIR3) {
+            // paired stage-3 row (t1, t2 / 2) = s ROWS3P + t1 R2 / 2 + t2 / 2,
+            // K entry d3 (t2 even) or P3OFF / 2 + d3 (t2 odd)
+            unsigned char* dst0 =
+                A + (s * T::ROWS3P + t1 * (R2 / 2)) * 16 + (d3 >> 2) * T::LBO3 + (d3 & 3) * 4;
+            unsigned char* dst1 = dst0 + (T::P3OFF / 8) * T::LBO3;
+#pragma unroll
+            for (int h = 0; h < W2 / 2; ++h) {
+              const int t2 = (W2 / 2) * half + h;
+              if (valid && t2 < R2)
+                st_shared_u32(((t2 & 1) ? dst1 : dst0) + (t2 >> 1) * 16,
+                              pack_h2_sat(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h + 1])));
+            }
+          } else {
+            // stage-3 row (t1, t2) = s ROWS3 + t1 R2 + t2, K entry d3
+            unsigned char* dst = A + (s * T::ROWS3 + t1 * R2) * 16 + (d3 >> 2) * T::LBO3 + (d3 & 3) * 4;
+#pragma unroll
+            for (int h = 0; h < W2 / 2; ++h) {
+              const int t2 = (W2 / 2) * half + h;
+              if (valid && t2 < R2)
+                st_shared_u32(dst + t2 * 16,
+                              pack_h2_sat(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h + 1])));
+            }
+          }
+        }
       }
-      if (lane == 0) atomicMax(&s_key[it & 1], kbest);
+    };
+    // ---- P4: |y|^2 maximum over the stage-3 outputs of chain x ----
+    // Only the row maximum is kept: the bin / hypothesis reduction compares
+    // powers alone, and the selected row of every (antenna, PRN) is searched
+    // again in FP32 (launch_refine), which finds its lag with the
+    // reference's tie rule.  Padding rows and residues >= S are skipped.
+    auto p4 = [&](int x, int g) -> float {
+      const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
+      float best = 0.f;
+      // tasks in batches of LB4: all loads of a batch in flight, one wait
+#pragma unroll
+      for (int i0 = 0; i0 < TPW4; i0 += LB4) {
+        uint32_t v[LB4][24];
+#pragma unroll
+        for (int i = 0; i < LB4; ++i) {
+          const int task = warp + (i0 + i) * NW;
+          if (i0 + i < TPW4 && task < NT4) {
+            const int t = task / (4 * HALVES3), half = (task >> 2) % HALVES3;
+            tmem_ld_stage3<T::PAIR3>(tb + (uint32_t)(t * T::N3), half, v[i]);
+          }
+        }
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < LB4; ++i) {
+          const int task = warp + (i0 + i) * NW;
+          if (i0 + i < TPW4 && task < NT4) {
+            const int r = (task / (4 * HALVES3)) * 128 + quad * 32 + lane;
+            if (r < T::NR3 && g * BC + r / T::ROWS3P < S) {
+#pragma unroll
+              for (int h = 0; h < 11; ++h)
+                best = fmaxf(best, fmaf(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h]),
+                                        __uint_as_float(v[i][2 * h + 1]) * __uint_as_float(v[i][2 * h + 1])));
+            }
+          }
+        }
+      }
+      return best;
+    };
+
+    for (int w = blockIdx.x; w < p.n_items && !failed; w += gridDim.x) {
+      const int ab_h = w / p.groups, g = w - ab_h * p.groups;
+      // this item's Z units, kept in registers for every PRN
+      uint4 zr[U];
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        const int e = tid + k * NTS;
+        zr[k] = make_uint4(0u, 0u, 0u, 0u);
+        if (e < T::UNITS) {
+          const int j = e / T::NR1, r = e - j * T::NR1;
+          const int s = r / T::ROWS1, u = r - s * T::ROWS1;
+          const int rho = g * BC + s;
+          if (rho < S) zr[k] = __ldcs(p.z16 + (((size_t)ab_h * S + rho) * 8 + j) * T::ROWS1 + u);
+        }
+      }
+      // chain x: wait for its code block, form its products, hand over
+      auto products = [&](int x) -> bool {
+        if (!warp_wait(&s_code[x], ph_code[x])) return false;
+        ph_code[x] ^= 1u;
+        p1(zr, A0 + x * T::A_BYTES, CODE0 + x * T::CODE_REGION);
+        signal(x);
+        return true;
+      };
+      for (int x = 0; x < 2 && !failed; ++x) failed = !products(x);
+      for (int r = 0; r < n_rounds && !failed; ++r) {
+        // P2, P3 for chain a then chain b, each after its own MMA stage
+#pragma unroll 1
+        for (int st = 0; st < 2 && !failed; ++st) {
+#pragma unroll 1
+          for (int x = 0; x < 2; ++x) {
+            if (!warp_wait(&s_done[x], ph_done[x])) {
+              failed = true;
+              break;
+            }
+            ph_done[x] ^= 1u;
+            tc_fence_after();
+            if (st == 0)
+              p2(x);
+            else
+              p3(x);
+            signal(x);
+          }
+        }
+        // P4 of this round, then at once the products of the chain's next
+        // round, so that the tensor cores are not left idle across rounds
+#pragma unroll 1
+        for (int x = 0; x < 2 && !failed; ++x) {
+          if (!warp_wait(&s_done[x], ph_done[x])) {
+            failed = true;
+            break;
+          }
+          ph_done[x] ^= 1u;
+          tc_fence_after();
+          // non-negative floats order like their bit patterns
+          const unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(p4(x, g)));
+          if (lane == 0 && bits != 0u)
+            atomicMax(p.keys + (size_t)ab_h * p.n_prn + prn_of(r, x), (unsigned long long)bits << 32);
+          if (r + 1 < n_rounds) failed = !products(x);
+        }
+      }
     }
+    if (failed && lane == 0) atomicExch(p.err, 1);
   }
 
-  if (failed) {
-    // the tensor cores did not answer in time: flag it, give the in-flight
-    // MMAs a second bounded window to finish, then release TMEM
-    if (tid == 0) atomicExch(p.err, 1);
-    bounded_wait(&s_bar, phase);
-    __syncthreads();
-  } else {
-    __syncthreads();
-    if (tid == 0 && pend >= 0) atomicMax(p.keys + pend, s_key[(it + 1) & 1]);
-  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -676,9 +817,9 @@ cudaError_t run_tc3(const PolyClass& pc, const SearchDims& dims, const void* d_b
   auto kern = pfa_tc3_kernel<M>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, T::SMEM);
   if (e != cudaSuccess) return e;
-  // two CTAs per SM: T::SMEM >= 80 KB keeps a third one out, so the two
-  // 256-column TMEM allocations always fit
-  int grid = num_sms * 2;
+  // one CTA per SM: T::SMEM is above half of the SM's shared memory, so the
+  // 512-column TMEM allocation never meets another one
+  int grid = num_sms;
   if (grid > p.n_items) grid = p.n_items;
   if (grid < 1) return cudaSuccess;
   kern<<<grid, kTcThreads, T::SMEM, st>>>(p);
@@ -696,13 +837,13 @@ void tc_scales(const PolyClass& pc, int* kz, int* kd) {
   *kd = k - *kz;
 }
 
-template <int M, bool CODE>
+template <int M>
 cudaError_t run_pack(const float2* src, long long n_seq, void* dst, float scale, int num_sms, cudaStream_t st) {
   const long long n_units = n_seq * 8 * T3<M>::ROWS1;
   if (n_units == 0) return cudaSuccess;
   long long blocks = (n_units + 255) / 256;
   if (blocks > (long long)num_sms * 16) blocks = (long long)num_sms * 16;
-  tc_pack_kernel<M, CODE><<<(int)blocks, 256, 0, st>>>(src, static_cast<uint4*>(dst), n_units, scale);
+  tc_pack_kernel<M><<<(int)blocks, 256, 0, st>>>(src, static_cast<uint4*>(dst), n_units, scale);
   kernel_launch_add(1);
   return cudaGetLastError();
 }
@@ -711,9 +852,9 @@ template <int M>
 std::vector<unsigned char> build_matrices() {
   using T = T3<M>;
   std::vector<unsigned char> b((size_t)(T::B1_BYTES + T::B2_BYTES + T::B3_BYTES), 0);
-  host_idft_matrix<31, T::N1, T::KB1>(b.data());
-  host_idft_matrix<T::R2, T::N2, T::KB2>(b.data() + T::B1_BYTES);
-  host_idft_matrix<T::R3, T::N3, T::KB3>(b.data() + T::B1_BYTES + T::B2_BYTES);
+  host_idft_matrix<31, T::N1, T::KB1, false>(b.data(), 0);
+  host_idft_matrix<T::R2, T::N2, T::KB2, false>(b.data() + T::B1_BYTES, 0);
+  host_idft_matrix<T::R3, T::N3, T::KB3, T::PAIR3>(b.data() + T::B1_BYTES + T::B2_BYTES, T::P3OFF);
   return b;
 }
 
@@ -721,7 +862,8 @@ std::vector<unsigned char> build_matrices() {
 
 size_t tc_operand_bytes(const PolyClass& pc, long long n_seq, bool code) {
   const int rows1 = pc.Lc / 31;  // R2 * R3
-  return (size_t)n_seq * 8 * rows1 * (code ? 32 : 16);
+  (void)code;
+  return (size_t)n_seq * 8 * rows1 * 16;
 }
 
 double tc_gemm_flops_per_point(int M) {
@@ -749,12 +891,9 @@ cudaError_t launch_tc_pack(const PolyClass& pc, const float2* d_src, long long n
   tc_scales(pc, &kz, &kd);
   const float scale = (float)(1.0 / (double)(1ull << (code ? kd : kz)));
   switch (pc.M) {
-    case 1: return code ? run_pack<1, true>(d_src, n_seq, d_dst, scale, num_sms, st)
-                        : run_pack<1, false>(d_src, n_seq, d_dst, scale, num_sms, st);
-    case 4: return code ? run_pack<4, true>(d_src, n_seq, d_dst, scale, num_sms, st)
-                        : run_pack<4, false>(d_src, n_seq, d_dst, scale, num_sms, st);
-    case 10: return code ? run_pack<10, true>(d_src, n_seq, d_dst, scale, num_sms, st)
-                         : run_pack<10, false>(d_src, n_seq, d_dst, scale, num_sms, st);
+    case 1: return run_pack<1>(d_src, n_seq, d_dst, scale, num_sms, st);
+    case 4: return run_pack<4>(d_src, n_seq, d_dst, scale, num_sms, st);
+    case 10: return run_pack<10>(d_src, n_seq, d_dst, scale, num_sms, st);
   }
   return cudaErrorInvalidValue;
 }
