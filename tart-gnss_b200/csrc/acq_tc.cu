@@ -198,21 +198,27 @@ __device__ __forceinline__ uint32_t bounded_wait(uint64_t* bar, uint32_t phase) 
   return done;
 }
 
-// factorisation Lc = 31 * R2 * R3 and the number of code-phase residues
-// (transforms) a CTA runs together
+// factorisation Lc = 31 * R2 * R3, the number of code-phase residues
+// (transforms) a CTA runs together, the order of the stage-2 rows (S2O, see
+// T3) and the padding of the K-chunk strides of stages 2 and 3 (16-byte
+// units), chosen for the fewest shared-memory bank conflicts of the
+// transposition stores
 template <int M>
 struct Tc3Cfg;
 template <>
 struct Tc3Cfg<1> {
-  static constexpr int R2 = 3, R3 = 11, BC = 4;
+  static constexpr int R2 = 3, R3 = 11, BC = 4, PAD2 = 1, PAD3 = 1;
+  static constexpr bool S2O = false;
 };
 template <>
 struct Tc3Cfg<4> {
-  static constexpr int R2 = 12, R3 = 11, BC = 2;
+  static constexpr int R2 = 12, R3 = 11, BC = 2, PAD2 = 3, PAD3 = 1;
+  static constexpr bool S2O = false;
 };
 template <>
 struct Tc3Cfg<10> {
-  static constexpr int R2 = 30, R3 = 11, BC = 1;
+  static constexpr int R2 = 30, R3 = 11, BC = 1, PAD2 = 2, PAD3 = 1;
+  static constexpr bool S2O = true;
 };
 
 template <int M>
@@ -228,8 +234,13 @@ struct T3 {
   static constexpr bool PAIR3 = R2 % 2 == 0;
   static constexpr int P3OFF = 24;
   static_assert(2 * R3 <= P3OFF, "paired stage-3 halves");
-  // rows (transform columns) of each stage for one residue
-  static constexpr int ROWS1 = R2 * R3, ROWS2 = 31 * R3, ROWS3 = 31 * R2;
+  // rows (transform columns) of each stage for one residue.  Stage-2 row
+  // (t1, d3) is t1 R3 + d3, or with S2O ((d3 / 4) 32 + t1) 4 + d3 % 4 (384
+  // rows, some of them padding): a warp then holds 8 consecutive t1 x 4
+  // values of d3 % 4, whose stage-3 stores fall in 32 different banks
+  static constexpr bool S2O = Tc3Cfg<M>::S2O;
+  static_assert(!S2O || R3 <= 12, "S2O: three groups of four d3");
+  static constexpr int ROWS1 = R2 * R3, ROWS2 = S2O ? 384 : 31 * R3, ROWS3 = 31 * R2;
   static constexpr int ROWS3P = PAIR3 ? ROWS3 / 2 : ROWS3;  // stage-3 operand rows
   static constexpr int NR1 = BC * ROWS1, NR2 = BC * ROWS2, NR3 = BC * ROWS3P;
   static constexpr int TILES1 = (NR1 + 127) / 128, TILES2 = (NR2 + 127) / 128, TILES3 = (NR3 + 127) / 128;
@@ -241,7 +252,8 @@ struct T3 {
   static constexpr int CHAIN_COLS = cmax3(TILES1 * N1, TILES2 * N2, TILES3 * N3);
   static_assert(CHAIN_COLS <= kTcTmemCols / 2, "two chains in the CTA's TMEM");
   // data operand regions: rows padded to whole tiles, K chunks lbo apart
-  static constexpr int LBO1 = TILES1 * 128 * 16 + 16, LBO2 = TILES2 * 128 * 16 + 16, LBO3 = TILES3 * 128 * 16 + 16;
+  static constexpr int LBO1 = TILES1 * 128 * 16 + 16, LBO2 = TILES2 * 128 * 16 + 16 * Tc3Cfg<M>::PAD2,
+                       LBO3 = TILES3 * 128 * 16 + 16 * Tc3Cfg<M>::PAD3;
   static constexpr int A_RAW = cmax3(K1 / 8 * LBO1, K2 / 8 * LBO2, K3 / 8 * LBO3);
   static constexpr int A_BYTES = (A_RAW + 1023) / 1024 * 1024;
   static constexpr int B1_BYTES = N1 * KB1, B2_BYTES = N2 * KB2, B3_BYTES = N3 * KB3;
@@ -560,14 +572,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
     uint32_t ph_done[2] = {0u, 0u}, ph_code[2] = {0u, 0u};
     bool failed = false;
 
-    // bounded wait of the whole warp: lane 0 polls, every lane then acquires
-    // the completed phase itself
+    // bounded wait of the whole warp: every lane tests the phase (one
+    // instruction for the warp when it has completed, the common case); a
+    // warp that must wait polls until all its lanes have seen it complete
     auto warp_wait = [&](uint64_t* bar, uint32_t ph) -> bool {
-      uint32_t ok = 1u;
-      if (lane == 0) ok = bounded_wait(bar, ph);
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      if (ok) (void)mbar_try_wait(bar, ph);
-      return ok != 0u;
+      if (__all_sync(0xffffffffu, mbar_try_wait(bar, ph))) return true;
+      return __all_sync(0xffffffffu, bounded_wait(bar, ph)) != 0;
     };
     // chain x's operands are written and its accumulator read: hand over
     auto signal = [&](int x) {
@@ -624,13 +634,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
           const bool valid = r < T::NR1;
           const int s = r / T::ROWS1, u = r - s * T::ROWS1;
           const int d3 = u / R2, d2 = u - d3 * R2;
-          // stage-2 row (t1, d3) = s ROWS2 + t1 R3 + d3, K entry d2
-          unsigned char* dst = A + (s * T::ROWS2 + d3) * 16 + (d2 >> 2) * T::LBO2 + (d2 & 3) * 4;
+          // stage-2 row (t1, d3), K entry d2
+          constexpr int T1_STRIDE = T::S2O ? 4 * 16 : R3 * 16;
+          unsigned char* dst = A + (s * T::ROWS2 + (T::S2O ? (d3 >> 2) * 128 + (d3 & 3) : d3)) * 16 +
+                               (d2 >> 2) * T::LBO2 + (d2 & 3) * 4;
 #pragma unroll
           for (int h = 0; h < 16; ++h) {
             const int t1 = 16 * half + h;
             if (valid && t1 < 31)
-              st_shared_u32(dst + t1 * R3 * 16,
+              st_shared_u32(dst + t1 * T1_STRIDE,
                             pack_h2_sat(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h + 1])));
           }
         }
@@ -660,9 +672,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
         if (task < NT3) {
           const int t = task / (4 * CS2), half = (task >> 2) % CS2;
           const int r = t * 128 + quad * 32 + lane;
-          const bool valid = r < T::NR2;
           const int s = r / T::ROWS2, q = r - s * T::ROWS2;
-          const int t1 = q / R3, d3 = q - t1 * R3;
+          const int t1 = T::S2O ? (q & 127) >> 2 : q / R3;
+          const int d3 = T::S2O ? 4 * (q >> 7) + (q & 3) : q - t1 * R3;
+          const bool valid = r < T::NR2 && (!T::S2O || (d3 < R3 && t1 < 31));
           if (T::PAIR3) {
             // paired stage-3 row (t1, t2 / 2) = s ROWS3P + t1 R2 / 2 + t2 / 2,
             // K entry d3 (t2 even) or P3OFF / 2 + d3 (t2 odd)
