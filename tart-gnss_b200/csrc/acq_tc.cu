@@ -198,26 +198,26 @@ __device__ __forceinline__ uint32_t bounded_wait(uint64_t* bar, uint32_t phase) 
   return done;
 }
 
-// factorisation Lc = 31 * R2 * R3, the number of code-phase residues
-// (transforms) a CTA runs together, the order of the stage-2 rows (S2O, see
-// T3) and the padding of the K-chunk strides of stages 2 and 3 (16-byte
-// units), chosen for the fewest shared-memory bank conflicts of the
-// transposition stores
+// factorisation Lc = 31 * R2 * R3 in NST stages (Lc = 1023 runs as the two
+// stages 31 x 33, R3 = 1), the number of code-phase residues (transforms) a
+// CTA runs together, the order of the stage-2 rows (S2O, see T3) and the
+// padding of the K-chunk strides of stages 2 and 3 (16-byte units), chosen
+// for the fewest shared-memory bank conflicts of the transposition stores
 template <int M>
 struct Tc3Cfg;
 template <>
 struct Tc3Cfg<1> {
-  static constexpr int R2 = 3, R3 = 11, BC = 4, PAD2 = 1, PAD3 = 1;
+  static constexpr int R2 = 33, R3 = 1, NST = 2, BC = 8, PAD2 = 1, PAD3 = 1;
   static constexpr bool S2O = false;
 };
 template <>
 struct Tc3Cfg<4> {
-  static constexpr int R2 = 12, R3 = 11, BC = 2, PAD2 = 3, PAD3 = 1;
+  static constexpr int R2 = 12, R3 = 11, NST = 3, BC = 2, PAD2 = 3, PAD3 = 1;
   static constexpr bool S2O = false;
 };
 template <>
 struct Tc3Cfg<10> {
-  static constexpr int R2 = 30, R3 = 11, BC = 1, PAD2 = 2, PAD3 = 1;
+  static constexpr int R2 = 30, R3 = 11, NST = 3, BC = 1, PAD2 = 2, PAD3 = 1;
   static constexpr bool S2O = true;
 };
 
@@ -225,13 +225,14 @@ template <int M>
 struct T3 {
   static constexpr int R2 = Tc3Cfg<M>::R2, R3 = Tc3Cfg<M>::R3, BC = Tc3Cfg<M>::BC;
   static constexpr int LC = 1023 * M, OCOLS = 33 * M;
+  static constexpr int NST = Tc3Cfg<M>::NST;
   static_assert(31 * R2 * R3 == LC, "factorisation");
-  static_assert(R3 == 11, "the epilogue reads 22 TMEM columns per transform");
+  static_assert(NST == 2 ? R3 == 1 : R3 == 11, "the epilogue reads 22 TMEM columns per stage-3 transform");
   // With R2 even the stage-3 transforms (t1, 2j) and (t1, 2j + 1) share one
   // operand row: K entries [0, 2 R3) and [P3OFF, P3OFF + 2 R3), against a
   // block-diagonal DFT-R3 matrix whose outputs land in accumulator columns
   // [0, 2 R3) and [P3OFF, P3OFF + 2 R3).
-  static constexpr bool PAIR3 = R2 % 2 == 0;
+  static constexpr bool PAIR3 = NST == 3 && R2 % 2 == 0;
   static constexpr int P3OFF = 24;
   static_assert(2 * R3 <= P3OFF, "paired stage-3 halves");
   // rows (transform columns) of each stage for one residue.  Stage-2 row
@@ -241,22 +242,30 @@ struct T3 {
   static constexpr bool S2O = Tc3Cfg<M>::S2O;
   static_assert(!S2O || R3 <= 12, "S2O: three groups of four d3");
   static constexpr int ROWS1 = R2 * R3, ROWS2 = S2O ? 384 : 31 * R3, ROWS3 = 31 * R2;
-  static constexpr int ROWS3P = PAIR3 ? ROWS3 / 2 : ROWS3;  // stage-3 operand rows
+  static constexpr int ROWS3P = NST == 2 ? 0 : PAIR3 ? ROWS3 / 2 : ROWS3;  // stage-3 operand rows
   static constexpr int NR1 = BC * ROWS1, NR2 = BC * ROWS2, NR3 = BC * ROWS3P;
   static constexpr int TILES1 = (NR1 + 127) / 128, TILES2 = (NR2 + 127) / 128, TILES3 = (NR3 + 127) / 128;
-  static constexpr int K1 = 64, K2 = pad16(2 * R2), K3 = PAIR3 ? 2 * P3OFF : pad16(2 * R3);
-  static_assert(K2 <= 64 && K3 <= 64, "one swizzle atom per matrix row");
+  static constexpr int K1 = 64, K2 = pad16(2 * R2), K3 = NST == 2 ? 0 : PAIR3 ? 2 * P3OFF : pad16(2 * R3);
+  static_assert(K2 <= 128 && K3 <= 64, "matrix rows of at most two (stage 2) or one swizzle atoms");
   static constexpr int N1 = K1, N2 = K2, N3 = K3;
   static constexpr int KB1 = 128, KB2 = K2 > 32 ? 128 : 64, KB3 = K3 > 32 ? 128 : 64;
+  // the stage-2 matrix in atoms of KB2 / 2 K entries; a K step (16 entries)
+  // never straddles two atoms
+  static constexpr int B2_ATOMS = (K2 + KB2 / 2 - 1) / (KB2 / 2), KS_PER_ATOM2 = KB2 / 32;
   // TMEM columns of one chain (its largest stage); two chains per CTA
   static constexpr int CHAIN_COLS = cmax3(TILES1 * N1, TILES2 * N2, TILES3 * N3);
   static_assert(CHAIN_COLS <= kTcTmemCols / 2, "two chains in the CTA's TMEM");
+  // the stage the epilogue reads: its tiles, rows per residue and in all,
+  // complex outputs per row
+  static constexpr int LAST_TILES = NST == 3 ? TILES3 : TILES2;
+  static constexpr int LAST_ROWS = NST == 3 ? ROWS3P : ROWS2, LAST_NR = NST == 3 ? NR3 : NR2;
+  static constexpr int LAST_OUT = NST == 3 ? R3 : R2;
   // data operand regions: rows padded to whole tiles, K chunks lbo apart
   static constexpr int LBO1 = TILES1 * 128 * 16 + 16, LBO2 = TILES2 * 128 * 16 + 16 * Tc3Cfg<M>::PAD2,
                        LBO3 = TILES3 * 128 * 16 + 16 * Tc3Cfg<M>::PAD3;
   static constexpr int A_RAW = cmax3(K1 / 8 * LBO1, K2 / 8 * LBO2, K3 / 8 * LBO3);
   static constexpr int A_BYTES = (A_RAW + 1023) / 1024 * 1024;
-  static constexpr int B1_BYTES = N1 * KB1, B2_BYTES = N2 * KB2, B3_BYTES = N3 * KB3;
+  static constexpr int B1_BYTES = N1 * KB1, B2_BYTES = B2_ATOMS * N2 * KB2, B3_BYTES = N3 * KB3;
   static_assert(B1_BYTES % 1024 == 0 && B2_BYTES % 1024 == 0 && B3_BYTES % 1024 == 0, "1024-byte aligned regions");
   // one (PRN, hypothesis) block of code units: 8 ROWS1 x 16 bytes
   static constexpr int CODE_BYTES = 8 * ROWS1 * 16;
@@ -309,12 +318,13 @@ __device__ __forceinline__ void st_shared_u32(unsigned char* p, uint32_t v) { *r
 // double precision and rounded once to FP16: row n = 2 t + (0 re | 1 im),
 // column k = 2 d + (0 re | 1 im), entries of exp(+2 pi i t d / R); zero
 // outside 2R x 2R.  PAIR repeats the block at row and column offset `off`.
+// `atom` selects the K entries [atom KB / 2, (atom + 1) KB / 2) written here.
 template <int R, int N, int KB, bool PAIR>
-void host_idft_matrix(unsigned char* dst, int off) {
+void host_idft_matrix(unsigned char* dst, int off, int atom = 0) {
   const double kPi = 3.14159265358979323846;
   for (int n = 0; n < N; ++n)
     for (int k = 0; k < KB / 2; ++k) {
-      int nn = n, kk = k;
+      int nn = n, kk = k + atom * (KB / 2);
       bool in = nn < 2 * R && kk < 2 * R;
       if (!in && PAIR && nn >= off && nn < off + 2 * R && kk >= off && kk < off + 2 * R) {
         nn -= off;
@@ -423,7 +433,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   constexpr int CS1 = T::N1 / 32, CS2 = T::N2 >= 32 ? T::N2 / 32 : 1;
   constexpr int W2 = T::N2 >= 32 ? 32 : T::N2;
   constexpr int HALVES3 = T::PAIR3 ? 2 : 1;
-  constexpr int NT2 = T::TILES1 * 4 * CS1, NT3 = T::TILES2 * 4 * CS2, NT4 = T::TILES3 * 4 * HALVES3;
+  constexpr int NT2 = T::TILES1 * 4 * CS1, NT3 = T::TILES2 * 4 * CS2, NT4 = T::LAST_TILES * 4 * HALVES3;
   constexpr int TPW2 = (NT2 + NW - 1) / NW, TPW3 = (NT3 + NW - 1) / NW, TPW4 = (NT4 + NW - 1) / NW;
   // P4 reads TMEM in batches of LB4 tasks: all loads of a batch in flight,
   // one wait
@@ -490,7 +500,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       for (int w = blockIdx.x; w < p.n_items && ok; w += gridDim.x) {
         for (int r = 0; r < n_rounds && ok; ++r) {
 #pragma unroll 1
-          for (int st = 0; st < 3 && ok; ++st) {
+          for (int st = 0; st < T::NST && ok; ++st) {
 #pragma unroll 1
             for (int x = 0; x < 2; ++x) {
               if (!bounded_wait(&s_ready[x], ph_ready[x])) {
@@ -523,7 +533,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
 #pragma unroll
                     for (int ks = 0; ks < T::K2 / 16; ++ks)
                       mma_f16(tm + (uint32_t)(t * T::N2), da + (uint64_t)(t * 128 + 2 * ks * (T::LBO2 >> 4)),
-                              db2 + 2 * ks, idesc_f16(T::N2), ks > 0 ? 1u : 0u);
+                              db2 + (uint64_t)((ks / T::KS_PER_ATOM2) * (T::N2 * T::KB2 >> 4) + 2 * (ks % T::KS_PER_ATOM2)),
+                              idesc_f16(T::N2), ks > 0 ? 1u : 0u);
                 } else {
                   const uint64_t da = desc_kchunks(ax, T::LBO3);
 #pragma unroll
@@ -710,35 +721,66 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
     // reference's tie rule.  Padding rows and residues >= S are skipped.
     auto p4 = [&](int x, int g) -> float {
       const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
+      // accumulator words read per task: 24 for a stage-3 transform (22 used)
+      constexpr int VW = 24;
       float best = 0.f;
-      // tasks in batches of LB4: all loads of a batch in flight, one wait
+      if constexpr (T::NST == 2) {
+        // two-stage split: the stage-2 row (2 R2 words used) in pieces of 48
+        // words, one task per warp at most
+        static_assert(TPW4 == 1, "one epilogue task per warp");
+        const int task = warp;
+        if (task < NT4) {
+          const int r = (task >> 2) * 128 + quad * 32 + lane;
+          const bool valid = r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S;
 #pragma unroll
-      for (int i0 = 0; i0 < TPW4; i0 += LB4) {
-        uint32_t v[LB4][24];
+          for (int c0 = 0; c0 < 2 * T::LAST_OUT; c0 += 48) {
+            uint32_t v[48];
 #pragma unroll
-        for (int i = 0; i < LB4; ++i) {
-          const int task = warp + (i0 + i) * NW;
-          if (i0 + i < TPW4 && task < NT4) {
-            const int t = task / (4 * HALVES3), half = (task >> 2) % HALVES3;
-            tmem_ld_stage3<T::PAIR3>(tb + (uint32_t)(t * T::N3), half, v[i]);
-          }
-        }
-        tmem_wait_ld();
+            for (int c = 0; c < 3; ++c) {
+              uint32_t(&a)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[16 * c]);
+              if (c0 + 16 * c < 2 * T::LAST_OUT) tmem_ld16(tb + (uint32_t)((task >> 2) * T::N2 + c0 + 16 * c), a);
+            }
+            tmem_wait_ld();
+            if (valid) {
 #pragma unroll
-        for (int i = 0; i < LB4; ++i) {
-          const int task = warp + (i0 + i) * NW;
-          if (i0 + i < TPW4 && task < NT4) {
-            const int r = (task / (4 * HALVES3)) * 128 + quad * 32 + lane;
-            if (r < T::NR3 && g * BC + r / T::ROWS3P < S) {
-#pragma unroll
-              for (int h = 0; h < 11; ++h)
-                best = fmaxf(best, fmaf(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h]),
-                                        __uint_as_float(v[i][2 * h + 1]) * __uint_as_float(v[i][2 * h + 1])));
+              for (int h = 0; h < 24; ++h)
+                if (c0 + 2 * h < 2 * T::LAST_OUT)
+                  best = fmaxf(best, fmaf(__uint_as_float(v[2 * h]), __uint_as_float(v[2 * h]),
+                                          __uint_as_float(v[2 * h + 1]) * __uint_as_float(v[2 * h + 1])));
             }
           }
         }
+        return best;
+      } else {
+        // tasks in batches of LB4: all loads of a batch in flight, one wait
+#pragma unroll
+        for (int i0 = 0; i0 < TPW4; i0 += LB4) {
+          uint32_t v[LB4][VW];
+#pragma unroll
+          for (int i = 0; i < LB4; ++i) {
+            const int task = warp + (i0 + i) * NW;
+            if (i0 + i < TPW4 && task < NT4) {
+              const int t = task / (4 * HALVES3), half = (task >> 2) % HALVES3;
+              tmem_ld_stage3<T::PAIR3>(tb + (uint32_t)(t * T::N3), half, v[i]);
+            }
+          }
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < LB4; ++i) {
+            const int task = warp + (i0 + i) * NW;
+            if (i0 + i < TPW4 && task < NT4) {
+              const int r = (task / (4 * HALVES3)) * 128 + quad * 32 + lane;
+              if (r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S) {
+#pragma unroll
+                for (int h = 0; h < T::LAST_OUT; ++h)
+                  best = fmaxf(best, fmaf(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h]),
+                                          __uint_as_float(v[i][2 * h + 1]) * __uint_as_float(v[i][2 * h + 1])));
+              }
+            }
+          }
+        }
+        return best;
       }
-      return best;
     };
 
     for (int w = blockIdx.x; w < p.n_items && !failed; w += gridDim.x) {
@@ -768,7 +810,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       for (int r = 0; r < n_rounds && !failed; ++r) {
         // P2, P3 for chain a then chain b, each after its own MMA stage
 #pragma unroll 1
-        for (int st = 0; st < 2 && !failed; ++st) {
+        for (int st = 0; st < T::NST - 1 && !failed; ++st) {
 #pragma unroll 1
           for (int x = 0; x < 2; ++x) {
             if (!warp_wait(&s_done[x], ph_done[x])) {
@@ -866,8 +908,10 @@ std::vector<unsigned char> build_matrices() {
   using T = T3<M>;
   std::vector<unsigned char> b((size_t)(T::B1_BYTES + T::B2_BYTES + T::B3_BYTES), 0);
   host_idft_matrix<31, T::N1, T::KB1, false>(b.data(), 0);
-  host_idft_matrix<T::R2, T::N2, T::KB2, false>(b.data() + T::B1_BYTES, 0);
-  host_idft_matrix<T::R3, T::N3, T::KB3, T::PAIR3>(b.data() + T::B1_BYTES + T::B2_BYTES, T::P3OFF);
+  for (int a = 0; a < T::B2_ATOMS; ++a)
+    host_idft_matrix<T::R2, T::N2, T::KB2, false>(b.data() + T::B1_BYTES + a * T::N2 * T::KB2, 0, a);
+  if (T::NST == 3)
+    host_idft_matrix<T::R3, T::N3, T::KB3, T::PAIR3>(b.data() + T::B1_BYTES + T::B2_BYTES, T::P3OFF);
   return b;
 }
 
@@ -882,7 +926,7 @@ size_t tc_operand_bytes(const PolyClass& pc, long long n_seq, bool code) {
 double tc_gemm_flops_per_point(int M) {
   // real-embedded DFT-R as a dense 2R x 2R GEMM: 8 R FLOPs per complex point and stage
   switch (M) {
-    case 1: return 8.0 * (31 + Tc3Cfg<1>::R2 + Tc3Cfg<1>::R3);
+    case 1: return 8.0 * (31 + Tc3Cfg<1>::R2);  // two stages
     case 4: return 8.0 * (31 + Tc3Cfg<4>::R2 + Tc3Cfg<4>::R3);
     case 10: return 8.0 * (31 + Tc3Cfg<10>::R2 + Tc3Cfg<10>::R3);
   }
