@@ -335,7 +335,7 @@ def main():
             else:
                 peak, src = 1400.0, "of fallback: sustained dense bf16 figure of the profiling recipe"
             bound = "tensor"
-            note = ("algorithmic FLOPs: the three DFT stages as dense real 2R x 2R GEMMs, 8 (31 + R2 + R3) "
+            note = ("algorithmic FLOPs: the DFT stages as dense real 2R x 2R GEMMs, 8 x (sum of the radices) "
                     "per complex output point")
         else:
             peak = fp32_peak_tflops(sm_mhz)

@@ -1,9 +1,9 @@
 // Tensor-core correlator (sm_100a, tcgen05): reduced-precision search.
 //
 // The inverse transform of every product Z * conj(C) (length Lc = 31 R2 R3,
-// (R2, R3) = (3, 11), (12, 11), (30, 11) for Lc = 1023, 4092, 10230) is a
-// Good-Thomas prime-factor transform whose three stages -- DFT-31, DFT-R2,
-// DFT-R3 -- all run on the 5th-generation tensor cores as GEMMs:
+// (R2, R3) = (33, 1), (12, 11), (30, 11) for Lc = 1023, 4092, 10230) is a
+// Good-Thomas prime-factor transform whose stages -- DFT-31, DFT-R2 and, for
+// R3 > 1, DFT-R3 -- all run on the 5th-generation tensor cores as GEMMs:
 //
 //   stage i:  D_i[row][n] = sum_k A_i[row][k] * B_i[n][k]
 //     A_i   = data, one row per transform column, K = 2 R_i halves
