@@ -110,7 +110,7 @@ __device__ __forceinline__ float2 wipe(const FrontParams& p, int row, int n, dou
   }
   const float ph = __double2float_rn(ph_d);           // (p * freq) as f32
   float sn, cs;
-  sincosf(ph, &sn, &cs);
+  sincos_phase(ph, &sn, &cs);
   return make_float2(cs * s, sn * s);
 }
 

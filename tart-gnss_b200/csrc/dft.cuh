@@ -29,6 +29,26 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 
+// sin and cos of the f32 carrier phase ph (the reference's `(p * f) as f32`,
+// correlate.rs:110-115), rounded to f32 from double-precision values: ph / 2pi
+// = n + t with 1/2pi as a two-term double (the product's rounding error
+// recovered with an FMA), |t| <= 1/2, then sincospi(2 t) in double.  The
+// reduced turn is exact to ~1e-20, so the f32 results are the correctly
+// rounded sin / cos except within ~1e-16 of a rounding boundary, and the cost
+// does not grow with |ph| (carrier phases reach ~5e5 rad over 20 ms).
+__device__ __forceinline__ void sincos_phase(float ph, float* sn, float* cs) {
+  constexpr double kInv2PiHi = 0x1.45f306dc9c883p-3;   // 1/2pi rounded to double
+  constexpr double kInv2PiLo = -0x1.6b01ec5417056p-57;  // 1/2pi - kInv2PiHi
+  const double x = (double)ph;
+  const double th = x * kInv2PiHi;
+  const double tl = fma(x, kInv2PiHi, -th) + x * kInv2PiLo;
+  const double t = (th - rint(th)) + tl;
+  double s, c;
+  sincospi(2.0 * t, &s, &c);
+  *sn = (float)s;
+  *cs = (float)c;
+}
+
 template <int R> __device__ __forceinline__ float kcos(int m);
 template <int R> __device__ __forceinline__ float ksin(int m);
 template <> __device__ __forceinline__ float kcos<3>(int m) { return kCos3[m]; }

@@ -186,7 +186,7 @@ __global__ void wipe_kernel(const float* __restrict__ sig, const double* __restr
   const int b = (int)(i / N), n = (int)(i - (long long)b * N);
   const float ph = __double2float_rn(pp[n] * fc[b]);
   float sn, cs;
-  sincosf(ph, &sn, &cs);
+  sincos_phase(ph, &sn, &cs);
   const float s = sig[n];
   X[i] = make_float2(cs * s, sn * s);
 }

@@ -41,7 +41,7 @@ __device__ __forceinline__ float2 wipe_bits(const NcFrontParams& p, int row, lon
   const float s = (float)(v - __ldg(p.src.mean + row));
   const float ph = __double2float_rn((p.src.pc * (double)n) * f);
   float sn, cs;
-  sincosf(ph, &sn, &cs);
+  sincos_phase(ph, &sn, &cs);
   return make_float2(cs * s, sn * s);
 }
 
