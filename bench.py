@@ -77,6 +77,38 @@ def synth_observation(seed, n_ant=N_ANT, n_samples=SAMPLES, chunk=163680):
     return bits, sats
 
 
+def synth_weak_observation(seed, n_ant=N_ANT, n_samples=SAMPLES, n_sats=8, chunk=163680):
+    """Weak-signal recording: n_sats GPS C/A satellites (PRNs 1-32) at C/N0
+    uniform 28-36 dB-Hz, code phase uniform, Doppler uniform +-4 kHz, random
+    +-1 navigation bits of 20 ms with a random bit-edge offset, per-antenna
+    carrier phases, unit Gaussian noise, sign-quantised.  Returns (bits,
+    satellites)."""
+    import tga
+    rng = np.random.default_rng(seed)
+    P = int(FS / 1000.0)
+    sats = []
+    for prn in rng.choice(np.arange(1, 33), size=n_sats, replace=False):
+        code = tga.code_resampled(0, int(prn), float(P), P).astype(np.float32)
+        sats.append(dict(prn=int(prn), code=code, delay=int(rng.integers(0, P)), dop=float(rng.uniform(-4000, 4000)),
+                         cn0=float(rng.uniform(28, 36)), edge=int(rng.integers(0, 20)),
+                         bits=rng.choice([-1.0, 1.0], size=n_samples // (20 * P) + 3).astype(np.float32)))
+    phase = np.exp(1j * rng.uniform(0, 2 * np.pi, size=(n_ant, len(sats)))).astype(np.complex64)
+    bits = np.empty((n_ant, n_samples // 8), np.uint8)
+    for t0 in range(0, n_samples, chunk):
+        n = min(chunk, n_samples - t0)
+        t = np.arange(t0, t0 + n)
+        U = np.empty((len(sats), n), np.complex64)
+        for k, s in enumerate(sats):
+            amp = 2.0 * math.sqrt(10.0 ** (s["cn0"] / 10.0) / FS)
+            idx = t + s["delay"]
+            chip = s["code"][idx % P] * s["bits"][(idx // P + s["edge"]) // 20]
+            ph = (2 * np.pi * ((4.092e6 + s["dop"]) / FS) * t) % (2 * np.pi)
+            U[k] = (amp * chip) * np.exp(1j * ph).astype(np.complex64)
+        v = (phase @ U).real + rng.standard_normal((n_ant, n), dtype=np.float32)
+        bits[:, t0 // 8:(t0 + n) // 8] = np.packbits(v >= 0.0, axis=1)
+    return bits, sats
+
+
 def synth_fine_observation(seed, n_ant=24, n=163680, sigma_chips=0.1):
     """Band-limited 1-bit recording for the fine-acquisition measurement: 6
     GPS C/A and 6 Galileo E1-C satellites at 45 dB-Hz, continuous delays and
@@ -365,34 +397,79 @@ def main():
         other = (oprec,) + measure(oprec)
     weak = None
     if not args.no_weak:
-        # weak-signal search on the same recording: GPS C/A PRNs 1-32, 10 ms
-        # coherent blocks x 10 (100 ms), 201 bins of 50 Hz; cells count
-        # (antenna, PRN, bin, code phase, block)
-        host = pinned.numpy()
+        # weak-signal search: GPS C/A PRNs 1-32, 10 ms coherent blocks x 10
+        # (100 ms), 201 bins of 50 Hz, on its own recording (8 satellites at
+        # 28-36 dB-Hz with navigation-bit transitions); both arithmetics, end
+        # to end through tga_search_noncoherent; cells count (antenna, PRN,
+        # bin, code phase, block)
+        wbits, wsats = synth_weak_observation(SEED + 1000 + rank, n_ant=n_ant)
+        whost = torch.from_numpy(wbits).pin_memory().numpy()
         kw = dict(prns=list(range(1, 33)), bin_step_hz=50.0, n_bins=201, coherent_periods=10, blocks=10)
-        for _ in range(args.warmup):
-            ctx.search_noncoherent(host, FS, tga.GPS, **kw)
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        wt = []
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(1.0)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            ctx.search_noncoherent(host, FS, tga.GPS, **kw)
-            wt.append(time.perf_counter() - t0)
-        w_s = statistics.mean(wt)
-        if world > 1:
-            t = torch.tensor([w_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            w_s = float(t.item())
         wcells = n_ant * 32 * 201 * 16368.0 * 10
-        weak = {"workload": "GPS C/A PRNs 1-32 x %d ant, 10 ms coherent x 10 blocks (100 ms), 201 x 50 Hz bins, "
-                            "FP32 non-coherent search through tga_search_noncoherent (host bits, end to end)" % n_ant,
-                "value": wcells * world / w_s, "unit": "cell-blocks/s", "ms_per_step": w_s * 1e3,
-                "cells_per_step_per_gpu": wcells}
+        runs = {}
+        for prec in (args.precision, "fp32" if args.precision == "fp16tc" else "fp16tc"):
+            ctx.set_precision(prec_id[prec])
+            for _ in range(args.warmup):
+                wout = ctx.search_noncoherent(whost, FS, tga.GPS, **kw)
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            wt = []
+            for _ in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(1.0)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                wout = ctx.search_noncoherent(whost, FS, tga.GPS, **kw)
+                wt.append(time.perf_counter() - t0)
+            w_s = statistics.mean(wt)
+            if world > 1:
+                t = torch.tensor([w_s], device="cuda", dtype=torch.float64)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                w_s = float(t.item())
+            # one more, untimed call with per-kernel events for the breakdown
+            lib.tga_set_profiling(ctx._h, 1)
+            ctx.search_noncoherent(whost, FS, tga.GPS, **kw)
+            kt = {k: v[0] for k, v in kernel_times().items()}
+            lib.tga_set_profiling(ctx._h, 0)
+            runs[prec] = (w_s, wout, kt)
+        ctx.set_precision(prec_id[args.precision])
+        dtype_name = {"fp32": "f32", "fp16tc": "f16-tc+f32"}
+        truth = {s["prn"]: s for s in wsats}
+        thr = 1.5  # detection: summed peak power > 1.5 x the second peak
+
+        def detect(out):
+            det = out["power"] > thr * out["second_power"]
+            hit = np.zeros(len(out), bool)
+            for i, c in enumerate(out):
+                s = truth.get(int(c["prn"]))
+                if s is not None:
+                    d = abs(int(c["best_codephase"]) - (16368 - s["delay"]) % 16368)
+                    hit[i] = min(d, 16368 - d) <= 1 and abs(c["frequency"] - s["dop"]) <= 50.0
+            present = np.array([int(c["prn"]) in truth for c in out])
+            return det, {"p_detect": float(np.mean(det[present] & hit[present])),
+                         "p_false_alarm": float(np.mean(det[~present])),
+                         "present_cells": int(present.sum()), "absent_cells": int((~present).sum())}
+
+        w_head, out_head, kt_head = runs[args.precision]
+        other_prec = "fp32" if args.precision == "fp16tc" else "fp16tc"
+        w_other, out_other, _ = runs[other_prec]
+        det_h, stats_h = detect(out_head)
+        det_o, stats_o = detect(out_other)
+        same_rows = bool(np.array_equal(out_head["best_codephase"][det_h], out_other["best_codephase"][det_o])
+                         and np.array_equal(out_head["best_freq_idx"][det_h], out_other["best_freq_idx"][det_o]))
+        weak = {"workload": "GPS C/A PRNs 1-32 x %d ant, 10 ms coherent x 10 blocks (100 ms), 201 x 50 Hz bins; "
+                            "8 satellites at C/N0 28-36 dB-Hz with navigation-bit transitions; "
+                            "tga_search_noncoherent from pinned host bits (end to end)" % n_ant,
+                "arithmetic": dtype_name[args.precision], "value": wcells * world / w_head,
+                "unit": "cell-blocks/s", "ms_per_step": w_head * 1e3, "cells_per_step_per_gpu": wcells,
+                "detection": dict(stats_h, threshold="power > %.1f x second_power, code phase within 1 sample "
+                                                     "and frequency within 50 Hz of the truth" % thr),
+                "kernels_ms": {k: v for k, v in kt_head.items() if k.startswith("nc_")},
+                "compare": {"arithmetic": dtype_name[other_prec], "value": wcells * world / w_other,
+                            "ms_per_step": w_other * 1e3, "speedup_of_weak": w_other / w_head,
+                            "detection": stats_o,
+                            "same_detections": bool(np.array_equal(det_h, det_o)) and same_rows}}
     clocks = clk.stop()
     sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
     value = cells * world / (ms_step / 1e3)

@@ -118,6 +118,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
       : "memory");
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
@@ -221,9 +230,14 @@ struct Tc3Cfg<10> {
   static constexpr bool S2O = true;
 };
 
-template <int M>
+// residues per work item of the non-coherent search (NCB): fewer than the
+// drop-in's, so that each chain keeps room in its 256 TMEM columns for the
+// |y|^2 accumulators (Lc = 1023 only)
+constexpr int kNcBC = 4;
+
+template <int M, bool NCB = false>
 struct T3 {
-  static constexpr int R2 = Tc3Cfg<M>::R2, R3 = Tc3Cfg<M>::R3, BC = Tc3Cfg<M>::BC;
+  static constexpr int R2 = Tc3Cfg<M>::R2, R3 = Tc3Cfg<M>::R3, BC = NCB ? kNcBC : Tc3Cfg<M>::BC;
   static constexpr int LC = 1023 * M, OCOLS = 33 * M;
   static constexpr int NST = Tc3Cfg<M>::NST;
   static_assert(31 * R2 * R3 == LC, "factorisation");
@@ -260,6 +274,12 @@ struct T3 {
   static constexpr int LAST_TILES = NST == 3 ? TILES3 : TILES2;
   static constexpr int LAST_ROWS = NST == 3 ? ROWS3P : ROWS2, LAST_NR = NST == 3 ? NR3 : NR2;
   static constexpr int LAST_OUT = NST == 3 ? R3 : R2;
+  // non-coherent search: per chain, |y|^2 sums over the blocks of the 33
+  // stage-2 outputs of every row in three chunks of 11, each in 16 TMEM
+  // columns from ACC0
+  static constexpr int ACC0 = CHAIN_COLS;
+  static_assert(!NCB || (M == 1 && NST == 2 && LAST_TILES == 1 && ACC0 % 16 == 0 && ACC0 + 48 <= kTcTmemCols / 2),
+                "non-coherent accumulators");
   // data operand regions: rows padded to whole tiles, K chunks lbo apart
   static constexpr int LBO1 = TILES1 * 128 * 16 + 16, LBO2 = TILES2 * 128 * 16 + 16 * Tc3Cfg<M>::PAD2,
                        LBO3 = TILES3 * 128 * 16 + 16 * Tc3Cfg<M>::PAD3;
@@ -386,9 +406,10 @@ struct Tc3Params {
   const uint4* d16;   // [n_prn][2] sequences of 8*ROWS1 units
   unsigned long long* keys;
   int* err;
-  int n_items;  // n_ab * 2 * groups: (row, residue group) work items
+  int n_items;  // n_ab * groups: (row, residue group) work items
   int groups;   // ceil(S / BC)
   int n_prn, S;
+  int B;        // coherent blocks summed non-coherently (1: the drop-in search)
   int skip_commit;  // test hook: see TGA_TEST_TC_SKIP_COMMIT
 };
 
@@ -424,9 +445,15 @@ __device__ __forceinline__ void tmem_ld_stage3(uint32_t taddr, int half, uint32_
 // (tcgen05.commit) and s_code[x] (bulk copy).  A tcgen05.mma holds its
 // thread until the tensor cores take it, so the issuing has a warp of its
 // own.  Every wait is bounded.
-template <int M>
+//
+// NCB (non-coherent search, Lc = 1023): the row is an (antenna, bin) and
+// every PRN pair runs through B coherent blocks; the chains keep per-lane
+// |y|^2 sums in TMEM and take the row maximum after the last block.  The Z
+// of the next block is loaded into the registers while the current block's
+// transform runs.
+template <int M, bool NCB>
 __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
-  using T = T3<M>;
+  using T = T3<M, NCB>;
   constexpr int NW = kSimtWarps, NTS = kSimtThreads, R2 = T::R2, R3 = T::R3, BC = T::BC, U = T::U;
   static_assert(NW % 4 == 0, "a warp task keeps its TMEM lane quadrant");
   // TMEM columns read by one warp task in the transposition phases
@@ -449,7 +476,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   unsigned char* B3 = B2 + T::B2_BYTES;
   unsigned char* CODE0 = B3 + T::B3_BYTES;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quad = warp & 3;
-  const int S = p.S, n_rounds = (p.n_prn + 1) / 2;
+  const int S = p.S, n_rounds = (p.n_prn + 1) / 2, B = NCB ? p.B : 1;
 
   if (warp == 0) {
     tmem_alloc(&s_tmem, kTcTmemCols);
@@ -487,7 +514,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       bool ok = true;
       // code block of chain x for round r of work item w
       auto fetch = [&](int x, int w, int r) {
-        const int hyp = (w / p.groups) & 1;
+        const int hyp = NCB ? 0 : (w / p.groups) & 1;
         const uint4* src = p.d16 + ((size_t)prn_of(r, x) * 2 + hyp) * 8 * T::ROWS1;
         mbar_arrive_expect_tx(&s_code[x], (uint32_t)T::CODE_BYTES);
         bulk_g2s(smem_addr(CODE0 + x * T::CODE_REGION), src, (uint32_t)T::CODE_BYTES, &s_code[x]);
@@ -499,6 +526,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       }
       for (int w = blockIdx.x; w < p.n_items && ok; w += gridDim.x) {
         for (int r = 0; r < n_rounds && ok; ++r) {
+#pragma unroll 1
+         for (int b = 0; b < B && ok; ++b) {
 #pragma unroll 1
           for (int st = 0; st < T::NST && ok; ++st) {
 #pragma unroll 1
@@ -547,8 +576,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
                 mma_commit(&s_done[x]);
                 ++commits[x];
               }
-              // chain x has read its code block: fetch its next one
-              if (st == 0) {
+              // chain x has read its code block for the last time: fetch its next one
+              if (st == 0 && b == B - 1) {
                 if (r + 1 < n_rounds)
                   fetch(x, w, r + 1);
                 else if (w + (int)gridDim.x < p.n_items)
@@ -556,6 +585,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
               }
             }
           }
+         }
         }
       }
       // drain: the last commit and the last bulk copy of each chain (after a
@@ -783,31 +813,90 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       }
     };
 
+    // ---- P4 of the non-coherent search: add block b's |y|^2 to the chain's
+    // TMEM sums; after the last block, the row maximum of the sums ----
+    // Warp w takes lane quadrant w % 4 and outputs [11 c, 11 c + 11), c = w / 4,
+    // of the single stage-2 tile.
+    auto p4_nc = [&](int x, int g, int b) -> float {
+      static_assert(!NCB || NW == 12, "three output chunks of four quadrants");
+      const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
+      const int c = warp >> 2;
+      const int s0 = c == 0 ? 0 : (c == 1 ? 16 : 40);  // 8-column aligned start covering [22 c, 22 c + 22)
+      const uint32_t tacc = tb + (uint32_t)(T::ACC0 + 16 * c);
+      uint32_t v[32], a[16];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        uint32_t(&q)[8] = *reinterpret_cast<uint32_t(*)[8]>(&v[8 * i]);
+        tmem_ld8(tb + (uint32_t)(s0 + 8 * i), q);
+      }
+      if (b > 0) tmem_ld16(tacc, a);
+      tmem_wait_ld();
+      float best = 0.f;
+      const int r = quad * 32 + lane;
+      const bool valid = r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S;
+#pragma unroll
+      for (int h = 0; h < 11; ++h) {
+        // the chunk starts 22 c - s0 = 0, 6 or 4 words into v
+        float re, im;
+        if (c == 0) {
+          re = __uint_as_float(v[2 * h]);
+          im = __uint_as_float(v[2 * h + 1]);
+        } else if (c == 1) {
+          re = __uint_as_float(v[6 + 2 * h]);
+          im = __uint_as_float(v[6 + 2 * h + 1]);
+        } else {
+          re = __uint_as_float(v[4 + 2 * h]);
+          im = __uint_as_float(v[4 + 2 * h + 1]);
+        }
+        const float pw = fmaf(re, re, im * im) + (b > 0 ? __uint_as_float(a[h]) : 0.f);
+        a[h] = __float_as_uint(pw);
+        best = fmaxf(best, pw);
+      }
+      if (b + 1 < B) {
+        tmem_st16(tacc, a);
+        tmem_wait_st();
+        return 0.f;
+      }
+      return valid ? best : 0.f;
+    };
+
     for (int w = blockIdx.x; w < p.n_items && !failed; w += gridDim.x) {
       const int ab_h = w / p.groups, g = w - ab_h * p.groups;
-      // this item's Z units, kept in registers for every PRN
+      // this item's Z units of block blk, in registers
       uint4 zr[U];
+      auto load_z = [&](int blk) {
 #pragma unroll
-      for (int k = 0; k < U; ++k) {
-        const int e = tid + k * NTS;
-        zr[k] = make_uint4(0u, 0u, 0u, 0u);
-        if (e < T::UNITS) {
-          const int j = e / T::NR1, r = e - j * T::NR1;
-          const int s = r / T::ROWS1, u = r - s * T::ROWS1;
-          const int rho = g * BC + s;
-          if (rho < S) zr[k] = __ldcs(p.z16 + (((size_t)ab_h * S + rho) * 8 + j) * T::ROWS1 + u);
+        for (int k = 0; k < U; ++k) {
+          const int e = tid + k * NTS;
+          zr[k] = make_uint4(0u, 0u, 0u, 0u);
+          if (e < T::UNITS) {
+            const int j = e / T::NR1, r = e - j * T::NR1;
+            const int s = r / T::ROWS1, u = r - s * T::ROWS1;
+            const int rho = g * BC + s;
+            if (rho < S)
+              zr[k] = __ldcs(p.z16 + ((((size_t)ab_h * B + blk) * S + rho) * 8 + j) * T::ROWS1 + u);
+          }
         }
-      }
-      // chain x: wait for its code block, form its products, hand over
-      auto products = [&](int x) -> bool {
-        if (!warp_wait(&s_code[x], ph_code[x])) return false;
-        ph_code[x] ^= 1u;
+      };
+      load_z(0);
+      // chain x: wait for its code block when a new PRN starts (the blocks of
+      // one PRN share it), form the products, hand over
+      auto products = [&](int x, bool new_code) -> bool {
+        if (new_code) {
+          if (!warp_wait(&s_code[x], ph_code[x])) return false;
+          ph_code[x] ^= 1u;
+        }
         p1(zr, A0 + x * T::A_BYTES, CODE0 + x * T::CODE_REGION);
         signal(x);
         return true;
       };
-      for (int x = 0; x < 2 && !failed; ++x) failed = !products(x);
-      for (int r = 0; r < n_rounds && !failed; ++r) {
+      for (int x = 0; x < 2 && !failed; ++x) failed = !products(x, true);
+      for (int r = 0; r < n_rounds && !failed; ++r)
+       for (int b = 0; b < B && !failed; ++b) {
+        const bool more = b + 1 < B || r + 1 < n_rounds;  // a next block of this item follows
+        // both chains have formed this block's products: bring the next
+        // block's Z into the registers while the transforms run
+        if (NCB && more) load_z(b + 1 < B ? b + 1 : 0);
         // P2, P3 for chain a then chain b, each after its own MMA stage
 #pragma unroll 1
         for (int st = 0; st < T::NST - 1 && !failed; ++st) {
@@ -837,12 +926,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
           ph_done[x] ^= 1u;
           tc_fence_after();
           // non-negative floats order like their bit patterns
-          const unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(p4(x, g)));
+          float pmax;
+          if constexpr (NCB)
+            pmax = p4_nc(x, g, b);
+          else
+            pmax = p4(x, g);
+          const unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(pmax));
           if (lane == 0 && bits != 0u)
             atomicMax(p.keys + (size_t)ab_h * p.n_prn + prn_of(r, x), (unsigned long long)bits << 32);
-          if (r + 1 < n_rounds) failed = !products(x);
+          if (more) failed = !products(x, b + 1 == B);
         }
-      }
+       }
     }
     if (failed && lane == 0) atomicExch(p.err, 1);
   }
@@ -853,11 +947,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   if (warp == 0) tmem_dealloc(tmem_base, kTcTmemCols);
 }
 
-template <int M>
-cudaError_t run_tc3(const PolyClass& pc, const SearchDims& dims, const void* d_bmat, const void* d_z16,
+template <int M, bool NCB>
+cudaError_t run_tc3(const PolyClass& pc, const SearchDims& dims, int B, const void* d_bmat, const void* d_z16,
                     const void* d_d16, unsigned long long* d_keys, int* d_err, int test_flags, int num_sms,
                     cudaStream_t st) {
-  using T = T3<M>;
+  using T = T3<M, NCB>;
   Tc3Params p = {};
   p.skip_commit = test_flags & 1;
   p.bmat = static_cast<const uint4*>(d_bmat);
@@ -868,8 +962,9 @@ cudaError_t run_tc3(const PolyClass& pc, const SearchDims& dims, const void* d_b
   p.n_prn = dims.n_prn;
   p.S = pc.S;
   p.groups = (pc.S + T::BC - 1) / T::BC;
-  p.n_items = dims.n_ant * dims.nb * 2 * p.groups;
-  auto kern = pfa_tc3_kernel<M>;
+  p.B = NCB ? B : 1;
+  p.n_items = dims.n_ant * dims.nb * (NCB ? 1 : 2) * p.groups;
+  auto kern = pfa_tc3_kernel<M, NCB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, T::SMEM);
   if (e != cudaSuccess) return e;
   // one CTA per SM: T::SMEM is above half of the SM's shared memory, so the
@@ -959,11 +1054,18 @@ cudaError_t launch_correlate_tc(const PolyClass& pc, const SearchDims& dims, con
                                 const void* d_d16, unsigned long long* d_keys, int* d_err, int test_flags,
                                 int num_sms, cudaStream_t st) {
   switch (pc.M) {
-    case 1: return run_tc3<1>(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
-    case 4: return run_tc3<4>(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
-    case 10: return run_tc3<10>(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
+    case 1: return run_tc3<1, false>(pc, dims, 1, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
+    case 4: return run_tc3<4, false>(pc, dims, 1, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
+    case 10: return run_tc3<10, false>(pc, dims, 1, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
   }
   return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_correlate_tc_nc(const PolyClass& pc, const SearchDims& dims, int B, const void* d_bmat,
+                                   const void* d_z16, const void* d_d16, unsigned long long* d_keys, int* d_err,
+                                   int test_flags, int num_sms, cudaStream_t st) {
+  if (pc.M != 1 || B < 1) return cudaErrorInvalidValue;
+  return run_tc3<1, true>(pc, dims, B, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
 }
 
 }  // namespace tga

@@ -103,6 +103,12 @@ cudaError_t launch_tc_pack(const PolyClass& pc, const float2* d_src, long long n
 cudaError_t launch_correlate_tc(const PolyClass& pc, const SearchDims& dims, const void* d_bmat, const void* d_z16,
                                 const void* d_d16, unsigned long long* d_keys, int* d_err, int test_flags,
                                 int num_sms, cudaStream_t st);
+// the non-coherent search (Lc = 1023): per (antenna, bin) row and PRN the
+// row maximum of |y|^2 summed over B coherent blocks; z16 holds the FP16 Z of
+// [n_ant * nb][B][S] sequences
+cudaError_t launch_correlate_tc_nc(const PolyClass& pc, const SearchDims& dims, int B, const void* d_bmat,
+                                   const void* d_z16, const void* d_d16, unsigned long long* d_keys, int* d_err,
+                                   int test_flags, int num_sms, cudaStream_t st);
 cudaError_t launch_reduce_bins(const SearchDims& dims, const unsigned long long* d_keys,
                                BestRow* d_best, cudaStream_t st);
 cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
@@ -162,6 +168,10 @@ cudaError_t launch_nc_correlate(const PolyClass& pc, const SearchDims& dims, int
                                 const float2* d_D, unsigned long long* d_keys, int num_sms, cudaStream_t st);
 cudaError_t launch_nc_reduce(const SearchDims& dims, const unsigned long long* d_keys, BestRow* d_best,
                              cudaStream_t st);
+// the selected row of every (antenna, PRN) re-evaluated in FP32 after a
+// reduced-precision non-coherent search (peak and lag replaced)
+cudaError_t launch_nc_refine(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
+                             const float2* d_D, BestRow* d_best, int num_sms, cudaStream_t st);
 cudaError_t launch_nc_second(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
                              const float2* d_D, BestRow* d_best, int chip_width, int num_sms, cudaStream_t st);
 

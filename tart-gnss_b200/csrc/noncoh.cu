@@ -79,14 +79,16 @@ __global__ void __launch_bounds__(256) nc_frontend_kernel(NcFrontParams p) {
   }
 }
 
-enum NcMode { NC_PEAK = 0, NC_SECOND = 1 };
+// NC_REFINE: the selected row of each (antenna, PRN) of a reduced-precision
+// search again in FP32: its peak and lag replace the row's
+enum NcMode { NC_PEAK = 0, NC_SECOND = 1, NC_REFINE = 2 };
 
 struct NcParams {
   const float2* z;  // [n_ab][B][S][Lc], digit layout
   const float2* D;  // [n_prn][2][Lc]; the cyclic spectrum (index 0) is used
   int n_items, n_prn, S, P, B, chip_width;
   unsigned long long* keys;  // NC_PEAK: [n_ab][n_prn]
-  BestRow* best;             // NC_SECOND: [n_ant][n_prn]
+  BestRow* best;             // NC_SECOND, NC_REFINE: [n_ant][n_prn]
 };
 
 template <int M, int BC, int NT, int MODE>
@@ -100,6 +102,7 @@ __global__ void __launch_bounds__(NT, 1) nc_correlate_kernel(NcParams p) {
   const int tid = threadIdx.x, S = p.S;
   const int groups = (S + BC - 1) / BC;
   for (int w = blockIdx.x; w < p.n_items; w += gridDim.x) {
+    constexpr bool ARGMAX = MODE == NC_PEAK || MODE == NC_REFINE;
     int ab, prn, tau_star = 0;
     if (MODE == NC_PEAK) {
       ab = w / p.n_prn;
@@ -181,7 +184,7 @@ __global__ void __launch_bounds__(NT, 1) nc_correlate_kernel(NcParams p) {
         const int c = rem / 33, b = rem - c * 33;
         const int lag = q + S * G::natural(a, b, c);
         const float pw = acc[i];
-        if (MODE == NC_PEAK) {
+        if (ARGMAX) {
           const unsigned long long k = ((unsigned long long)__float_as_uint(pw) << 32) | (unsigned)lag;
           kbest = k > kbest ? k : kbest;  // ties: the later lag (Iterator::max_by)
         } else {
@@ -192,7 +195,7 @@ __global__ void __launch_bounds__(NT, 1) nc_correlate_kernel(NcParams p) {
       }
       __syncthreads();
     }
-    if (MODE == NC_PEAK) {
+    if (ARGMAX) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long other = __shfl_xor_sync(0xffffffffu, kbest, o);
@@ -200,7 +203,14 @@ __global__ void __launch_bounds__(NT, 1) nc_correlate_kernel(NcParams p) {
       }
       if ((tid & 31) == 0) atomicMax(&s_key, kbest);
       __syncthreads();
-      if (tid == 0) p.keys[w] = s_key;
+      if (tid == 0) {
+        if (MODE == NC_PEAK) {
+          p.keys[w] = s_key;
+        } else {
+          p.best[w].tau = (int)(unsigned)(s_key & 0xffffffffull);
+          p.best[w].p = __uint_as_float((unsigned)(s_key >> 32));
+        }
+      }
     } else {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) pbest = fmaxf(pbest, __shfl_xor_sync(0xffffffffu, pbest, o));
@@ -347,6 +357,20 @@ cudaError_t launch_nc_second(const PolyClass& pc, const SearchDims& dims, int B,
   p.chip_width = chip_width;
   p.n_items = dims.n_ant * dims.n_prn;
   return dispatch_nc<NC_SECOND>(pc.M, p, num_sms, st);
+}
+
+cudaError_t launch_nc_refine(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
+                             const float2* d_D, BestRow* d_best, int num_sms, cudaStream_t st) {
+  NcParams p = {};
+  p.z = d_z;
+  p.D = d_D;
+  p.best = d_best;
+  p.n_prn = dims.n_prn;
+  p.S = pc.S;
+  p.P = pc.P;
+  p.B = B;
+  p.n_items = dims.n_ant * dims.n_prn;
+  return dispatch_nc<NC_REFINE>(pc.M, p, num_sms, st);
 }
 
 }  // namespace tga

@@ -1553,9 +1553,43 @@ int tga_search_noncoherent(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant_tot
           [&] { return launch_nc_frontend(src, dims, pc, opt->coherent_periods, B, opt->start, d_z, st); });
     timed(ctx, "nc_forward_z", (double)n_seq * pc.Lc * tf,
           [&] { return launch_forward_seqs(pc, n_seq, d_z, ctx->num_sms, st); });
-    timed(ctx, "nc_correlate", (double)n_ant * nb * n_prn * B * pc.P * (tf + 9.0),
-          [&] { return launch_nc_correlate(pc, dims, B, d_z, d_D, d_keys, ctx->num_sms, st); });
+    // the tensor-core path covers Lc = 1023 (GPS, SBAS, QZSS C/A); other code
+    // lengths run the FP32 search whatever the precision
+    const bool tc = ctx->precision == TGA_PRECISION_FP16_TC && pc.M == 1;
+    if (tc) {
+      int* d_err = (int*)ctx->buf("tc.err", sizeof(int));
+      void* d_z16 = ctx->buf("nc.z16", tc_operand_bytes(pc, n_seq, false));
+      void* d_d16 = ctx->buf("nc.d16", tc_operand_bytes(pc, (long long)n_prn * 2, true));
+      const std::string mat_name = "tcmat." + std::to_string(pc.M);
+      void* d_bmat = nullptr;
+      if (!ctx->uploaded.count(mat_name)) {
+        const std::vector<unsigned char> mats = tc_dft_matrices(pc.M);
+        d_bmat = ctx->buf(mat_name, mats.size());
+        CK(cudaMemcpy(d_bmat, mats.data(), mats.size(), cudaMemcpyHostToDevice));
+        ctx->uploaded[mat_name] = {};
+      } else {
+        d_bmat = ctx->buf(mat_name, 0);
+      }
+      timed(ctx, "nc_tc_pack", 0.0, [&] {
+        cudaError_t e = launch_tc_pack(pc, d_z, n_seq, false, d_z16, ctx->num_sms, st);
+        if (e == cudaSuccess) e = launch_tc_pack(pc, d_D, (long long)n_prn * 2, true, d_d16, ctx->num_sms, st);
+        return e;
+      });
+      CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+      CK(cudaMemsetAsync(d_keys, 0, (size_t)n_ant * nb * n_prn * sizeof(unsigned long long), st));
+      timed(ctx, "nc_correlate_tc", (double)n_ant * nb * n_prn * B * pc.P * tc_gemm_flops_per_point(pc.M), [&] {
+        return launch_correlate_tc_nc(pc, dims, B, d_bmat, d_z16, d_d16, d_keys, d_err, ctx->test_flags,
+                                      ctx->num_sms, st);
+      });
+      ctx->tc_err_pending = d_err;
+    } else {
+      timed(ctx, "nc_correlate", (double)n_ant * nb * n_prn * B * pc.P * (tf + 9.0),
+            [&] { return launch_nc_correlate(pc, dims, B, d_z, d_D, d_keys, ctx->num_sms, st); });
+    }
     timed(ctx, "nc_reduce", 0.0, [&] { return launch_nc_reduce(dims, d_keys, d_best, st); });
+    if (tc)
+      timed(ctx, "nc_refine", (double)n_ant * n_prn * B * pc.P * (tf + 9.0),
+            [&] { return launch_nc_refine(pc, dims, B, d_z, d_D, d_best, ctx->num_sms, st); });
     timed(ctx, "nc_second", (double)n_ant * n_prn * B * pc.P * (tf + 9.0), [&] {
       return launch_nc_second(pc, dims, B, d_z, d_D, d_best, chip_width_of(fs), ctx->num_sms, st);
     });
@@ -1563,6 +1597,7 @@ int tga_search_noncoherent(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant_tot
     CK(cudaMemcpyAsync(best.data(), d_best, best.size() * sizeof(BestRow), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     collect_times(ctx);
+    check_tc_error(ctx);
     ctx->last_cells = (double)n_ant * nb * n_prn * (double)P * B;
     // |y| of the polyphase correlator is Lc |r|; report (|r| sqrt(N))^2 per block
     const double scale = (double)opt->coherent_periods * (double)P / ((double)pc.Lc * (double)pc.Lc);
