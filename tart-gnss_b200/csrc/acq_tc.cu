@@ -118,15 +118,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
       : "memory");
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16};" ::"r"(taddr),
-      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
-      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
-      : "memory");
-}
-__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
@@ -230,14 +221,11 @@ struct Tc3Cfg<10> {
   static constexpr bool S2O = true;
 };
 
-// residues per work item of the non-coherent search (NCB): fewer than the
-// drop-in's, so that each chain keeps room in its 256 TMEM columns for the
-// |y|^2 accumulators (Lc = 1023 only)
-constexpr int kNcBC = 4;
-
+// NCB: the non-coherent search (Lc = 1023 only), with |y|^2 sums in shared
+// memory
 template <int M, bool NCB = false>
 struct T3 {
-  static constexpr int R2 = Tc3Cfg<M>::R2, R3 = Tc3Cfg<M>::R3, BC = NCB ? kNcBC : Tc3Cfg<M>::BC;
+  static constexpr int R2 = Tc3Cfg<M>::R2, R3 = Tc3Cfg<M>::R3, BC = Tc3Cfg<M>::BC;
   static constexpr int LC = 1023 * M, OCOLS = 33 * M;
   static constexpr int NST = Tc3Cfg<M>::NST;
   static_assert(31 * R2 * R3 == LC, "factorisation");
@@ -275,11 +263,11 @@ struct T3 {
   static constexpr int LAST_ROWS = NST == 3 ? ROWS3P : ROWS2, LAST_NR = NST == 3 ? NR3 : NR2;
   static constexpr int LAST_OUT = NST == 3 ? R3 : R2;
   // non-coherent search: per chain, |y|^2 sums over the blocks of the 33
-  // stage-2 outputs of every row in three chunks of 11, each in 16 TMEM
-  // columns from ACC0
-  static constexpr int ACC0 = CHAIN_COLS;
-  static_assert(!NCB || (M == 1 && NST == 2 && LAST_TILES == 1 && ACC0 % 16 == 0 && ACC0 + 48 <= kTcTmemCols / 2),
-                "non-coherent accumulators");
+  // stage-2 outputs of every row, as [33][LAST_TILES * 128] floats (rows
+  // fastest: a warp's 32 lanes touch 32 banks)
+  static_assert(!NCB || (M == 1 && NST == 2 && LAST_OUT == 33), "non-coherent search: Lc = 1023");
+  static constexpr int ACC_ROWS = LAST_TILES * 128;
+  static constexpr int ACC_BYTES = NCB ? (33 * ACC_ROWS * 4 + 1023) / 1024 * 1024 : 0;
   // data operand regions: rows padded to whole tiles, K chunks lbo apart
   static constexpr int LBO1 = TILES1 * 128 * 16 + 16, LBO2 = TILES2 * 128 * 16 + 16 * Tc3Cfg<M>::PAD2,
                        LBO3 = TILES3 * 128 * 16 + 16 * Tc3Cfg<M>::PAD3;
@@ -294,7 +282,7 @@ struct T3 {
   static constexpr int UNITS = NR1 * 8;
   static constexpr int U = (UNITS + kSimtThreads - 1) / kSimtThreads;
   static_assert(8 * ROWS1 < 65536 && 8 * LBO1 < 65536, "packed unit offsets");
-  static constexpr int SMEM_RAW = 2 * A_BYTES + B1_BYTES + B2_BYTES + B3_BYTES + 2 * CODE_REGION + 1024;
+  static constexpr int SMEM_RAW = 2 * A_BYTES + B1_BYTES + B2_BYTES + B3_BYTES + 2 * CODE_REGION + 2 * ACC_BYTES + 1024;
   // more than half of the SM's shared memory: one CTA, and so one 512-column
   // TMEM allocation, per SM
   static constexpr int SMEM = SMEM_RAW > 120 * 1024 ? SMEM_RAW : 120 * 1024;
@@ -447,10 +435,10 @@ __device__ __forceinline__ void tmem_ld_stage3(uint32_t taddr, int half, uint32_
 // own.  Every wait is bounded.
 //
 // NCB (non-coherent search, Lc = 1023): the row is an (antenna, bin) and
-// every PRN pair runs through B coherent blocks; the chains keep per-lane
-// |y|^2 sums in TMEM and take the row maximum after the last block.  The Z
-// of the next block is loaded into the registers while the current block's
-// transform runs.
+// every PRN pair runs through B coherent blocks; each thread keeps the |y|^2
+// sums of its epilogue outputs in shared memory and takes the row maximum
+// after the last block.  The Z of the next block is loaded into the
+// registers while the current block's transform runs.
 template <int M, bool NCB>
 __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   using T = T3<M, NCB>;
@@ -475,6 +463,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   unsigned char* B2 = B1 + T::B1_BYTES;
   unsigned char* B3 = B2 + T::B2_BYTES;
   unsigned char* CODE0 = B3 + T::B3_BYTES;
+  float* ACC = reinterpret_cast<float*>(CODE0 + 2 * T::CODE_REGION);  // [2 chains][33][ACC_ROWS] (NCB)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quad = warp & 3;
   const int S = p.S, n_rounds = (p.n_prn + 1) / 2, B = NCB ? p.B : 1;
 
@@ -814,50 +803,52 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
     };
 
     // ---- P4 of the non-coherent search: add block b's |y|^2 to the chain's
-    // TMEM sums; after the last block, the row maximum of the sums ----
-    // Warp w takes lane quadrant w % 4 and outputs [11 c, 11 c + 11), c = w / 4,
-    // of the single stage-2 tile.
+    // sums in shared memory; after the last block, the row maximum of the
+    // sums ----  Tasks are (stage-2 tile, lane quadrant, outputs
+    // [11 c, 11 c + 11)), task = warp + i NW.
     auto p4_nc = [&](int x, int g, int b) -> float {
-      static_assert(!NCB || NW == 12, "three output chunks of four quadrants");
+      constexpr int NTN = T::LAST_TILES * 4 * 3, TPWN = (NTN + NW - 1) / NW;
       const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
-      const int c = warp >> 2;
-      const int s0 = c == 0 ? 0 : (c == 1 ? 16 : 40);  // 8-column aligned start covering [22 c, 22 c + 22)
-      const uint32_t tacc = tb + (uint32_t)(T::ACC0 + 16 * c);
-      uint32_t v[32], a[16];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        uint32_t(&q)[8] = *reinterpret_cast<uint32_t(*)[8]>(&v[8 * i]);
-        tmem_ld8(tb + (uint32_t)(s0 + 8 * i), q);
-      }
-      if (b > 0) tmem_ld16(tacc, a);
-      tmem_wait_ld();
+      float* acc = ACC + (size_t)x * (T::ACC_BYTES / 4);
       float best = 0.f;
-      const int r = quad * 32 + lane;
-      const bool valid = r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S;
 #pragma unroll
-      for (int h = 0; h < 11; ++h) {
-        // the chunk starts 22 c - s0 = 0, 6 or 4 words into v
-        float re, im;
-        if (c == 0) {
-          re = __uint_as_float(v[2 * h]);
-          im = __uint_as_float(v[2 * h + 1]);
-        } else if (c == 1) {
-          re = __uint_as_float(v[6 + 2 * h]);
-          im = __uint_as_float(v[6 + 2 * h + 1]);
-        } else {
-          re = __uint_as_float(v[4 + 2 * h]);
-          im = __uint_as_float(v[4 + 2 * h + 1]);
+      for (int i = 0; i < TPWN; ++i) {
+        const int task = warp + i * NW;
+        if (task >= NTN) break;
+        const int t = task / 12, c = (task >> 2) % 3;
+        const int s0 = c == 0 ? 0 : (c == 1 ? 16 : 40);  // 8-column aligned start covering [22 c, 22 c + 22)
+        uint32_t v[32];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          uint32_t(&q)[8] = *reinterpret_cast<uint32_t(*)[8]>(&v[8 * k]);
+          tmem_ld8(tb + (uint32_t)(t * T::N2 + s0 + 8 * k), q);
         }
-        const float pw = fmaf(re, re, im * im) + (b > 0 ? __uint_as_float(a[h]) : 0.f);
-        a[h] = __float_as_uint(pw);
-        best = fmaxf(best, pw);
+        tmem_wait_ld();
+        const int r = t * 128 + quad * 32 + lane;
+        const bool valid = r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S;
+        float* a = acc + (size_t)(11 * c) * T::ACC_ROWS + r;
+#pragma unroll
+        for (int h = 0; h < 11; ++h) {
+          // the chunk starts 22 c - s0 = 0, 6 or 4 words into v
+          float re, im;
+          if (c == 0) {
+            re = __uint_as_float(v[2 * h]);
+            im = __uint_as_float(v[2 * h + 1]);
+          } else if (c == 1) {
+            re = __uint_as_float(v[6 + 2 * h]);
+            im = __uint_as_float(v[6 + 2 * h + 1]);
+          } else {
+            re = __uint_as_float(v[4 + 2 * h]);
+            im = __uint_as_float(v[4 + 2 * h + 1]);
+          }
+          const float pw = fmaf(re, re, im * im) + (b > 0 ? a[h * T::ACC_ROWS] : 0.f);
+          if (b + 1 < B)
+            a[h * T::ACC_ROWS] = pw;
+          else if (valid)
+            best = fmaxf(best, pw);
+        }
       }
-      if (b + 1 < B) {
-        tmem_st16(tacc, a);
-        tmem_wait_st();
-        return 0.f;
-      }
-      return valid ? best : 0.f;
+      return best;
     };
 
     for (int w = blockIdx.x; w < p.n_items && !failed; w += gridDim.x) {
