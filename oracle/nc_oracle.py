@@ -3,8 +3,11 @@
 The reference crate has no non-coherent mode; this restates the extension
 implemented by tga_search_noncoherent on top of the reference's own steps:
 antenna prep (acquisition.rs:281-294: +-1, mean over the whole row,
-(v - mean) as f32), wipe-off (correlate.rs:110-115: phase (p * f) as f32,
-f32 cos / sin), circular correlation with the code as
+(v - mean) as f32), wipe-off by the carrier exp(+i 2 pi f (n - n0) / fs)
+with n0 the first sample of the block (the sign convention of
+correlate.rs:110-115; the phase is exact, not the reference's f32-rounded
+absolute phase, whose rounding step reaches 0.25 rad over 100 ms), circular
+correlation with the code as
 IFFT(FFT(x) conj(FFT(code))) (correlate.rs:118-133), here of each coherent
 block folded into one code period and accumulated as N |corr|^2 over the
 blocks (N samples per block, the square of the reference's |IFFT_N| /
@@ -27,7 +30,6 @@ def search_nc(bits, fs, c, prns, ants, center, step, nb, K, B, start):
     N = K * P
     fc = [center + (i - (nb - 1) // 2) * step for i in range(nb)]
     cw = math.ceil(fs / 1.023e6)
-    pc = 2.0 * math.pi / fs
     out = []
     for prn in prns:
         code = O.resampled_code(c, prn, float(P), P).astype(np.float64)
@@ -37,10 +39,10 @@ def search_nc(bits, fs, c, prns, ants, center, step, nb, K, B, start):
             for f in fc:
                 acc = np.zeros(P)
                 for b in range(B):
-                    n = start + b * N + np.arange(N)
-                    ph = ((pc * n.astype(np.float64)) * f).astype(np.float32)
-                    x = v[a, n]
-                    iq = (np.cos(ph) * x).astype(np.float64) + 1j * (np.sin(ph) * x).astype(np.float64)
+                    n0 = start + b * N
+                    n = n0 + np.arange(N)
+                    x = v[a, n].astype(np.float64)
+                    iq = x * np.exp(2j * np.pi * (f * np.arange(N, dtype=np.float64) / fs))
                     fold = iq.reshape(K, P).sum(axis=0)
                     corr = np.fft.ifft(np.fft.fft(fold) * Cc)
                     acc += N * np.abs(corr) ** 2

@@ -3,9 +3,9 @@
 //
 // The drop-in search (correlate.rs:91-183) correlates one two-period window.
 // This mode extends it the usual way for weak signals: block b covers
-// samples [start + b K P, start + (b+1) K P); its K periods are wiped off with
-// the reference's phase convention ((p * f) as f32, correlate.rs:110-115),
-// folded into one period (a cyclic correlation with the periodic code), split
+// samples [start + b K P, start + (b+1) K P); its K periods are wiped off by
+// the exact carrier phase from the block start (the sign convention of
+// correlate.rs:110-115), folded into one period (a cyclic correlation with the periodic code), split
 // into the S polyphase residues and transformed like the drop-in Z; the
 // correlator multiplies by the code spectrum, inverts, and adds |y|^2 of
 // every block into a shared-memory accumulator before it takes the maximum
@@ -35,16 +35,23 @@ struct NcFrontParams {
 
 constexpr int kNcJ = 64;  // chips per CTA
 
-__device__ __forceinline__ float2 wipe_bits(const NcFrontParams& p, int row, long long n, double f) {
-  const uint8_t byte = __ldg(p.src.bits + (size_t)row * p.src.row_bytes + (n >> 3));
-  const double v = ((byte >> (7 - (int)(n & 7))) & 1) ? 1.0 : -1.0;
-  const float s = (float)(v - __ldg(p.src.mean + row));
-  const float ph = __double2float_rn((p.src.pc * (double)n) * f);
-  float sn, cs;
-  sincos_phase(ph, &sn, &cs);
-  return make_float2(cs * s, sn * s);
+// bit n of the row (1 for a + sample)
+__device__ __forceinline__ int sample_bit(const uint8_t* __restrict__ row_bits, long long n) {
+  return (__ldg(row_bits + (n >> 3)) >> (7 - (int)(n & 7))) & 1;
 }
 
+// exp(+i 2 pi t) for a turn count t given in double precision: the turn is
+// reduced to [-1/2, 1/2] in double, the phasor computed in f32
+__device__ __forceinline__ float2 phasor_turns(double t) {
+  float s, c;
+  sincospif((float)(2.0 * (t - rint(t))), &s, &c);
+  return make_float2(c, s);
+}
+
+// Block b of K periods starting at n0 is wiped off by exp(+i 2 pi f (n - n0)
+// / fs) and folded into one period.  With the exact (linear) phase the fold
+// factors: x(m) = exp(i phi(m)) sum_k s(n0 + k P + m) exp(i phi(k P)), so a
+// folded sample costs K real-by-complex FMAs and one phasor.
 __global__ void __launch_bounds__(256) nc_frontend_kernel(NcFrontParams p) {
   extern __shared__ float2 fsm[];
   const int S = p.S, P = p.P, Lc = p.Lc;
@@ -52,16 +59,29 @@ __global__ void __launch_bounds__(256) nc_frontend_kernel(NcFrontParams p) {
   const int ant_slot = ab / p.nb, bin = ab - ant_slot * p.nb;
   const int row = p.src.ant[ant_slot];
   const double f = p.fc[bin];
+  const double turns_per_sample = f * p.src.pc / 6.283185307179586;  // f / fs
   const long long n0 = p.start + (long long)blk * p.K * P;
   const int j0 = blockIdx.x * kNcJ;
   const int nj = min(kNcJ, Lc - j0);
   const int cnt = nj * S + S - 1;
+  const int span = kNcJ * S + S;
+  float2* rot = fsm + span + span / S + 1;  // exp(i phi(k P)), k < K
+  for (int k = threadIdx.x; k < p.K; k += blockDim.x) rot[k] = phasor_turns(turns_per_sample * (double)k * (double)P);
+  // the two sample values (+-1 - mean) as f32 (acquisition.rs:281-294)
+  const double mean = __ldg(p.src.mean + row);
+  const float s_one = (float)(1.0 - mean), s_zero = (float)(-1.0 - mean);
+  const uint8_t* row_bits = p.src.bits + (size_t)row * p.src.row_bytes;
+  __syncthreads();
   for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
     int m = S * j0 + i;
     if (m >= P) m -= P;  // the folded block is P-periodic
-    float2 x = make_float2(0.f, 0.f);
-    for (int k = 0; k < p.K; ++k) x = cadd(x, wipe_bits(p, row, n0 + (long long)k * P + m, f));
-    fsm[i + i / S] = x;
+    float2 acc = make_float2(0.f, 0.f);
+    for (int k = 0; k < p.K; ++k) {
+      const float s = sample_bit(row_bits, n0 + (long long)k * P + m) ? s_one : s_zero;
+      acc.x = fmaf(s, rot[k].x, acc.x);
+      acc.y = fmaf(s, rot[k].y, acc.y);
+    }
+    fsm[i + i / S] = cmul(acc, phasor_turns(turns_per_sample * (double)m));
   }
   __syncthreads();
   const size_t seq0 = ((size_t)ab * p.B + blk) * S;
@@ -310,7 +330,7 @@ cudaError_t launch_nc_frontend(const SampleSource& src, const SearchDims& dims, 
   for (int i = 0; i < kMaxPulse; ++i) p.pulse[i] = pc.pulse[i];
   p.z = d_z;
   const int span = kNcJ * pc.S + pc.S;
-  const size_t smem = (size_t)(span + span / pc.S + 1) * sizeof(float2);
+  const size_t smem = (size_t)(span + span / pc.S + 1 + K) * sizeof(float2);
   const long long gy = (long long)dims.n_ant * dims.nb * B;
   if (gy > 65535) return cudaErrorInvalidValue;
   dim3 grid((pc.Lc + kNcJ - 1) / kNcJ, (unsigned)gy);

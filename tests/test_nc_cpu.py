@@ -37,7 +37,9 @@ def test_one_two_period_block_is_the_dropin_cc_hypothesis():
     nc = NC.search_nc(bits, FS, O.GPS, [7], [0], 4.092e6, step, len(grid), 2, 1, 0)[0]
     assert nc["best_codephase"] == r["best_codephase"] % P
     assert nc["best_freq_idx"] == r["best_freq_idx"]
-    assert abs(nc["power"] - r["signal_strength"] ** 2) <= 1e-6 * nc["power"]
+    # the drop-in rounds the carrier phase to f32 (up to 0.002 rad over two
+    # periods), the non-coherent mode uses the exact phase: ~1e-4 in power
+    assert abs(nc["power"] - r["signal_strength"] ** 2) <= 2e-4 * nc["power"]
 
 
 def test_weak_satellite_found_with_noncoherent_sums():
