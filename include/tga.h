@@ -309,9 +309,13 @@ int tga_code_resampled(int constellation, int prn, double samples_per_code,
  * An extension of the drop-in search (no reference counterpart; the crate
  * searches one two-period window): `blocks` consecutive coherent blocks of
  * `coherent_periods` code periods starting at sample `start`; each block is
- * wiped off with the reference's phase convention (correlate.rs:110-115),
- * folded into one period and correlated cyclically with the code; |y|^2 is
- * summed over the blocks before the peak search.  Doppler bins are centred:
+ * wiped off by the exact carrier phase measured from its first sample (the
+ * sign convention of correlate.rs:110-115), folded into one period and
+ * correlated cyclically with the code; |y|^2 is summed over the blocks before
+ * the peak search.  With TGA_PRECISION_FP16_TC and a 1023-chip code (GPS,
+ * SBAS, QZSS C/A) the bins are chosen on the tensor cores and the selected
+ * row of every (antenna, PRN) is re-evaluated in FP32; other codes run the
+ * FP32 search in either precision.  Doppler bins are centred:
  * center_freq + (i - (n_bins - 1) / 2) * bin_step_hz.  Ties: the later lag
  * within a bin, the later bin across bins; second peak at a circular
  * distance of more than ceil(fs / 1.023 MHz) samples from the peak.  Needs an
