@@ -153,9 +153,11 @@ __global__ void __launch_bounds__(256) frontend_kernel(FrontParams p) {
   for (int o = threadIdx.x; o < S * nj; o += blockDim.x) {
     const int rho = o / nj, jj = o - rho * nj;
     float2 za = make_float2(0.f, 0.f), zb = make_float2(0.f, 0.f);
-    const int base = jj * S + rho;
+    // tap s reads sample i = jj S + rho + s at padded index i + i / S, and
+    // i / S = jj + (rho + s >= S) since rho + s < 2 S: no division per tap
+    const int base = jj * S + rho + jj;
     for (int s = 0; s < S; ++s) {
-      const int i = base + s, pi = i + i / S;
+      const int pi = base + s + (rho + s >= S ? 1 : 0);
       const float w = p.pulse[s];
       za.x = fmaf(w, fsh[pi].x, za.x);
       za.y = fmaf(w, fsh[pi].y, za.y);

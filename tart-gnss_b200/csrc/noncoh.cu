@@ -88,12 +88,14 @@ __global__ void __launch_bounds__(256) nc_frontend_kernel(NcFrontParams p) {
   for (int o = threadIdx.x; o < S * nj; o += blockDim.x) {
     const int rho = o / nj, jj = o - rho * nj;
     float2 z = make_float2(0.f, 0.f);
-    const int base = jj * S + rho;
+    // tap s reads sample i = jj S + rho + s at padded index i + i / S, and
+    // i / S = jj + (rho + s >= S) since rho + s < 2 S: no division per tap
+    const int base = jj * S + rho + jj;
     for (int s = 0; s < S; ++s) {
-      const int i = base + s;
+      const float2 v = fsm[base + s + (rho + s >= S ? 1 : 0)];
       const float w = p.pulse[s];
-      z.x = fmaf(w, fsm[i + i / S].x, z.x);
-      z.y = fmaf(w, fsm[i + i / S].y, z.y);
+      z.x = fmaf(w, v.x, z.x);
+      z.y = fmaf(w, v.y, z.y);
     }
     p.z[(seq0 + rho) * Lc + j0 + jj] = z;
   }
