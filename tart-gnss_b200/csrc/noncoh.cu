@@ -66,22 +66,59 @@ __global__ void __launch_bounds__(256) nc_frontend_kernel(NcFrontParams p) {
   const int cnt = nj * S + S - 1;
   const int span = kNcJ * S + S;
   float2* rot = fsm + span + span / S + 1;  // exp(i phi(k P)), k < K
-  for (int k = threadIdx.x; k < p.K; k += blockDim.x) rot[k] = phasor_turns(turns_per_sample * (double)k * (double)P);
+  float2* step = rot + p.K;                 // exp(i phi(j)), j < 8
+  for (int k = threadIdx.x; k < p.K + 8; k += blockDim.x)
+    rot[k] = k < p.K ? phasor_turns(turns_per_sample * (double)k * (double)P)
+                     : phasor_turns(turns_per_sample * (double)(k - p.K));
   // the two sample values (+-1 - mean) as f32 (acquisition.rs:281-294)
   const double mean = __ldg(p.src.mean + row);
   const float s_one = (float)(1.0 - mean), s_zero = (float)(-1.0 - mean);
   const uint8_t* row_bits = p.src.bits + (size_t)row * p.src.row_bytes;
+  const long long row_bits_n = (long long)p.src.row_bytes * 8;
   __syncthreads();
-  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-    int m = S * j0 + i;
-    if (m >= P) m -= P;  // the folded block is P-periodic
-    float2 acc = make_float2(0.f, 0.f);
-    for (int k = 0; k < p.K; ++k) {
-      const float s = sample_bit(row_bits, n0 + (long long)k * P + m) ? s_one : s_zero;
-      acc.x = fmaf(s, rot[k].x, acc.x);
-      acc.y = fmaf(s, rot[k].y, acc.y);
+  // folded sample i (period position m = S j0 + i, mod P) at fsm[i + i / S]
+  auto store = [&](int i, float2 v) { fsm[i + i / S] = v; };
+  // eight consecutive folded samples per thread: one 16-bit window of each
+  // period holds all eight bits
+  for (int i0 = 8 * threadIdx.x; i0 < cnt; i0 += 8 * blockDim.x) {
+    int m0 = S * j0 + i0;
+    if (m0 >= P) m0 -= P;  // the folded block is P-periodic
+    if (m0 + 7 < P) {
+      float2 acc[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[j] = make_float2(0.f, 0.f);
+      for (int k = 0; k < p.K; ++k) {
+        const long long n = n0 + (long long)k * P + m0;
+        const long long byte = n >> 3;
+        unsigned w = (unsigned)__ldg(row_bits + byte) << 8;
+        if (((byte + 1) << 3) < row_bits_n) w |= __ldg(row_bits + byte + 1);
+        w <<= (int)(n & 7);  // sample n + j is bit 15 - j
+        const float2 r = rot[k];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const float sv = (w >> (15 - j)) & 1u ? s_one : s_zero;
+          acc[j].x = fmaf(sv, r.x, acc[j].x);
+          acc[j].y = fmaf(sv, r.y, acc[j].y);
+        }
+      }
+      const float2 ph0 = phasor_turns(turns_per_sample * (double)m0);
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (i0 + j < cnt) store(i0 + j, cmul(acc[j], cmul(ph0, step[j])));
+    } else {
+      // the group straddles the end of the period: one sample at a time
+      for (int j = 0; j < 8 && i0 + j < cnt; ++j) {
+        int m = m0 + j;
+        if (m >= P) m -= P;
+        float2 acc = make_float2(0.f, 0.f);
+        for (int k = 0; k < p.K; ++k) {
+          const float sv = sample_bit(row_bits, n0 + (long long)k * P + m) ? s_one : s_zero;
+          acc.x = fmaf(sv, rot[k].x, acc.x);
+          acc.y = fmaf(sv, rot[k].y, acc.y);
+        }
+        store(i0 + j, cmul(acc, phasor_turns(turns_per_sample * (double)m)));
+      }
     }
-    fsm[i + i / S] = cmul(acc, phasor_turns(turns_per_sample * (double)m));
   }
   __syncthreads();
   const size_t seq0 = ((size_t)ab * p.B + blk) * S;
@@ -332,7 +369,7 @@ cudaError_t launch_nc_frontend(const SampleSource& src, const SearchDims& dims, 
   for (int i = 0; i < kMaxPulse; ++i) p.pulse[i] = pc.pulse[i];
   p.z = d_z;
   const int span = kNcJ * pc.S + pc.S;
-  const size_t smem = (size_t)(span + span / pc.S + 1 + K) * sizeof(float2);
+  const size_t smem = (size_t)(span + span / pc.S + 1 + K + 8) * sizeof(float2);
   const long long gy = (long long)dims.n_ant * dims.nb * B;
   if (gy > 65535) return cudaErrorInvalidValue;
   dim3 grid((pc.Lc + kNcJ - 1) / kNcJ, (unsigned)gy);
