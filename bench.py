@@ -207,6 +207,37 @@ def cpu_sample_baseline(threads, repeats=1):
     return cells / dt, dt, desc
 
 
+def fp64_peak_errors(bits, runs, threads):
+    """Peak-metric error of the GPU searches against the oracle in float64 on
+    a bounded sample of the benchmark recording (antenna 0, the PRNs of the
+    CPU baseline sample, all 41 bins): per constellation, the largest
+    relative error of signal_strength and whether code phase, bin and
+    hypothesis equal the FP64 result.  runs: {arithmetic: cells}."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import acq_oracle as O
+    names = {O.GPS: "GPS L1 C/A", O.SBAS: "SBAS", O.QZSS: "QZSS", O.GALILEO: "Galileo E1-C",
+             O.BEIDOU: "BeiDou B1C", O.L1C: "GPS L1C"}
+    sample = {O.GPS: [1, 2, 3, 4], O.SBAS: [120, 121], O.QZSS: [184], O.GALILEO: [1, 2], O.BEIDOU: [1, 2],
+              O.L1C: [1, 2]}
+    ub = np.unpackbits(bits[:1], axis=1)
+    out = {}
+    for c, prns in sample.items():
+        ref = O.acquire_all(ub, FS, c, prn_filter=prns, precision="f64", threads=threads)
+        per = {}
+        for arith, cells in runs.items():
+            worst, same = 0.0, True
+            for r in ref["results"]:
+                rc = r["cells"][0]
+                g = cells[(cells["constellation"] == c) & (cells["prn"] == rc["prn"]) & (cells["antenna"] == 0)][0]
+                worst = max(worst, abs(g["signal_strength"] - rc["signal_strength"]) / rc["signal_strength"])
+                same &= (int(g["best_codephase"]) == int(rc["best_codephase"]) and
+                         int(g["best_freq_idx"]) == int(rc["best_freq_idx"]) and
+                         int(g["hypothesis"]) == int(rc["hypothesis"]))
+            per[arith] = {"max_rel_peak_error": worst, "same_cell": bool(same)}
+        out[names[c]] = per
+    return out
+
+
 def fp32_peak_tflops(sm_mhz, n_sm=148):
     return n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
 
@@ -521,6 +552,12 @@ def main():
                            "speedup_of_headline": value / ovalue, "same_detections": same,
                            "detected_cells": int(da.sum()), "cells": int(len(da)),
                            "roofline": roofline(oagg, oprec, sm_mhz), "gpu_launches": olaunch}
+    if rank == 0 and other is not None and not args.no_cpu_baseline:
+        line["peak_error_vs_fp64"] = {
+            "sample": "antenna 0, PRNs GPS 1-4, SBAS 120-121, QZSS 184, Galileo 1-2, BeiDou 1-2, L1C 1-2, 41 bins; "
+                      "oracle (reference algorithm) in float64",
+            "per_constellation": fp64_peak_errors(bits_np, {dtype[args.precision]: out, dtype[other[0]]: other[5]},
+                                                  os.cpu_count() or 1)}
     if weak is not None:
         line["weak_signal"] = weak
     if not args.no_fine:
