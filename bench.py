@@ -77,9 +77,9 @@ def synth_observation(seed, n_ant=N_ANT, n_samples=SAMPLES, chunk=163680):
     return bits, sats
 
 
-def synth_weak_observation(seed, n_ant=N_ANT, n_samples=SAMPLES, n_sats=8, chunk=163680):
+def synth_weak_observation(seed, n_ant=N_ANT, n_samples=SAMPLES, n_sats=8, chunk=163680, cn0=(28.0, 36.0)):
     """Weak-signal recording: n_sats GPS C/A satellites (PRNs 1-32) at C/N0
-    uniform 28-36 dB-Hz, code phase uniform, Doppler uniform +-4 kHz, random
+    uniform in cn0 (28-36 dB-Hz), code phase uniform, Doppler uniform +-4 kHz, random
     +-1 navigation bits of 20 ms with a random bit-edge offset, per-antenna
     carrier phases, unit Gaussian noise, sign-quantised.  Returns (bits,
     satellites)."""
@@ -90,7 +90,7 @@ def synth_weak_observation(seed, n_ant=N_ANT, n_samples=SAMPLES, n_sats=8, chunk
     for prn in rng.choice(np.arange(1, 33), size=n_sats, replace=False):
         code = tga.code_resampled(0, int(prn), float(P), P).astype(np.float32)
         sats.append(dict(prn=int(prn), code=code, delay=int(rng.integers(0, P)), dop=float(rng.uniform(-4000, 4000)),
-                         cn0=float(rng.uniform(28, 36)), edge=int(rng.integers(0, 20)),
+                         cn0=float(rng.uniform(*cn0)), edge=int(rng.integers(0, 20)),
                          bits=rng.choice([-1.0, 1.0], size=n_samples // (20 * P) + 3).astype(np.float32)))
     phase = np.exp(1j * rng.uniform(0, 2 * np.pi, size=(n_ant, len(sats)))).astype(np.complex64)
     bits = np.empty((n_ant, n_samples // 8), np.uint8)
@@ -293,6 +293,8 @@ def main():
                          "(default), or FP32 CUDA cores")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the second arithmetic (the FP32 fused search beside the tensor-core one)")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the plain GPS C/A search (1 antenna, 1 ms coherent x 10, 21 x 500 Hz bins)")
     ap.add_argument("--no-weak", action="store_true",
                     help="skip the weak-signal non-coherent search (10 ms coherent x 10, 201 x 50 Hz bins)")
     ap.add_argument("--no-fine", action="store_true", help="skip the fine-acquisition measurement")
@@ -426,6 +428,52 @@ def main():
     if not args.no_compare:
         oprec = "fp32" if args.precision == "fp16tc" else "fp16tc"
         other = (oprec,) + measure(oprec)
+    plain = None
+    if not args.no_plain:
+        # plain GPS C/A acquisition: 1 antenna, 10 ms (1 ms coherent x 10
+        # non-coherent sums), PRNs 1-32, 21 x 500 Hz bins, 4 satellites at
+        # 45 dB-Hz with navigation bits; both arithmetics, and (rank 0) the
+        # oracle on the same bits: PRN set, code phase and bin compared
+        pbits, psats = synth_weak_observation(SEED + 2000 + rank, n_ant=1, n_samples=163680, n_sats=4,
+                                              cn0=(45.0, 45.0))
+        pkw = dict(prns=list(range(1, 33)), bin_step_hz=500.0, n_bins=21, coherent_periods=1, blocks=10)
+        pcells = 1 * 32 * 21 * 16368.0 * 10
+        pres = {}
+        for prec in ("fp16tc", "fp32"):
+            ctx.set_precision(prec_id[prec])
+            for _ in range(args.warmup):
+                pout = ctx.search_noncoherent(pbits, FS, tga.GPS, **pkw)
+            pt = []
+            for _ in range(args.steps):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                pout = ctx.search_noncoherent(pbits, FS, tga.GPS, **pkw)
+                pt.append(time.perf_counter() - t0)
+            pres[prec] = (statistics.mean(pt), pout)
+        ctx.set_precision(prec_id[args.precision])
+        ptruth = {s["prn"]: s for s in psats}
+
+        def pdet(out):
+            return {int(c["prn"]): (int(c["best_codephase"]), int(c["best_freq_idx"]))
+                    for c in out if c["power"] > 1.5 * c["second_power"]}
+
+        plain = {"workload": "GPS C/A PRNs 1-32 x 1 antenna, 1 ms coherent x 10 blocks (10 ms), 21 x 500 Hz bins, "
+                             "4 satellites at 45 dB-Hz with navigation bits; tga_search_noncoherent end to end",
+                 "unit": "cell-blocks/s", "cells_per_step": pcells}
+        for prec, (t_s, pout) in pres.items():
+            d = pdet(pout)
+            found = sum(1 for prn, s in ptruth.items() if prn in d and d[prn][0] == (16368 - s["delay"]) % 16368)
+            plain[prec] = {"value": pcells / t_s, "ms_per_step": t_s * 1e3, "detected_prns": sorted(d),
+                           "injected_found": "%d of %d" % (found, len(ptruth))}
+        plain["same_detections"] = pdet(pres["fp16tc"][1]) == pdet(pres["fp32"][1])
+        if rank == 0 and not args.no_cpu_baseline:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import nc_oracle
+            ref = nc_oracle.search_nc(pbits, FS, tga.GPS, list(range(1, 33)), [0], 4.092e6, 500.0, 21, 1, 10, 0)
+            rdet = {int(r["prn"]): (int(r["best_codephase"]), int(r["best_freq_idx"])) for r in ref
+                    if r["power"] > 1.5 * r["second_power"]}
+            plain["oracle_equal"] = {prec: pdet(pout) == rdet for prec, (t_s, pout) in pres.items()}
+
     weak = None
     if not args.no_weak:
         # weak-signal search: GPS C/A PRNs 1-32, 10 ms coherent blocks x 10
@@ -558,6 +606,8 @@ def main():
                       "oracle (reference algorithm) in float64",
             "per_constellation": fp64_peak_errors(bits_np, {dtype[args.precision]: out, dtype[other[0]]: other[5]},
                                                   os.cpu_count() or 1)}
+    if plain is not None:
+        line["plain_gps"] = plain
     if weak is not None:
         line["weak_signal"] = weak
     if not args.no_fine:
