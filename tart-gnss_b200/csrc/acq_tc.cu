@@ -34,6 +34,11 @@
 // work on one chain while the warps transpose the other; a dedicated warp
 // issues the MMAs.  Every wait is bounded (1 s): on expiry the kernel sets
 // *err, drains (again bounded), frees its TMEM and returns.
+//
+// The same kernel (NCB) runs the non-coherent search at Lc = 1023: every PRN
+// pair goes through B coherent blocks, the Z of each block is loaded into the
+// registers in turn, and the |y|^2 of the blocks are summed in shared memory
+// before the row maximum.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
