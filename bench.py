@@ -466,7 +466,7 @@ def main():
             plain[prec] = {"value": pcells / t_s, "ms_per_step": t_s * 1e3, "detected_prns": sorted(d),
                            "injected_found": "%d of %d" % (found, len(ptruth))}
         plain["same_detections"] = pdet(pres["fp16tc"][1]) == pdet(pres["fp32"][1])
-        if rank == 0 and not args.no_cpu_baseline:
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
             import nc_oracle
             ref = nc_oracle.search_nc(pbits, FS, tga.GPS, list(range(1, 33)), [0], 4.092e6, 500.0, 21, 1, 10, 0)
@@ -600,7 +600,7 @@ def main():
                            "speedup_of_headline": value / ovalue, "same_detections": same,
                            "detected_cells": int(da.sum()), "cells": int(len(da)),
                            "roofline": roofline(oagg, oprec, sm_mhz), "gpu_launches": olaunch}
-    if rank == 0 and other is not None and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and other is not None and not args.no_cpu_baseline:
         line["peak_error_vs_fp64"] = {
             "sample": "antenna 0, PRNs GPS 1-4, SBAS 120-121, QZSS 184, Galileo 1-2, BeiDou 1-2, L1C 1-2, 41 bins; "
                       "oracle (reference algorithm) in float64",
