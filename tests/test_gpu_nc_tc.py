@@ -100,3 +100,36 @@ def test_expired_wait_is_a_timeout(ctx):
         ctx.set_precision(tga.PRECISION_FP32)
     f32, tc = _both(ctx, bits, tga.GPS, prns=[3], bin_step_hz=500.0, n_bins=3, coherent_periods=1, blocks=2)
     assert tc["best_codephase"][0] == f32["best_codephase"][0] == (P - 100) % P
+
+
+@pytest.mark.parametrize("fs", [4.092e6, 8.184e6], ids=["S4", "S8"])
+def test_other_integer_rates(ctx, fs):
+    """4 and 8 samples per chip: fewer polyphase residues in the front end and
+    smaller folded magnitudes ahead of the FP16 scaling; IF at fs/4."""
+    import math
+    Pf = O.period_samples(O.GPS, fs)
+    n = 12 * Pf
+    rng = np.random.default_rng(int(fs) % 997)
+    t = np.arange(n)
+    x = rng.standard_normal((2, n))
+    sats = [(9, 1234, 900.0), (27, Pf - 3, -1750.0)]
+    for prn, delay, dop in sats:
+        code = O.resampled_code(O.GPS, prn, float(Pf), Pf).astype(np.float64)
+        amp = 2.0 * math.sqrt(10.0 ** (40.0 / 10.0) / fs)
+        for a in range(2):
+            x[a] += amp * code[(t + delay) % Pf] * np.cos(2 * np.pi * (fs / 4 + dop) / fs * t + rng.uniform(0, 6.28))
+    bits = np.packbits(x >= 0, axis=1)
+    kw = dict(prns=[9, 27, 14], center_freq=fs / 4, bin_step_hz=250.0, n_bins=21, coherent_periods=4, blocks=3)
+    ctx.set_precision(tga.PRECISION_FP32)
+    f32 = ctx.search_noncoherent(bits, fs, tga.GPS, **kw)
+    ctx.set_precision(tga.PRECISION_FP16_TC)
+    try:
+        tc = ctx.search_noncoherent(bits, fs, tga.GPS, **kw)
+    finally:
+        ctx.set_precision(tga.PRECISION_FP32)
+    same = _same_row_same_power(f32, tc)
+    present = f32["prn"] != 14
+    assert np.all(same[present])
+    for g in tc[present]:
+        delay = dict((p, d) for p, d, _ in sats)[int(g["prn"])]
+        assert int(g["best_codephase"]) == (Pf - delay) % Pf

@@ -104,3 +104,26 @@ def test_tc_wait_expiry_reports_timeout_and_context_survives():
         c.set_precision(tga.PRECISION_FP32)
         f = c.acquire_single(tga.GPS, sig, pp, fs, 4.092e6, 6000.0, 7, period)
     assert (r.best_codephase, r.best_freq_idx) == (f.best_codephase, f.best_freq_idx)
+
+
+@pytest.mark.parametrize("fs", [2.046e6, 4.092e6, 8.184e6], ids=["S2", "S4", "S8"])
+@pytest.mark.parametrize("c,prn", [(O.GPS, 11), (O.GALILEO, 4), (O.BEIDOU, 21)], ids=["gps", "galileo", "beidou"])
+def test_tc_other_integer_rates_match_fp32(ctxs, fs, c, prn):
+    """Rates with 2, 4 and 8 samples per chip take the fused polyphase front
+    end with fewer residues (and smaller folded magnitudes before the FP16
+    scaling); the tensor-core search keeps the FP32 mode's answer there too.
+    The IF sits at fs/4 so the carrier is below Nyquist at every rate."""
+    f32, tc = ctxs
+    fc = fs / 4
+    period = O.period_samples(c, fs)
+    code = O.resampled_code(c, prn, float(period), 2 * period)
+    cont = synth_signal_cn0(code, period, (prn * 7919) % period, fc + 1734.0, fs, 47.0, 0x5A7E + prn, False)
+    sig = quantize_bipolar_demean(cont.astype(np.float64))
+    pp = phasepoints(fs, len(sig))
+    a = f32.acquire_single(c, sig, pp, fs, fc, 6000.0, prn, period)
+    b = tc.acquire_single(c, sig, pp, fs, fc, 6000.0, prn, period)
+    assert (b.best_codephase, b.best_freq_idx, b.hypothesis) == (a.best_codephase, a.best_freq_idx, a.hypothesis)
+    assert rel(b.signal_strength, a.signal_strength) <= REL_TOL
+    assert rel(b.second_peak, a.second_peak) <= REL_TOL
+    assert detected(a.signal_strength, a.second_peak)
+    assert int(round(a.codephase_frac * period)) % period == (period - (prn * 7919) % period) % period
