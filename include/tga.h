@@ -222,8 +222,8 @@ int tga_set_profiling(tga_ctx* ctx, int enable);
 /* Arithmetic of the correlation search.
  *  TGA_PRECISION_FP32 (default): every transform stage in FP32 on the CUDA
  *    cores; results within 1e-4 of the reference algorithm.
- *  TGA_PRECISION_FP16_TC: the DFT-31 stage of the search runs on the tensor
- *    cores (tcgen05, FP16 operands, FP32 accumulation); the row chosen for
+ *  TGA_PRECISION_FP16_TC: the inverse transforms of the search run on the
+ *    tensor cores (tcgen05, FP16 operands, FP32 accumulation); the row chosen for
  *    every (antenna, PRN) is then re-evaluated in FP32, so reported peak, lag
  *    and second peak are FP32 values; only the choice of Doppler bin and
  *    hypothesis among near-equal candidates can differ from the FP32 mode. */
@@ -240,6 +240,21 @@ int tga_set_precision(tga_ctx* ctx, int precision);
  * 4092, 10230): 0 = default; 1 (10230 only) = two polyphase branches per
  * CTA sharing the code spectrum.  Results are identical; only speed varies. */
 int tga_set_variant(tga_ctx* ctx, int lc, int variant);
+/* CUDA graphs for tga_acquire_all / tga_acquire_all_device (enabled by
+ * default).  A search plan (bits buffer, shapes, options, precision,
+ * variant) runs eagerly on its first call, is captured into a CUDA graph on
+ * its second and is replayed from that graph after that; a reallocation of
+ * the context's buffers rebuilds it.  Results are the same either way.
+ * Calls with profiling enabled, and plans with constellations on the
+ * generic path, run eagerly.  No counterpart in the reference (a CPU
+ * library); it serves the batched search's launch path. */
+int tga_set_graphs(tga_ctx* ctx, int enable);
+/* How the last tga_acquire_all* call ran: eagerly, captured then launched,
+ * or replayed from a graph captured earlier. */
+#define TGA_GRAPH_NONE 0
+#define TGA_GRAPH_CAPTURED 1
+#define TGA_GRAPH_REPLAYED 2
+int tga_last_graph(const tga_ctx* ctx, int* state);
 int tga_kernel_times(const tga_ctx* ctx, int cap, const char** names, double* ms,
                      int32_t* launches, double* flops, int* n);
 

@@ -404,6 +404,7 @@ static int g_variant10 = 0;
 void set_pfa_variant(int M, int v) {
   if (M == 10) g_variant10 = v;
 }
+int pfa_variant(int M) { return M == 10 ? g_variant10 : 0; }
 
 template <int M, int V, int MODE>
 static cudaError_t run_pfa(const PfaParams& p, int n_work_slots, int num_sms, cudaStream_t st) {

@@ -141,6 +141,7 @@ cudaError_t launch_bits_to_signal(const uint8_t* d_bits, size_t row_bytes, int r
 // Selects an alternative launch configuration of the transform kernels for
 // third digit M (tuning; 0 = default).
 void set_pfa_variant(int M, int v);
+int pfa_variant(int M);
 
 // fine acquisition: per (task, antenna) the complex sums R, dR/dtau, dR/df,
 // d2R/dtau2, d2R/df2, d2R/dtau df (un-normalised), zeroed and accumulated

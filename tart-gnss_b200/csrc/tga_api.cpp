@@ -79,11 +79,30 @@ struct tga_ctx {
   std::map<std::string, ClassCache> class_cache;
   std::map<std::pair<int, int>, std::vector<int8_t>> chip_cache;
   std::map<std::string, std::vector<std::pair<int, int>>> uploaded;  // device chips buffer -> PRN list
+  // CUDA graphs of the --all pipeline, one per plan (key: everything the
+  // launches capture by value).  A plan runs eagerly on its first call, is
+  // captured on its second and replayed after that.  `gen` counts buffer
+  // (re)allocations: a graph captured under another generation holds stale
+  // pointers and is rebuilt.
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    size_t gen = 0;
+    bool seen = false, failed = false;
+    int launches = 0;
+    double cells = 0.0;
+    uint64_t d2h = 0;
+    int* tc_err = nullptr;
+  };
+  bool graphs_enabled = true;
+  size_t gen = 0;
+  std::map<std::string, GraphEntry> graphs;
+  int last_graph = TGA_GRAPH_NONE;
   // pinned host staging for results
   void* pinned = nullptr;
   size_t pinned_cap = 0;
   void* host_pinned(size_t bytes) {
     if (pinned_cap >= bytes && pinned) return pinned;
+    ++gen;
     if (pinned) cudaFreeHost(pinned);
     pinned = nullptr;
     pinned_cap = 0;
@@ -107,6 +126,7 @@ struct tga_ctx {
   void* buf(const std::string& name, size_t bytes) {
     DevBuf& b = bufs[name];
     if (b.cap >= bytes && b.p) return b.p;
+    ++gen;
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.cap = 0;
@@ -241,6 +261,81 @@ void check_tc_error(tga_ctx* ctx) {
   if (flag) throw TimeoutError("tensor-core correlator: a bounded wait on the MMA pipeline expired");
 }
 
+// Runs `enqueue` (launches and stream-ordered copies only) for the plan
+// `key`: eagerly on the plan's first call, captured into a CUDA graph and
+// launched on its second, replayed from the graph after that.  A replay
+// restores what the enqueue would have recorded (launch count, cells, bytes
+// read back, the tensor-core error flag).  A capture that fails for any
+// reason leaves the plan eager.
+template <class F>
+void run_planned(tga_ctx* ctx, const std::string& key, F&& enqueue) {
+  ctx->last_graph = TGA_GRAPH_NONE;
+  if (!ctx->graphs_enabled || ctx->profiling) {
+    enqueue();
+    return;
+  }
+  if (ctx->graphs.size() >= 64 && !ctx->graphs.count(key)) {
+    for (auto& kv : ctx->graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    ctx->graphs.clear();
+  }
+  tga_ctx::GraphEntry& ge = ctx->graphs[key];
+  if (ge.exec && ge.gen != ctx->gen) {
+    cudaGraphExecDestroy(ge.exec);
+    ge.exec = nullptr;
+  }
+  if (ge.exec) {
+    CK(cudaGraphLaunch(ge.exec, ctx->stream));
+    kernel_launch_add(ge.launches);
+    ctx->last_cells += ge.cells;
+    ctx->d2h += ge.d2h;
+    ctx->tc_err_pending = ge.tc_err;
+    ctx->last_graph = TGA_GRAPH_REPLAYED;
+    return;
+  }
+  if (!ge.seen || ge.failed) {
+    enqueue();
+    ge.seen = true;
+    return;
+  }
+  const int l0 = kernel_launch_count();
+  const double c0 = ctx->last_cells;
+  const uint64_t d0 = ctx->d2h;
+  const size_t gen0 = ctx->gen;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  bool ok = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+  if (ok) {
+    try {
+      enqueue();
+    } catch (const std::exception&) {
+      ok = false;
+    }
+    ok = (cudaStreamEndCapture(ctx->stream, &g) == cudaSuccess) && ok && g && ctx->gen == gen0;
+    if (ok) ok = cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+  }
+  if (!ok) {
+    cudaGetLastError();
+    if (ex) cudaGraphExecDestroy(ex);
+    ge.failed = true;
+    kernel_launch_count_reset();
+    kernel_launch_add(l0);
+    ctx->last_cells = c0;
+    ctx->d2h = d0;
+    enqueue();
+    return;
+  }
+  ge.exec = ex;
+  ge.gen = ctx->gen;
+  ge.launches = kernel_launch_count() - l0;
+  ge.cells = ctx->last_cells - c0;
+  ge.d2h = ctx->d2h - d0;
+  ge.tc_err = ctx->tc_err_pending;
+  CK(cudaGraphLaunch(ex, ctx->stream));
+  ctx->last_graph = TGA_GRAPH_CAPTURED;
+}
+
 // FP32 operations per transform point of one length-Lc inverse transform as
 // implemented (DFT-31 1950 flops per 31 points, DFT-33 948 per 33, DFT-4 16
 // per 4, DFT-10 124 per 10; FMA = 2), excluding the input product (6) and
@@ -327,20 +422,33 @@ struct SearchOut {
   std::vector<CellOut> cells;  // [n_ant][n_prn] of the group
 };
 
-// Runs the fused pipeline for one class group, asynchronously on the
-// context stream.  The finalised cells land in host_out (pinned memory,
-// n_ant * n_prn CellOut) once the stream reaches that point.
-void run_group(tga_ctx* ctx, const ClassGroup& grp, const SampleSource& src, const double* d_fc, int nb,
-               double center, int want_cn0, int chip_width, const std::string& tag, CellOut* host_out) {
+// Device buffers of one class group, allocated (and the code chips and DFT
+// matrices uploaded) by prepare_group before anything is launched, so that
+// enqueue_group is launches and stream-ordered copies only and can be
+// captured into a CUDA graph.
+struct GroupBufs {
+  int8_t* chips = nullptr;
+  const int8_t* tables = nullptr;
+  float2* z = nullptr;
+  float2* D = nullptr;
+  unsigned long long* keys = nullptr;
+  BestRow* best = nullptr;
+  CellOut* cells = nullptr;
+  int* err = nullptr;
+  void* z16 = nullptr;
+  void* d16 = nullptr;
+  void* bmat = nullptr;
+};
+
+GroupBufs prepare_group(tga_ctx* ctx, const ClassGroup& grp, int n_ant, int nb, const std::string& tag) {
   const PolyClass& pc = grp.pc;
-  const int n_ant = src.n_ant;
   const int n_prn = (int)grp.prns.size();
   const int n_ab = n_ant * nb;
   cudaStream_t st = ctx->stream;
-
+  GroupBufs b;
   // code chips and ACR table ids -> device (re-uploaded only when the PRN list changes)
   const size_t chip_bytes = (size_t)n_prn * pc.Lc;
-  int8_t* d_chips = (int8_t*)ctx->buf(tag + ".chips", chip_bytes + (size_t)n_prn);
+  b.chips = (int8_t*)ctx->buf(tag + ".chips", chip_bytes + (size_t)n_prn);
   auto up = ctx->uploaded.find(tag + ".chips");
   if (up == ctx->uploaded.end() || up->second != grp.prns) {
     std::vector<int8_t> chips(chip_bytes + (size_t)n_prn);
@@ -349,19 +457,46 @@ void run_group(tga_ctx* ctx, const ClassGroup& grp, const SampleSource& src, con
       std::memcpy(&chips[(size_t)i * pc.Lc], ch.data(), (size_t)pc.Lc);
       chips[chip_bytes + i] = (int8_t)info(grp.prns[i].first).acr_table;
     }
-    CK(cudaMemcpyAsync(d_chips, chips.data(), chips.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(b.chips, chips.data(), chips.size(), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));  // chips is a host temporary
     ctx->h2d += chips.size();
     ctx->uploaded[tag + ".chips"] = grp.prns;
   }
-  const int8_t* d_tables = d_chips + chip_bytes;
+  b.tables = b.chips + chip_bytes;
+  b.z = (float2*)ctx->buf(tag + ".z", (size_t)n_ab * 2 * pc.S * pc.Lc * sizeof(float2));
+  b.D = (float2*)ctx->buf(tag + ".D", (size_t)n_prn * 2 * pc.Lc * sizeof(float2));
+  b.keys = (unsigned long long*)ctx->buf(tag + ".keys", (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long));
+  b.best = (BestRow*)ctx->buf(tag + ".best", (size_t)n_ant * n_prn * sizeof(BestRow));
+  b.cells = (CellOut*)ctx->buf(tag + ".cells", (size_t)n_ant * n_prn * sizeof(CellOut));
+  if (ctx->precision == TGA_PRECISION_FP16_TC) {
+    b.err = (int*)ctx->buf("tc.err", sizeof(int));
+    const long long n_zseq = (long long)n_ab * 2 * pc.S;
+    b.z16 = ctx->buf(tag + ".z16", tc_operand_bytes(pc, n_zseq, false));
+    b.d16 = ctx->buf(tag + ".d16", tc_operand_bytes(pc, (long long)n_prn * 2, true));
+    // DFT matrices of the class (they depend on Lc only), uploaded once per context
+    const std::string mat_name = "tcmat." + std::to_string(pc.M);
+    if (!ctx->uploaded.count(mat_name)) {
+      const std::vector<unsigned char> mats = tc_dft_matrices(pc.M);
+      b.bmat = ctx->buf(mat_name, mats.size());
+      CK(cudaMemcpy(b.bmat, mats.data(), mats.size(), cudaMemcpyHostToDevice));
+      ctx->uploaded[mat_name] = {};
+    } else {
+      b.bmat = ctx->buf(mat_name, 0);
+    }
+  }
+  return b;
+}
 
-  float2* d_z = (float2*)ctx->buf(tag + ".z", (size_t)n_ab * 2 * pc.S * pc.Lc * sizeof(float2));
-  float2* d_D = (float2*)ctx->buf(tag + ".D", (size_t)n_prn * 2 * pc.Lc * sizeof(float2));
-  unsigned long long* d_keys =
-      (unsigned long long*)ctx->buf(tag + ".keys", (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long));
-  BestRow* d_best = (BestRow*)ctx->buf(tag + ".best", (size_t)n_ant * n_prn * sizeof(BestRow));
-  CellOut* d_cells = (CellOut*)ctx->buf(tag + ".cells", (size_t)n_ant * n_prn * sizeof(CellOut));
+// Enqueues the fused pipeline of one class group on the context stream
+// (launches, memsets and the copy of the finalised cells into host_out,
+// pinned memory of n_ant * n_prn CellOut).
+void enqueue_group(tga_ctx* ctx, const ClassGroup& grp, const GroupBufs& b, const SampleSource& src,
+                   const double* d_fc, int nb, double center, int want_cn0, int chip_width, CellOut* host_out) {
+  const PolyClass& pc = grp.pc;
+  const int n_ant = src.n_ant;
+  const int n_prn = (int)grp.prns.size();
+  const int n_ab = n_ant * nb;
+  cudaStream_t st = ctx->stream;
 
   SearchDims dims;
   dims.n_ant = n_ant;
@@ -372,54 +507,40 @@ void run_group(tga_ctx* ctx, const ClassGroup& grp, const SampleSource& src, con
   const double tf = transform_flops_per_point(pc.M);
   const std::string cls = "[Lc=" + std::to_string(pc.Lc) + "]";
   timed(ctx, ("code_spectra" + cls).c_str(), (double)n_prn * 2 * pc.Lc * tf,
-        [&] { return launch_code_spectra(pc, d_chips, n_prn, d_D, ctx->num_sms, st); });
+        [&] { return launch_code_spectra(pc, b.chips, n_prn, b.D, ctx->num_sms, st); });
   timed(ctx, ("frontend" + cls).c_str(), (double)n_ab * 2 * pc.P * pc.S * 4.0,
-        [&] { return launch_frontend(src, dims, pc, d_z, st); });
+        [&] { return launch_frontend(src, dims, pc, b.z, st); });
   timed(ctx, ("forward_z" + cls).c_str(), (double)n_ab * 2 * pc.P * tf,
-        [&] { return launch_forward_z(pc, n_ab, d_z, ctx->num_sms, st); });
+        [&] { return launch_forward_z(pc, n_ab, b.z, ctx->num_sms, st); });
   if (ctx->precision == TGA_PRECISION_FP16_TC) {
-    int* d_err = (int*)ctx->buf("tc.err", sizeof(int));
     const long long n_zseq = (long long)n_ab * 2 * pc.S;
-    void* d_z16 = ctx->buf(tag + ".z16", tc_operand_bytes(pc, n_zseq, false));
-    void* d_d16 = ctx->buf(tag + ".d16", tc_operand_bytes(pc, (long long)n_prn * 2, true));
-    // DFT matrices of the class (they depend on Lc only), uploaded once per context
-    const std::string mat_name = "tcmat." + std::to_string(pc.M);
-    void* d_bmat = nullptr;
-    if (!ctx->uploaded.count(mat_name)) {
-      const std::vector<unsigned char> mats = tc_dft_matrices(pc.M);
-      d_bmat = ctx->buf(mat_name, mats.size());
-      CK(cudaMemcpy(d_bmat, mats.data(), mats.size(), cudaMemcpyHostToDevice));
-      ctx->uploaded[mat_name] = {};
-    } else {
-      d_bmat = ctx->buf(mat_name, 0);
-    }
     timed(ctx, ("tc_pack" + cls).c_str(), 0.0, [&] {
-      cudaError_t e = launch_tc_pack(pc, d_z, n_zseq, false, d_z16, ctx->num_sms, st);
-      if (e == cudaSuccess) e = launch_tc_pack(pc, d_D, (long long)n_prn * 2, true, d_d16, ctx->num_sms, st);
+      cudaError_t e = launch_tc_pack(pc, b.z, n_zseq, false, b.z16, ctx->num_sms, st);
+      if (e == cudaSuccess) e = launch_tc_pack(pc, b.D, (long long)n_prn * 2, true, b.d16, ctx->num_sms, st);
       return e;
     });
-    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
-    CK(cudaMemsetAsync(d_keys, 0, (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(b.err, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(b.keys, 0, (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long), st));
     // tensor-core FLOPs of the three DFT stages as dense real GEMMs
     timed(ctx, ("correlate_tc" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * tc_gemm_flops_per_point(pc.M),
           [&] {
-            return launch_correlate_tc(pc, dims, d_bmat, d_z16, d_d16, d_keys, d_err, ctx->test_flags, ctx->num_sms,
+            return launch_correlate_tc(pc, dims, b.bmat, b.z16, b.d16, b.keys, b.err, ctx->test_flags, ctx->num_sms,
                                        st);
           });
-    ctx->tc_err_pending = d_err;
+    ctx->tc_err_pending = b.err;
   } else {
     timed(ctx, ("correlate" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * (tf + 9.0),
-          [&] { return launch_correlate(pc, dims, d_z, d_D, d_keys, ctx->num_sms, st); });
+          [&] { return launch_correlate(pc, dims, b.z, b.D, b.keys, ctx->num_sms, st); });
   }
-  timed(ctx, ("reduce_bins" + cls).c_str(), 0.0, [&] { return launch_reduce_bins(dims, d_keys, d_best, st); });
+  timed(ctx, ("reduce_bins" + cls).c_str(), 0.0, [&] { return launch_reduce_bins(dims, b.keys, b.best, st); });
   if (ctx->precision == TGA_PRECISION_FP16_TC)
     timed(ctx, ("refine" + cls).c_str(), (double)n_ant * n_prn * pc.P * (tf + 9.0),
-          [&] { return launch_refine(pc, dims, d_z, d_D, d_best, ctx->num_sms, st); });
+          [&] { return launch_refine(pc, dims, b.z, b.D, b.best, ctx->num_sms, st); });
   timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * pc.P * (tf + 9.0),
-        [&] { return launch_second_peak(pc, dims, d_z, d_D, d_best, chip_width, ctx->num_sms, st); });
+        [&] { return launch_second_peak(pc, dims, b.z, b.D, b.best, chip_width, ctx->num_sms, st); });
   timed(ctx, ("finalize" + cls).c_str(), 0.0,
-        [&] { return launch_finalize(pc, dims, d_best, center, d_tables, want_cn0, d_cells, st); });
-  CK(cudaMemcpyAsync(host_out, d_cells, (size_t)n_ant * n_prn * sizeof(CellOut), cudaMemcpyDeviceToHost, st));
+        [&] { return launch_finalize(pc, dims, b.best, center, b.tables, want_cn0, b.cells, st); });
+  CK(cudaMemcpyAsync(host_out, b.cells, (size_t)n_ant * n_prn * sizeof(CellOut), cudaMemcpyDeviceToHost, st));
   ctx->d2h += (size_t)n_ant * n_prn * sizeof(CellOut);
   ctx->last_cells += (double)n_ant * nb * n_prn * (double)pc.P;
 }
@@ -517,24 +638,14 @@ int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, si
   }
 
   cudaStream_t st = ctx->stream;
-  CK(cudaEventRecord(ctx->ev0, st));
-  // antenna means over the whole rows
+  // buffers and uploads first (host side, outside any graph)
   double* d_mean = (double*)ctx->buf("mean", n_ant_total * sizeof(double));
-  timed(ctx, "antenna_means", 0.0, [&] { return launch_antenna_means(d_bits, (int)n_ant_total, row_bytes, d_mean, st); });
   int32_t* d_ants = (int32_t*)ctx->buf("ants", ants.size() * sizeof(int32_t));
-  CK(cudaMemcpyAsync(d_ants, ants.data(), ants.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   double* d_fc = (double*)ctx->buf("fc", fc.size() * sizeof(double));
-  CK(cudaMemcpyAsync(d_fc, fc.data(), fc.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-  ctx->h2d += ants.size() * sizeof(int32_t) + fc.size() * sizeof(double);
-
-  SampleSource src;
-  src.bits = d_bits;
-  src.row_bytes = row_bytes;
-  src.mean = d_mean;
-  src.ant = d_ants;
-  src.n_ant = (int)ants.size();
-  src.pc = kTau / fs;
-
+  std::vector<GroupBufs> gbufs;
+  for (const auto& g : groups)
+    gbufs.push_back(prepare_group(ctx, g, (int)ants.size(), nb,
+                                  "g" + std::to_string(g.pc.P) + "_" + std::to_string(g.pc.Lc)));
   size_t n_group_cells = 0;
   for (const auto& g : groups) n_group_cells += ants.size() * g.prns.size();
   CellOut* pinned = (CellOut*)ctx->host_pinned((n_group_cells ? n_group_cells : 1) * sizeof(CellOut));
@@ -546,9 +657,49 @@ int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, si
       off += ants.size() * groups[gi].prns.size();
     }
   }
-  for (size_t gi = 0; gi < groups.size(); ++gi)
-    run_group(ctx, groups[gi], src, d_fc, nb, opt->center_freq, opt->cn0, chip_width_of(fs),
-              "g" + std::to_string(groups[gi].pc.P) + "_" + std::to_string(groups[gi].pc.Lc), gout[gi]);
+  // the call's antenna list and Doppler grid
+  CK(cudaMemcpyAsync(d_ants, ants.data(), ants.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_fc, fc.data(), fc.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  ctx->h2d += ants.size() * sizeof(int32_t) + fc.size() * sizeof(double);
+
+  SampleSource src;
+  src.bits = d_bits;
+  src.row_bytes = row_bytes;
+  src.mean = d_mean;
+  src.ant = d_ants;
+  src.n_ant = (int)ants.size();
+  src.pc = kTau / fs;
+
+  auto enqueue = [&] {
+    // antenna means over the whole rows
+    timed(ctx, "antenna_means", 0.0,
+          [&] { return launch_antenna_means(d_bits, (int)n_ant_total, row_bytes, d_mean, st); });
+    for (size_t gi = 0; gi < groups.size(); ++gi)
+      enqueue_group(ctx, groups[gi], gbufs[gi], src, d_fc, nb, opt->center_freq, opt->cn0, chip_width_of(fs),
+                    gout[gi]);
+  };
+  CK(cudaEventRecord(ctx->ev0, st));
+  if (generic_consts.empty()) {
+    // the plan: everything the launches take by value or by address
+    std::string key;
+    char kb[160];
+    std::snprintf(kb, sizeof kb, "%p/%zu/%zu/%a/%a/%d/%d/%d/%d/%d/%d|", (const void*)d_bits, n_ant_total, row_bytes,
+                  fs, opt->center_freq, nb, opt->cn0, ctx->precision, ctx->test_flags, pfa_variant(10),
+                  chip_width_of(fs));
+    key = kb;
+    for (int32_t a : ants) key += std::to_string(a) + ",";
+    key += "|";
+    for (const auto& g : groups)
+      for (const auto& cp : g.prns) key += std::to_string(cp.first) + ":" + std::to_string(cp.second) + ",";
+    for (double f : fc) {
+      std::snprintf(kb, sizeof kb, "%a,", f);
+      key += kb;
+    }
+    run_planned(ctx, key, enqueue);
+  } else {
+    ctx->last_graph = TGA_GRAPH_NONE;
+    enqueue();
+  }
   // generic path: per (constellation, antenna, PRN), reference algorithm on the GPU
   std::map<int, std::vector<CellOut>> gen_out;  // constellation -> [prn][ant]
   for (int c : generic_consts) {
@@ -752,8 +903,9 @@ int acquire_single_impl(tga_ctx* ctx, int c, const float* h_sig, const double* h
   g.consts.push_back(c);
   g.prns.push_back({c, prn});
   ctx->h2d += n * (sizeof(float) + sizeof(double));
+  const GroupBufs gb = prepare_group(ctx, g, 1, nb, "single");
   CellOut* cell = (CellOut*)ctx->host_pinned(sizeof(CellOut));
-  run_group(ctx, g, src, d_fc, nb, center, 0, chip_width_of(fs), "single", cell);
+  enqueue_group(ctx, g, gb, src, d_fc, nb, center, 0, chip_width_of(fs), cell);
   CK(cudaStreamSynchronize(st));
   ctx->last_launches = kernel_launch_count();
   collect_times(ctx);
@@ -834,6 +986,8 @@ int tga_destroy(tga_ctx* ctx) {
   if (!ctx) return TGA_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   for (auto& kv : ctx->bufs)
     if (kv.second.p) cudaFree(kv.second.p);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -938,6 +1092,18 @@ int tga_set_precision(tga_ctx* ctx, int precision) {
 int tga_set_variant(tga_ctx* ctx, int lc, int variant) {
   if (!ctx || (lc != 1023 && lc != 4092 && lc != 10230) || variant < 0 || variant > 1) return TGA_ERR_INVALID_ARG;
   set_pfa_variant(lc / 1023, variant);
+  return TGA_OK;
+}
+
+int tga_set_graphs(tga_ctx* ctx, int enable) {
+  if (!ctx) return TGA_ERR_INVALID_ARG;
+  ctx->graphs_enabled = enable != 0;
+  return TGA_OK;
+}
+
+int tga_last_graph(const tga_ctx* ctx, int* state) {
+  if (!ctx || !state) return TGA_ERR_INVALID_ARG;
+  *state = ctx->last_graph;
   return TGA_OK;
 }
 

@@ -34,6 +34,7 @@ GPS_SEARCH_BAND = 6000.0
 ACR_TABLE = {GPS: 0, SBAS: 0, QZSS: 0, GALILEO: 1, BEIDOU: 2, L1C: 3}
 PRECISION_FP32, PRECISION_FP16_TC = 0, 1
 TEST_TC_SKIP_COMMIT = 1
+GRAPH_NONE, GRAPH_CAPTURED, GRAPH_REPLAYED = 0, 1, 2
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no sm_100 device", 4: "out of memory",
           5: "unsupported", 6: "timeout", 7: "capacity"}
@@ -155,6 +156,8 @@ def lib():
     L.tga_stream.argtypes = [_P]
     L.tga_stream.restype = ctypes.c_void_p
     L.tga_set_profiling.argtypes = [_P, i32]
+    L.tga_set_graphs.argtypes = [_P, i32]
+    L.tga_last_graph.argtypes = [_P, ctypes.POINTER(ctypes.c_int)]
     L.tga_set_variant.argtypes = [_P, i32, i32]
     L.tga_set_precision.argtypes = [_P, i32]
     L.tga_set_test_flags.argtypes = [_P, i32]
@@ -391,6 +394,20 @@ class Context:
     def set_precision(self, precision):
         """0 = FP32 (default), 1 = FP16 tensor-core search with FP32 refinement."""
         self._check(lib().tga_set_precision(self._h, int(precision)))
+
+    def set_profiling(self, enable):
+        """Per-kernel CUDA-event timing of later calls (tga_kernel_times)."""
+        self._check(lib().tga_set_profiling(self._h, 1 if enable else 0))
+
+    def set_graphs(self, enable):
+        """CUDA-graph capture and replay of repeated acquire_all plans (on by default)."""
+        self._check(lib().tga_set_graphs(self._h, 1 if enable else 0))
+
+    def last_graph(self):
+        """GRAPH_NONE (eager), GRAPH_CAPTURED or GRAPH_REPLAYED for the last acquire_all call."""
+        v = ctypes.c_int()
+        self._check(lib().tga_last_graph(self._h, ctypes.byref(v)))
+        return v.value
 
     def last_stats(self):
         cells, launches, ms = ctypes.c_double(), ctypes.c_int32(), ctypes.c_double()
