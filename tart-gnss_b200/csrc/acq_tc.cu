@@ -213,17 +213,17 @@ struct Tc3Cfg;
 template <>
 struct Tc3Cfg<1> {
   static constexpr int R2 = 33, R3 = 1, NST = 2, BC = 8, PAD2 = 1, PAD3 = 1;
-  static constexpr bool S2O = false;
+  static constexpr bool S2O = false, PADR1 = false;
 };
 template <>
 struct Tc3Cfg<4> {
   static constexpr int R2 = 12, R3 = 11, NST = 3, BC = 2, PAD2 = 3, PAD3 = 1;
-  static constexpr bool S2O = false;
+  static constexpr bool S2O = false, PADR1 = false;
 };
 template <>
 struct Tc3Cfg<10> {
-  static constexpr int R2 = 30, R3 = 11, NST = 3, BC = 1, PAD2 = 2, PAD3 = 1;
-  static constexpr bool S2O = true;
+  static constexpr int R2 = 30, R3 = 11, NST = 3, BC = 1, PAD2 = 1, PAD3 = 1;
+  static constexpr bool S2O = true, PADR1 = true;
 };
 
 // NCB: the non-coherent search (Lc = 1023 only), with |y|^2 sums in shared
@@ -250,8 +250,27 @@ struct T3 {
   static_assert(!S2O || R3 <= 12, "S2O: three groups of four d3");
   static constexpr int ROWS1 = R2 * R3, ROWS2 = S2O ? 384 : 31 * R3, ROWS3 = 31 * R2;
   static constexpr int ROWS3P = NST == 2 ? 0 : PAIR3 ? ROWS3 / 2 : ROWS3;  // stage-3 operand rows
-  static constexpr int NR1 = BC * ROWS1, NR2 = BC * ROWS2, NR3 = BC * ROWS3P;
-  static constexpr int TILES1 = (NR1 + 127) / 128, TILES2 = (NR2 + 127) / 128, TILES3 = (NR3 + 127) / 128;
+  // stage-1 operand rows of one residue.  With PADR1 the row of (d2, d3) is
+  // 32 d3 + d2 (rows 32 d3 + R2 .. 32 d3 + 31 are padding, never written nor
+  // read back): a warp's TMEM lanes then hold one d3 and its R2 values of
+  // d2, whose stage-2 stores (K entries d2, chunks LBO2 apart with LBO2 / 16
+  // odd) fall in 32 different banks.  Otherwise the rows are d3 R2 + d2.
+  static constexpr bool PADR1 = Tc3Cfg<M>::PADR1;
+  static_assert(!PADR1 || R2 <= 32, "PADR1: one warp of lanes per d3");
+  static constexpr int ROWS1P = PADR1 ? 32 * R3 : ROWS1;
+  // NR1 counts the product rows (units), NR1P the stage-1 operand rows
+  static constexpr int NR1 = BC * ROWS1, NR1P = BC * ROWS1P, NR2 = BC * ROWS2, NR3 = BC * ROWS3P;
+  static constexpr int TILES1 = (NR1P + 127) / 128, TILES2 = (NR2 + 127) / 128, TILES3 = (NR3 + 127) / 128;
+  // stage-1 operand row of product row r (residue r / ROWS1)
+  __device__ static __forceinline__ int arow1(int r) {
+    if constexpr (PADR1) {
+      const int s = r / ROWS1, u = r - s * ROWS1;
+      const int d3 = u / R2;
+      return s * ROWS1P + 32 * d3 + (u - d3 * R2);
+    } else {
+      return r;
+    }
+  }
   static constexpr int K1 = 64, K2 = pad16(2 * R2), K3 = NST == 2 ? 0 : PAIR3 ? 2 * P3OFF : pad16(2 * R3);
   static_assert(K2 <= 128 && K3 <= 64, "matrix rows of at most two (stage 2) or one swizzle atoms");
   static constexpr int N1 = K1, N2 = K2, N3 = K3;
@@ -602,7 +621,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       const int e = tid + k * NTS;
       const int j = e / T::NR1, r = e - j * T::NR1;
       const int u = r - (r / T::ROWS1) * T::ROWS1;
-      uoff[k] = e < T::UNITS ? ((uint32_t)(j * T::ROWS1 + u) << 16) | (uint32_t)(r * 16 + j * T::LBO1) : 0u;
+      uoff[k] = e < T::UNITS ? ((uint32_t)(j * T::ROWS1 + u) << 16) | (uint32_t)(T::arow1(r) * 16 + j * T::LBO1)
+                             : 0u;
     }
     uint32_t ph_done[2] = {0u, 0u}, ph_code[2] = {0u, 0u};
     bool failed = false;
@@ -666,9 +686,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
         if (task < NT2) {
           const int t = task / (4 * CS1), half = (task >> 2) % CS1;
           const int r = t * 128 + quad * 32 + lane;
-          const bool valid = r < T::NR1;
-          const int s = r / T::ROWS1, u = r - s * T::ROWS1;
-          const int d3 = u / R2, d2 = u - d3 * R2;
+          int s, d3, d2;
+          bool valid;
+          if constexpr (T::PADR1) {
+            s = r / T::ROWS1P;
+            const int u = r - s * T::ROWS1P;
+            d3 = u >> 5;
+            d2 = u & 31;
+            valid = s < BC && d2 < R2;
+          } else {
+            s = r / T::ROWS1;
+            const int u = r - s * T::ROWS1;
+            d3 = u / R2;
+            d2 = u - d3 * R2;
+            valid = r < T::NR1;
+          }
           // stage-2 row (t1, d3), K entry d2
           constexpr int T1_STRIDE = T::S2O ? 4 * 16 : R3 * 16;
           unsigned char* dst = A + (s * T::ROWS2 + (T::S2O ? (d3 >> 2) * 128 + (d3 & 3) : d3)) * 16 +
