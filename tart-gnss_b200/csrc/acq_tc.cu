@@ -213,17 +213,17 @@ struct Tc3Cfg;
 template <>
 struct Tc3Cfg<1> {
   static constexpr int R2 = 33, R3 = 1, NST = 2, BC = 8, PAD2 = 1, PAD3 = 1;
-  static constexpr bool S2O = false, PADR1 = false;
+  static constexpr bool S2O = false, PADR1 = false, T1F3 = false;
 };
 template <>
 struct Tc3Cfg<4> {
   static constexpr int R2 = 12, R3 = 11, NST = 3, BC = 2, PAD2 = 3, PAD3 = 1;
-  static constexpr bool S2O = false, PADR1 = false;
+  static constexpr bool S2O = true, PADR1 = false, T1F3 = true;
 };
 template <>
 struct Tc3Cfg<10> {
   static constexpr int R2 = 30, R3 = 11, NST = 3, BC = 1, PAD2 = 1, PAD3 = 1;
-  static constexpr bool S2O = true, PADR1 = true;
+  static constexpr bool S2O = true, PADR1 = true, T1F3 = false;
 };
 
 // NCB: the non-coherent search (Lc = 1023 only), with |y|^2 sums in shared
@@ -250,6 +250,12 @@ struct T3 {
   static_assert(!S2O || R3 <= 12, "S2O: three groups of four d3");
   static constexpr int ROWS1 = R2 * R3, ROWS2 = S2O ? 384 : 31 * R3, ROWS3 = 31 * R2;
   static constexpr int ROWS3P = NST == 2 ? 0 : PAIR3 ? ROWS3 / 2 : ROWS3;  // stage-3 operand rows
+  // T1F3: the paired stage-3 row of (t1, j = t2 / 2) is j 31 + t1 instead of
+  // t1 R2 / 2 + j (any order serves: the epilogue only takes the maximum
+  // over the rows); with S2O a warp's 8 consecutive t1 then store to 8
+  // consecutive rows
+  static constexpr bool T1F3 = Tc3Cfg<M>::T1F3;
+  static_assert(!T1F3 || PAIR3, "T1F3: paired stage 3");
   // stage-1 operand rows of one residue.  With PADR1 the row of (d2, d3) is
   // 32 d3 + d2 (rows 32 d3 + R2 .. 32 d3 + 31 are padding, never written nor
   // read back): a warp's TMEM lanes then hold one d3 and its R2 values of
@@ -746,14 +752,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
           if (T::PAIR3) {
             // paired stage-3 row (t1, t2 / 2) = s ROWS3P + t1 R2 / 2 + t2 / 2,
             // K entry d3 (t2 even) or P3OFF / 2 + d3 (t2 odd)
-            unsigned char* dst0 =
-                A + (s * T::ROWS3P + t1 * (R2 / 2)) * 16 + (d3 >> 2) * T::LBO3 + (d3 & 3) * 4;
+            constexpr int JSTRIDE = T::T1F3 ? 31 * 16 : 16;  // bytes between rows j and j + 1
+            unsigned char* dst0 = A + (s * T::ROWS3P + (T::T1F3 ? t1 : t1 * (R2 / 2))) * 16 + (d3 >> 2) * T::LBO3 +
+                                  (d3 & 3) * 4;
             unsigned char* dst1 = dst0 + (T::P3OFF / 8) * T::LBO3;
 #pragma unroll
             for (int h = 0; h < W2 / 2; ++h) {
               const int t2 = (W2 / 2) * half + h;
               if (valid && t2 < R2)
-                st_shared_u32(((t2 & 1) ? dst1 : dst0) + (t2 >> 1) * 16,
+                st_shared_u32(((t2 & 1) ? dst1 : dst0) + (t2 >> 1) * JSTRIDE,
                               pack_h2_sat(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h + 1])));
             }
           } else {
