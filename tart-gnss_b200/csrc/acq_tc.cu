@@ -180,7 +180,9 @@ constexpr int cmax3(int a, int b, int c) { return a > b ? (a > c ? a : c) : (b >
 
 constexpr int kSimtWarps = 12;  // a multiple of the 4 TMEM lane quadrants
 constexpr int kSimtThreads = 32 * kSimtWarps;
-constexpr int kTcThreads = kSimtThreads + 32;  // and the warp that issues the tensor-core work
+// and the warp that issues the tensor-core work, and the warp that fetches
+// the code blocks
+constexpr int kTcThreads = kSimtThreads + 64;
 constexpr int kTcTmemCols = 512;
 constexpr long long kWaitPolls = 1LL << 22;
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per wait on the tensor cores
@@ -453,7 +455,9 @@ __device__ __forceinline__ void tmem_ld_stage3(uint32_t taddr, int half, uint32_
 // runs two chains through the PRNs in pairs: chain x takes PRN 2 i + x (the
 // last PRN twice when their number is odd; the key update is idempotent).
 // Each chain has its own code block in shared memory, fetched for its next
-// PRN with one bulk copy as soon as the chain's products are formed.  Per
+// PRN with one bulk copy as soon as the chain's products are formed, by a
+// warp of its own (s_p1[x]: the 12 SIMT warps have read the block for the
+// last time), so that the MMA warp does nothing but wait, issue and commit.  Per
 // PRN pair:
 //   SIMT warps:  P1(a) P1(b) P2(a) P2(b) P3(a) P3(b) P4(a) P4(b)
 //   MMA warp:          M1(a) M1(b) M2(a) M2(b) M3(a) M3(b)
@@ -469,6 +473,51 @@ __device__ __forceinline__ void tmem_ld_stage3(uint32_t taddr, int half, uint32_
 // sums of its epilogue outputs in shared memory and takes the row maximum
 // after the last block.  The Z of the next block is loaded into the
 // registers while the current block's transform runs.
+// The code warp's thread: after the 12 SIMT warps have formed chain x's
+// products of a PRN's last block (s_p1[x]), bulk-copy the chain's next code
+// block into its slot (s_code[x]).  Its own function, so that its registers
+// are allocated apart from the SIMT warps'.
+template <class T, bool NCB>
+__device__ __noinline__ void code_warp(const Tc3Params& p, uint64_t* s_p1, uint64_t* s_code, unsigned char* CODE0,
+                                       int n_rounds) {
+  auto prn_of = [&](int r, int x) -> int { return 2 * r + x < p.n_prn ? 2 * r + x : p.n_prn - 1; };
+  uint32_t ph_p1[2] = {0u, 0u};
+  int fetches[2] = {0, 0};
+  bool ok = true;
+  // code block of chain x for round r of work item w
+  auto fetch = [&](int x, int w, int r) {
+    const int hyp = NCB ? 0 : (w / p.groups) & 1;
+    const uint4* src = p.d16 + ((size_t)prn_of(r, x) * 2 + hyp) * 8 * T::ROWS1;
+    mbar_arrive_expect_tx(&s_code[x], (uint32_t)T::CODE_BYTES);
+    bulk_g2s(smem_addr(CODE0 + x * T::CODE_REGION), src, (uint32_t)T::CODE_BYTES, &s_code[x]);
+    ++fetches[x];
+  };
+  if ((int)blockIdx.x < p.n_items && n_rounds > 0) {
+    fetch(0, blockIdx.x, 0);
+    fetch(1, blockIdx.x, 0);
+  }
+#pragma unroll 1
+  for (int w = blockIdx.x; w < p.n_items && ok; w += gridDim.x)
+#pragma unroll 1
+    for (int r = 0; r < n_rounds && ok; ++r)
+#pragma unroll 1
+      for (int x = 0; x < 2 && ok; ++x) {
+        if (!bounded_wait(&s_p1[x], ph_p1[x])) {
+          ok = false;
+          break;
+        }
+        ph_p1[x] ^= 1u;
+        if (r + 1 < n_rounds)
+          fetch(x, w, r + 1);
+        else if (w + (int)gridDim.x < p.n_items)
+          fetch(x, w + gridDim.x, 0);
+      }
+  // drain: the last bulk copy of each chain
+  for (int x = 0; x < 2; ++x)
+    if (fetches[x] > 0) bounded_wait(&s_code[x], (uint32_t)((fetches[x] - 1) & 1));
+  if (!ok) atomicExch(p.err, 1);
+}
+
 template <int M, bool NCB>
 __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   using T = T3<M, NCB>;
@@ -485,7 +534,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   constexpr int LB4 = TPW4 < 2 ? TPW4 : 2;
   constexpr int kBatch = (U + 1) / 2;
   extern __shared__ unsigned char smem_raw[];
-  __shared__ uint64_t s_ready[2], s_done[2], s_code[2];
+  __shared__ uint64_t s_ready[2], s_done[2], s_code[2], s_p1[2];
   __shared__ uint32_t s_tmem;
   const uint32_t raw = smem_addr(smem_raw);
   unsigned char* A0 = smem_raw + ((1024 - (raw & 1023)) & 1023);
@@ -506,6 +555,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       mbar_init(&s_ready[x], NW);
       mbar_init(&s_done[x], 1);
       mbar_init(&s_code[x], 1);
+      mbar_init(&s_p1[x], NW);
     }
   }
   // operand rows and K entries that no stage writes (padding) must hold
@@ -529,20 +579,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       const uint64_t db2 = Lay<T::KB2>::desc(smem_addr(B2));
       const uint64_t db3 = Lay<T::KB3>::desc(smem_addr(B3));
       uint32_t ph_ready[2] = {0u, 0u};
-      int commits[2] = {0, 0}, fetches[2] = {0, 0};
+      int commits[2] = {0, 0};
       bool ok = true;
-      // code block of chain x for round r of work item w
-      auto fetch = [&](int x, int w, int r) {
-        const int hyp = NCB ? 0 : (w / p.groups) & 1;
-        const uint4* src = p.d16 + ((size_t)prn_of(r, x) * 2 + hyp) * 8 * T::ROWS1;
-        mbar_arrive_expect_tx(&s_code[x], (uint32_t)T::CODE_BYTES);
-        bulk_g2s(smem_addr(CODE0 + x * T::CODE_REGION), src, (uint32_t)T::CODE_BYTES, &s_code[x]);
-        ++fetches[x];
-      };
-      if ((int)blockIdx.x < p.n_items && n_rounds > 0) {
-        fetch(0, blockIdx.x, 0);
-        fetch(1, blockIdx.x, 0);
-      }
       for (int w = blockIdx.x; w < p.n_items && ok; w += gridDim.x) {
         for (int r = 0; r < n_rounds && ok; ++r) {
 #pragma unroll 1
@@ -595,26 +633,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
                 mma_commit(&s_done[x]);
                 ++commits[x];
               }
-              // chain x has read its code block for the last time: fetch its next one
-              if (st == 0 && b == B - 1) {
-                if (r + 1 < n_rounds)
-                  fetch(x, w, r + 1);
-                else if (w + (int)gridDim.x < p.n_items)
-                  fetch(x, w + gridDim.x, 0);
-              }
             }
           }
          }
         }
       }
-      // drain: the last commit and the last bulk copy of each chain (after a
-      // timeout they may still be in flight)
-      for (int x = 0; x < 2; ++x) {
+      // drain: the last commit of each chain (after a timeout it may still
+      // be in flight)
+      for (int x = 0; x < 2; ++x)
         if (commits[x] > 0) bounded_wait(&s_done[x], (uint32_t)((commits[x] - 1) & 1));
-        if (fetches[x] > 0) bounded_wait(&s_code[x], (uint32_t)((fetches[x] - 1) & 1));
-      }
       if (!ok) atomicExch(p.err, 1);
     }
+    __syncwarp();
+  } else if (warp == NW + 1) {
+    // ---------------- code warp: one thread fetches the code blocks ----------------
+    if (lane == 0) code_warp<T, NCB>(p, s_p1, s_code, CODE0, n_rounds);
     __syncwarp();
   } else {
     // ---------------- SIMT warps ----------------
@@ -669,112 +702,120 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
         }
       }
     };
+    // P2 and P3 read the accumulators in chunks of 16 columns (8 complex
+    // outputs) through two register buffers: the load of chunk q + 1 is in
+    // flight while chunk q is rounded and stored
     // ---- P2: stage-1 accumulators -> stage-2 rows (t1, d3), K = d2 ----
     auto p2 = [&](int x) {
       unsigned char* A = A0 + x * T::A_BYTES;
       const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
-      uint32_t v[TPW2][32];
-#pragma unroll
-      for (int i = 0; i < TPW2; ++i) {
-        const int task = warp + i * NW;
+      constexpr int NQ = TPW2 * 2;  // a task is 32 columns
+      uint32_t buf[2][16];
+      auto load = [&](int q) {
+        const int task = warp + (q >> 1) * NW;
         if (task < NT2) {
           const int t = task / (4 * CS1), half = (task >> 2) % CS1;
-          uint32_t(&a)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[i][0]);
-          uint32_t(&b)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[i][16]);
-          tmem_ld16(tb + (uint32_t)(t * T::N1 + 32 * half), a);
-          tmem_ld16(tb + (uint32_t)(t * T::N1 + 32 * half + 16), b);
+          tmem_ld16(tb + (uint32_t)(t * T::N1 + 32 * half + 16 * (q & 1)), buf[q & 1]);
         }
-      }
+      };
+      auto store = [&](int q) {
+        const int task = warp + (q >> 1) * NW;
+        if (task >= NT2) return;
+        const int t = task / (4 * CS1), half = (task >> 2) % CS1;
+        const int r = t * 128 + quad * 32 + lane;
+        int s, d3, d2;
+        bool valid;
+        if constexpr (T::PADR1) {
+          s = r / T::ROWS1P;
+          const int u = r - s * T::ROWS1P;
+          d3 = u >> 5;
+          d2 = u & 31;
+          valid = s < BC && d2 < R2;
+        } else {
+          s = r / T::ROWS1;
+          const int u = r - s * T::ROWS1;
+          d3 = u / R2;
+          d2 = u - d3 * R2;
+          valid = r < T::NR1;
+        }
+        // stage-2 row (t1, d3), K entry d2
+        constexpr int T1_STRIDE = T::S2O ? 4 * 16 : R3 * 16;
+        unsigned char* dst = A + (s * T::ROWS2 + (T::S2O ? (d3 >> 2) * 128 + (d3 & 3) : d3)) * 16 +
+                             (d2 >> 2) * T::LBO2 + (d2 & 3) * 4;
+#pragma unroll
+        for (int h = 0; h < 8; ++h) {
+          const int t1 = 16 * half + 8 * (q & 1) + h;
+          if (valid && t1 < 31)
+            st_shared_u32(dst + t1 * T1_STRIDE,
+                          pack_h2_sat(__uint_as_float(buf[q & 1][2 * h]), __uint_as_float(buf[q & 1][2 * h + 1])));
+        }
+      };
+      load(0);
       tmem_wait_ld();
 #pragma unroll
-      for (int i = 0; i < TPW2; ++i) {
-        const int task = warp + i * NW;
-        if (task < NT2) {
-          const int t = task / (4 * CS1), half = (task >> 2) % CS1;
-          const int r = t * 128 + quad * 32 + lane;
-          int s, d3, d2;
-          bool valid;
-          if constexpr (T::PADR1) {
-            s = r / T::ROWS1P;
-            const int u = r - s * T::ROWS1P;
-            d3 = u >> 5;
-            d2 = u & 31;
-            valid = s < BC && d2 < R2;
-          } else {
-            s = r / T::ROWS1;
-            const int u = r - s * T::ROWS1;
-            d3 = u / R2;
-            d2 = u - d3 * R2;
-            valid = r < T::NR1;
-          }
-          // stage-2 row (t1, d3), K entry d2
-          constexpr int T1_STRIDE = T::S2O ? 4 * 16 : R3 * 16;
-          unsigned char* dst = A + (s * T::ROWS2 + (T::S2O ? (d3 >> 2) * 128 + (d3 & 3) : d3)) * 16 +
-                               (d2 >> 2) * T::LBO2 + (d2 & 3) * 4;
-#pragma unroll
-          for (int h = 0; h < 16; ++h) {
-            const int t1 = 16 * half + h;
-            if (valid && t1 < 31)
-              st_shared_u32(dst + t1 * T1_STRIDE,
-                            pack_h2_sat(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h + 1])));
-          }
-        }
+      for (int q = 0; q < NQ; ++q) {
+        if (q + 1 < NQ) load(q + 1);
+        store(q);
+        if (q + 1 < NQ) tmem_wait_ld();
       }
     };
     // ---- P3: stage-2 accumulators -> stage-3 rows (t1, t2), K = d3 ----
     auto p3 = [&](int x) {
       unsigned char* A = A0 + x * T::A_BYTES;
       const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
-      uint32_t v[TPW3][W2];
-#pragma unroll
-      for (int i = 0; i < TPW3; ++i) {
-        const int task = warp + i * NW;
+      constexpr int CPT = W2 / 16;  // chunks per task
+      constexpr int NQ = TPW3 * CPT;
+      uint32_t buf[2][16];
+      auto load = [&](int q) {
+        const int task = warp + (q / CPT) * NW;
         if (task < NT3) {
           const int t = task / (4 * CS2), half = (task >> 2) % CS2;
+          tmem_ld16(tb + (uint32_t)(t * T::N2 + W2 * half + 16 * (q % CPT)), buf[q & 1]);
+        }
+      };
+      auto store = [&](int q) {
+        const int task = warp + (q / CPT) * NW;
+        if (task >= NT3) return;
+        const int t = task / (4 * CS2), half = (task >> 2) % CS2;
+        const int r = t * 128 + quad * 32 + lane;
+        const int s = r / T::ROWS2, qq = r - s * T::ROWS2;
+        const int t1 = T::S2O ? (qq & 127) >> 2 : qq / R3;
+        const int d3 = T::S2O ? 4 * (qq >> 7) + (qq & 3) : qq - t1 * R3;
+        const bool valid = r < T::NR2 && (!T::S2O || (d3 < R3 && t1 < 31));
+        const uint32_t* v = buf[q & 1];
+        if (T::PAIR3) {
+          // paired stage-3 row (t1, t2 / 2) = s ROWS3P + t1 R2 / 2 + t2 / 2
+          // (T1F3: s ROWS3P + (t2 / 2) 31 + t1), K entry d3 (t2 even) or
+          // P3OFF / 2 + d3 (t2 odd)
+          constexpr int JSTRIDE = T::T1F3 ? 31 * 16 : 16;  // bytes between rows j and j + 1
+          unsigned char* dst0 = A + (s * T::ROWS3P + (T::T1F3 ? t1 : t1 * (R2 / 2))) * 16 + (d3 >> 2) * T::LBO3 +
+                                (d3 & 3) * 4;
+          unsigned char* dst1 = dst0 + (T::P3OFF / 8) * T::LBO3;
 #pragma unroll
-          for (int c = 0; c < W2 / 16; ++c) {
-            uint32_t(&a)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[i][16 * c]);
-            tmem_ld16(tb + (uint32_t)(t * T::N2 + W2 * half + 16 * c), a);
+          for (int h = 0; h < 8; ++h) {
+            const int t2 = (W2 / 2) * half + 8 * (q % CPT) + h;
+            if (valid && t2 < R2)
+              st_shared_u32(((t2 & 1) ? dst1 : dst0) + (t2 >> 1) * JSTRIDE,
+                            pack_h2_sat(__uint_as_float(v[2 * h]), __uint_as_float(v[2 * h + 1])));
+          }
+        } else {
+          // stage-3 row (t1, t2) = s ROWS3 + t1 R2 + t2, K entry d3
+          unsigned char* dst = A + (s * T::ROWS3 + t1 * R2) * 16 + (d3 >> 2) * T::LBO3 + (d3 & 3) * 4;
+#pragma unroll
+          for (int h = 0; h < 8; ++h) {
+            const int t2 = (W2 / 2) * half + 8 * (q % CPT) + h;
+            if (valid && t2 < R2)
+              st_shared_u32(dst + t2 * 16, pack_h2_sat(__uint_as_float(v[2 * h]), __uint_as_float(v[2 * h + 1])));
           }
         }
-      }
+      };
+      load(0);
       tmem_wait_ld();
 #pragma unroll
-      for (int i = 0; i < TPW3; ++i) {
-        const int task = warp + i * NW;
-        if (task < NT3) {
-          const int t = task / (4 * CS2), half = (task >> 2) % CS2;
-          const int r = t * 128 + quad * 32 + lane;
-          const int s = r / T::ROWS2, q = r - s * T::ROWS2;
-          const int t1 = T::S2O ? (q & 127) >> 2 : q / R3;
-          const int d3 = T::S2O ? 4 * (q >> 7) + (q & 3) : q - t1 * R3;
-          const bool valid = r < T::NR2 && (!T::S2O || (d3 < R3 && t1 < 31));
-          if (T::PAIR3) {
-            // paired stage-3 row (t1, t2 / 2) = s ROWS3P + t1 R2 / 2 + t2 / 2,
-            // K entry d3 (t2 even) or P3OFF / 2 + d3 (t2 odd)
-            constexpr int JSTRIDE = T::T1F3 ? 31 * 16 : 16;  // bytes between rows j and j + 1
-            unsigned char* dst0 = A + (s * T::ROWS3P + (T::T1F3 ? t1 : t1 * (R2 / 2))) * 16 + (d3 >> 2) * T::LBO3 +
-                                  (d3 & 3) * 4;
-            unsigned char* dst1 = dst0 + (T::P3OFF / 8) * T::LBO3;
-#pragma unroll
-            for (int h = 0; h < W2 / 2; ++h) {
-              const int t2 = (W2 / 2) * half + h;
-              if (valid && t2 < R2)
-                st_shared_u32(((t2 & 1) ? dst1 : dst0) + (t2 >> 1) * JSTRIDE,
-                              pack_h2_sat(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h + 1])));
-            }
-          } else {
-            // stage-3 row (t1, t2) = s ROWS3 + t1 R2 + t2, K entry d3
-            unsigned char* dst = A + (s * T::ROWS3 + t1 * R2) * 16 + (d3 >> 2) * T::LBO3 + (d3 & 3) * 4;
-#pragma unroll
-            for (int h = 0; h < W2 / 2; ++h) {
-              const int t2 = (W2 / 2) * half + h;
-              if (valid && t2 < R2)
-                st_shared_u32(dst + t2 * 16,
-                              pack_h2_sat(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h + 1])));
-            }
-          }
-        }
+      for (int q = 0; q < NQ; ++q) {
+        if (q + 1 < NQ) load(q + 1);
+        store(q);
+        if (q + 1 < NQ) tmem_wait_ld();
       }
     };
     // ---- P4: |y|^2 maximum over the stage-3 outputs of chain x ----
@@ -925,7 +966,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
         signal(x);
         return true;
       };
-      for (int x = 0; x < 2 && !failed; ++x) failed = !products(x, true);
+      // after the products of a PRN's last block the code warp may refill
+      // the chain's code block
+      auto released = [&](int x) {
+        if (lane == 0) mbar_arrive(&s_p1[x]);
+      };
+      for (int x = 0; x < 2 && !failed; ++x) {
+        failed = !products(x, true);
+        if (!failed && B == 1) released(x);
+      }
       for (int r = 0; r < n_rounds && !failed; ++r)
        for (int b = 0; b < B && !failed; ++b) {
         const bool more = b + 1 < B || r + 1 < n_rounds;  // a next block of this item follows
@@ -969,7 +1018,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
           const unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(pmax));
           if (lane == 0 && bits != 0u)
             atomicMax(p.keys + (size_t)ab_h * p.n_prn + prn_of(r, x), (unsigned long long)bits << 32);
-          if (more) failed = !products(x, b + 1 == B);
+          // the next products are those of block b + 1, or of the next
+          // round's block 0
+          if (more) {
+            failed = !products(x, b + 1 == B);
+            if (!failed && (NCB ? (b + 1 < B ? b + 1 : 0) == B - 1 : true)) released(x);
+          }
         }
        }
     }
