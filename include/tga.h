@@ -202,6 +202,22 @@ int tga_acquire_all_device(tga_ctx* ctx, const uint8_t* d_packed_bits, size_t n_
                            size_t row_bytes, double sampling_freq, const tga_all_options* opt,
                            tga_cell* out, size_t out_capacity, size_t* n_out);
 
+/* --benchmark (main.rs:482-694): for GPS, Galileo, BeiDou, SBAS, QZSS and
+ * L1C in that order, one PRN (1, 1, 1, 120, 184, 1) on antenna 0 of the
+ * observation.  setup_s = host extraction of every antenna's de-meaned f32
+ * window and phasepoints (main.rs:497-517), search_s = the single-PRN
+ * acquisition through tga_acquire_single (wall clock, result read back).
+ * out receives 6 entries. */
+typedef struct {
+  int32_t constellation;
+  int32_t prn;
+  double setup_s;
+  double search_s;
+  tga_result result;
+} tga_bench_entry;
+int tga_benchmark(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, size_t row_bytes,
+                  double sampling_freq, tga_bench_entry out[6]);
+
 /* Number of cells tga_acquire_all would produce for these options. */
 int tga_all_cell_count(size_t n_ant, const tga_all_options* opt, size_t* n_cells);
 

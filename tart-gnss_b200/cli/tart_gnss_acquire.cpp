@@ -208,49 +208,28 @@ int main(int argc, char** argv) {
 
   if (a.benchmark) {
     // main.rs:482-694: one PRN per constellation on antenna 0; setup = antenna
-    // extraction, search = the single-PRN acquisition.
-    struct E { const char* name; int c, prn; };
-    const E es[6] = {{"GPS", TGA_GPS, 1}, {"Galileo", TGA_GALILEO, 1}, {"BeiDou", TGA_BEIDOU, 1},
-                     {"SBAS", TGA_SBAS, 120}, {"QZSS", TGA_QZSS, 184}, {"L1C", TGA_L1C, 1}};
+    // extraction, search = the single-PRN acquisition (tga_benchmark).
+    const char* names[6] = {"GPS", "Galileo", "BeiDou", "SBAS", "QZSS", "L1C"};
+    std::fprintf(stderr, "Running benchmark (one PRN per constellation, setup timed separately)...\n");
+    tga_bench_entry be[6];
+    rc = tga_benchmark(ctx, obs.data, n_ant, obs.row_bytes, fs, be);
+    if (rc != TGA_OK) {
+      std::fprintf(stderr, "%s\n", tga_last_error(ctx));
+      return 1;
+    }
     std::string json = "[";
     double tot_setup = 0, tot_search = 0;
-    std::fprintf(stderr, "Running benchmark (one PRN per constellation, setup timed separately)...\n");
     for (int e = 0; e < 6; ++e) {
-      const E& en = es[e];
-      size_t per = (en.c == TGA_GPS || en.c == TGA_SBAS || en.c == TGA_QZSS) ? (size_t)(fs / 1000.0)
-                   : (size_t)(fs * ((en.c == TGA_GALILEO) ? 4092.0 / 1.023e6 : 10230.0 / 1.023e6));
-      const size_t n_rec = obs.row_bytes * 8, n = std::min(2 * per, n_rec);
-      std::fprintf(stderr, "  %s (PRN %d)...\n", en.name, en.prn);
-      auto t0 = std::chrono::steady_clock::now();
-      std::vector<float> sig(n);
-      std::vector<double> pp(n);
-      long ones = 0;
-      for (size_t k = 0; k < obs.row_bytes; ++k) ones += __builtin_popcount(obs.data[k]);
-      const double mean = (2.0 * (double)ones - (double)n_rec) / (double)n_rec;
-      const double pc = 6.283185307179586 / fs;
-      for (size_t k = 0; k < n; ++k) {
-        const double v = ((obs.data[k >> 3] >> (7 - (k & 7))) & 1) ? 1.0 : -1.0;
-        sig[k] = (float)(v - mean);
-        pp[k] = pc * (double)k;
-      }
-      auto t1 = std::chrono::steady_clock::now();
-      tga_result r;
-      rc = tga_acquire_single(ctx, en.c, sig.data(), pp.data(), n, fs, 4.092e6, 6000.0, en.prn, per, &r);
-      auto t2 = std::chrono::steady_clock::now();
-      if (rc != TGA_OK) {
-        std::fprintf(stderr, "%s\n", tga_last_error(ctx));
-        return 1;
-      }
-      const double setup = std::chrono::duration<double>(t1 - t0).count();
-      const double search = std::chrono::duration<double>(t2 - t1).count();
+      const double setup = be[e].setup_s, search = be[e].search_s;
+      std::fprintf(stderr, "  %s (PRN %d)...\n", names[e], be[e].prn);
       tot_setup += setup;
       tot_search += search;
-      std::fprintf(stderr, "    %s: setup=%.4fs  search=%.4fs  total=%.4fs\n", en.name, setup, search, setup + search);
+      std::fprintf(stderr, "    %s: setup=%.4fs  search=%.4fs  total=%.4fs\n", names[e], setup, search, setup + search);
       char b1[64], b2[64], b3[64];
       tga_format_f64(setup, b1, sizeof b1);
       tga_format_f64(search, b2, sizeof b2);
       tga_format_f64(setup + search, b3, sizeof b3);
-      json += std::string(e ? ",\n" : "\n") + "  {\n    \"constellation\": \"" + en.name + "\",\n    \"prns\": 1,\n" +
+      json += std::string(e ? ",\n" : "\n") + "  {\n    \"constellation\": \"" + names[e] + "\",\n    \"prns\": 1,\n" +
               "    \"setup_s\": " + b1 + ",\n    \"search_s\": " + b2 + ",\n    \"duration_s\": " + b3 + "\n  }";
     }
     json += "\n]";

@@ -1047,6 +1047,55 @@ int tga_acquire_all(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, si
   });
 }
 
+int tga_benchmark(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, size_t row_bytes, double fs,
+                  tga_bench_entry out[6]) {
+  return guarded(ctx, [&] {
+    if (!h_packed_bits || !out || n_ant == 0 || row_bytes == 0) throw InvalidArg("empty observation or null output");
+    if (!(fs > 0.0)) throw InvalidArg("sampling frequency must be positive");
+    // main.rs:518-595: samples per period as `usize` truncations of f64 products
+    const size_t per_ms = (size_t)(fs / 1000.0);
+    const size_t per_gal = (size_t)(fs * (4092.0 / 1.023e6));
+    const size_t per_10ms = (size_t)(fs * (10230.0 / 1.023e6));
+    struct E {
+      int c, prn;
+      size_t per;
+    };
+    const E es[6] = {{TGA_GPS, 1, per_ms},    {TGA_GALILEO, 1, per_gal}, {TGA_BEIDOU, 1, per_10ms},
+                     {TGA_SBAS, 120, per_ms}, {TGA_QZSS, 184, per_ms},   {TGA_L1C, 1, per_10ms}};
+    const size_t n_rec = row_bytes * 8;
+    const double pc = kTau / fs;
+    for (int e = 0; e < 6; ++e) {
+      const auto t0 = std::chrono::steady_clock::now();
+      // setup: every antenna's window, as extract_ant_data (main.rs:497-517)
+      const size_t n = std::min(2 * es[e].per, n_rec);
+      std::vector<std::vector<float>> sig(n_ant, std::vector<float>(n));
+      std::vector<double> pp(n);
+      for (size_t k = 0; k < n; ++k) pp[k] = pc * (double)k;
+      for (size_t a = 0; a < n_ant; ++a) {
+        const uint8_t* row = h_packed_bits + a * row_bytes;
+        long long ones = 0;
+        for (size_t k = 0; k < row_bytes; ++k) ones += __builtin_popcount(row[k]);
+        const double mean = (2.0 * (double)ones - (double)n_rec) / (double)n_rec;
+        for (size_t k = 0; k < n; ++k) sig[a][k] = (float)((((row[k >> 3] >> (7 - (k & 7))) & 1) ? 1.0 : -1.0) - mean);
+      }
+      const auto t1 = std::chrono::steady_clock::now();
+      // every entry uses IF 4.092 MHz and a 6 kHz band (acquisition.rs:72-75,
+      // sbas.rs:24-27, qzss.rs:24-27, l1c.rs:27-30, main.rs:525-590)
+      tga_result r;
+      const int rc =
+          acquire_single_impl(ctx, es[e].c, sig[0].data(), pp.data(), n, fs, 4.092e6, 6000.0, es[e].prn, es[e].per, &r);
+      if (rc != TGA_OK) return rc;
+      const auto t2 = std::chrono::steady_clock::now();
+      out[e].constellation = es[e].c;
+      out[e].prn = es[e].prn;
+      out[e].setup_s = std::chrono::duration<double>(t1 - t0).count();
+      out[e].search_s = std::chrono::duration<double>(t2 - t1).count();
+      out[e].result = r;
+    }
+    return TGA_OK;
+  });
+}
+
 int tga_all_cell_count(size_t n_ant, const tga_all_options* opt, size_t* n_cells) {
   if (!opt || !n_cells) return TGA_ERR_INVALID_ARG;
   try {

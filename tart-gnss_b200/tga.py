@@ -53,6 +53,11 @@ class Result(ctypes.Structure):
                 ("hypothesis", ctypes.c_int32), ("path", ctypes.c_int32)]
 
 
+class BenchEntry(ctypes.Structure):
+    _fields_ = [("constellation", ctypes.c_int32), ("prn", ctypes.c_int32), ("setup_s", ctypes.c_double),
+                ("search_s", ctypes.c_double), ("result", Result)]
+
+
 class Cell(ctypes.Structure):
     _fields_ = [("constellation", ctypes.c_int32), ("prn", ctypes.c_int32), ("antenna", ctypes.c_int32),
                 ("best_freq_idx", ctypes.c_int32), ("best_codephase", ctypes.c_int64),
@@ -157,6 +162,7 @@ def lib():
     L.tga_stream.restype = ctypes.c_void_p
     L.tga_set_profiling.argtypes = [_P, i32]
     L.tga_set_graphs.argtypes = [_P, i32]
+    L.tga_benchmark.argtypes = [_P, _P, sz, sz, dbl, _P]
     L.tga_last_graph.argtypes = [_P, ctypes.POINTER(ctypes.c_int)]
     L.tga_set_variant.argtypes = [_P, i32, i32]
     L.tga_set_precision.argtypes = [_P, i32]
@@ -394,6 +400,16 @@ class Context:
     def set_precision(self, precision):
         """0 = FP32 (default), 1 = FP16 tensor-core search with FP32 refinement."""
         self._check(lib().tga_set_precision(self._h, int(precision)))
+
+    def benchmark(self, packed_bits, sampling_freq):
+        """--benchmark: one PRN per constellation on antenna 0, setup and
+        search timed separately; list of dicts in the reference's order."""
+        bits = np.ascontiguousarray(packed_bits, dtype=np.uint8)
+        out = (BenchEntry * 6)()
+        self._check(lib().tga_benchmark(self._h, _ptr(bits), bits.shape[0], bits.shape[1], float(sampling_freq),
+                                        out))
+        return [{"constellation": e.constellation, "prn": e.prn, "setup_s": e.setup_s, "search_s": e.search_s,
+                 "result": e.result} for e in out]
 
     def set_profiling(self, enable):
         """Per-kernel CUDA-event timing of later calls (tga_kernel_times)."""

@@ -1,6 +1,8 @@
 """The tart-gnss-acquire CLI end to end on a cut-down copy of the reference's
 real TART recording: acquisition JSON (--gps --cn0) and the RFI report
-(--rfi) equal what the library produces for the same rows."""
+(--rfi) equal what the library produces for the same rows; --benchmark
+prints the reference's schema, and tga_benchmark's searches equal the
+single-PRN calls they time."""
 import json
 import os
 import subprocess
@@ -43,3 +45,35 @@ def test_cli_rfi_json(tmp_path):
         want = ctx.rfi_scan(o["data"], o["sampling_frequency"], as_json=True)
     assert open(path).read().strip() == want.strip()
     assert len(json.loads(want)["channels"]) == 24
+
+
+def test_cli_benchmark_schema():
+    doc = json.loads(_run(["--benchmark"]))
+    assert [d["constellation"] for d in doc] == ["GPS", "Galileo", "BeiDou", "SBAS", "QZSS", "L1C"]
+    for d in doc:
+        assert list(d) == ["constellation", "prns", "setup_s", "search_s", "duration_s"]
+        assert d["prns"] == 1 and d["search_s"] > 0 and d["setup_s"] >= 0
+        assert abs(d["duration_s"] - d["setup_s"] - d["search_s"]) < 1e-9
+
+
+def test_library_benchmark_equals_single_prn_calls():
+    import numpy as np
+    o = tga.read_hdf5(FIXTURE)
+    bits, fs = o["data"], o["sampling_frequency"]
+    with tga.Context(0) as ctx:
+        entries = ctx.benchmark(bits, fs)
+        assert [(e["constellation"], e["prn"]) for e in entries] == [
+            (tga.GPS, 1), (tga.GALILEO, 1), (tga.BEIDOU, 1), (tga.SBAS, 120), (tga.QZSS, 184), (tga.L1C, 1)]
+        ub = np.unpackbits(bits[0]).astype(np.float64) * 2 - 1
+        sig_all = (ub - ub.mean()).astype(np.float32)
+        for e in entries:
+            per = {tga.GALILEO: int(fs * (4092.0 / 1.023e6)), tga.BEIDOU: int(fs * (10230.0 / 1.023e6)),
+                   tga.L1C: int(fs * (10230.0 / 1.023e6))}.get(e["constellation"], int(fs / 1000.0))
+            n = min(2 * per, len(sig_all))
+            pp = 2 * np.pi / fs * np.arange(n)
+            r = ctx.acquire_single(e["constellation"], sig_all[:n], pp, fs, 4.092e6, 6000.0, e["prn"], per)
+            g = e["result"]
+            assert (g.best_codephase, g.best_freq_idx, g.hypothesis) == (r.best_codephase, r.best_freq_idx,
+                                                                         r.hypothesis)
+            assert g.signal_strength == r.signal_strength and g.second_peak == r.second_peak
+            assert e["search_s"] > 0
