@@ -529,6 +529,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   constexpr int HALVES3 = T::PAIR3 ? 2 : 1;
   constexpr int NT2 = T::TILES1 * 4 * CS1, NT3 = T::TILES2 * 4 * CS2, NT4 = T::LAST_TILES * 4 * HALVES3;
   constexpr int TPW2 = (NT2 + NW - 1) / NW, TPW3 = (NT3 + NW - 1) / NW, TPW4 = (NT4 + NW - 1) / NW;
+  // P2 / P3: the 12 warps cover the 4 lane quadrants of 3 tiles at a time
+  static_assert(NW == 12 && T::TILES1 % 3 == 0 && (T::NST == 2 || T::TILES2 % 3 == 0), "P2/P3 task map");
   // P4 reads TMEM in batches of LB4 tasks: all loads of a batch in flight,
   // one wait
   constexpr int LB4 = TPW4 < 2 ? TPW4 : 2;
@@ -709,19 +711,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
     auto p2 = [&](int x) {
       unsigned char* A = A0 + x * T::A_BYTES;
       const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
+      // warp w reads lane quadrant w % 4 of tiles w / 4 + 3 k, all CS1
+      // column halves: task i is tile w / 4 + 3 (i / CS1), half i % CS1,
+      // known at compile time but for the tile
       constexpr int NQ = TPW2 * 2;  // a task is 32 columns
       uint32_t buf[2][16];
       auto load = [&](int q) {
-        const int task = warp + (q >> 1) * NW;
-        if (task < NT2) {
-          const int t = task / (4 * CS1), half = (task >> 2) % CS1;
-          tmem_ld16(tb + (uint32_t)(t * T::N1 + 32 * half + 16 * (q & 1)), buf[q & 1]);
-        }
+        const int i = q >> 1, t = (warp >> 2) + 3 * (i / CS1), half = i % CS1;
+        tmem_ld16(tb + (uint32_t)(t * T::N1 + 32 * half + 16 * (q & 1)), buf[q & 1]);
       };
       auto store = [&](int q) {
-        const int task = warp + (q >> 1) * NW;
-        if (task >= NT2) return;
-        const int t = task / (4 * CS1), half = (task >> 2) % CS1;
+        const int i = q >> 1, t = (warp >> 2) + 3 * (i / CS1), half = i % CS1;
         const int r = t * 128 + quad * 32 + lane;
         int s, d3, d2;
         bool valid;
@@ -763,20 +763,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
     auto p3 = [&](int x) {
       unsigned char* A = A0 + x * T::A_BYTES;
       const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
+      // tasks as in P2: tile w / 4 + 3 (i / CS2), half i % CS2
       constexpr int CPT = W2 / 16;  // chunks per task
       constexpr int NQ = TPW3 * CPT;
       uint32_t buf[2][16];
       auto load = [&](int q) {
-        const int task = warp + (q / CPT) * NW;
-        if (task < NT3) {
-          const int t = task / (4 * CS2), half = (task >> 2) % CS2;
-          tmem_ld16(tb + (uint32_t)(t * T::N2 + W2 * half + 16 * (q % CPT)), buf[q & 1]);
-        }
+        const int i = q / CPT, t = (warp >> 2) + 3 * (i / CS2), half = i % CS2;
+        tmem_ld16(tb + (uint32_t)(t * T::N2 + W2 * half + 16 * (q % CPT)), buf[q & 1]);
       };
       auto store = [&](int q) {
-        const int task = warp + (q / CPT) * NW;
-        if (task >= NT3) return;
-        const int t = task / (4 * CS2), half = (task >> 2) % CS2;
+        const int i = q / CPT, t = (warp >> 2) + 3 * (i / CS2), half = i % CS2;
         const int r = t * 128 + quad * 32 + lane;
         const int s = r / T::ROWS2, qq = r - s * T::ROWS2;
         const int t1 = T::S2O ? (qq & 127) >> 2 : qq / R3;
