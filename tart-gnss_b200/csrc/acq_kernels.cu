@@ -258,6 +258,8 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
           p.Dout[(size_t)seq_of(s) * LC + G::offset(a, b, c)] = make_float2(v.x, -v.y);
         } else {
           const float pw = fmaf(v.x, v.x, v.y * v.y);
+          if (MODE == REFINE && p.rowbuf)
+            p.rowbuf[((size_t)w * S + seq_of(s)) * LC + G::row_pos(a, b, c)] = pw;
           if (ARGMAX) {
             const int code = ((seq_of(s) * 31 + a) * 33 + b) * 16 + c;
             if (pw == pmax) {
@@ -499,16 +501,73 @@ cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, cons
 }
 
 cudaError_t launch_refine(const PolyClass& pc, const SearchDims& dims, const float2* d_Z, const float2* d_D,
-                          BestRow* d_best, int num_sms, cudaStream_t st) {
+                          BestRow* d_best, float* d_rowbuf, int num_sms, cudaStream_t st) {
   PfaParams p = {};
   p.z = const_cast<float2*>(d_Z);
   p.D = d_D;
   p.best = d_best;
+  p.rowbuf = d_rowbuf;
   p.n_prn = dims.n_prn;
   p.S = pc.S;
   p.P = pc.P;
   p.n_items = dims.n_ant * dims.n_prn;
   return dispatch_pfa<REFINE>(pc.M, p, p.n_items, num_sms, st);
+}
+
+// Second peak from the rows REFINE left in rowbuf (correlate.rs:157-175, the
+// rule of pfa_kernel mode SECOND): the 2 cw + 1 lags within cw of the peak
+// lag are overwritten with -1, then the row maximum, at least 0.  The lags
+// near the peak are located through their CRT digits (a, b, c) =
+// (t mod 31, t mod 33, t mod M) of t = lag / S in residue lag mod S.
+template <int M>
+__global__ void __launch_bounds__(256) second_scan_kernel(float* __restrict__ rowbuf, BestRow* __restrict__ best,
+                                                          int n_items, int S, int P, int cw) {
+  using G = Geo<M>;
+  __shared__ unsigned s_max;
+  for (int w = blockIdx.x; w < n_items; w += gridDim.x) {
+    float* row = rowbuf + (size_t)w * P;
+    if (threadIdx.x == 0) s_max = 0u;
+    const int tau = best[w].tau;
+    for (int d = (int)threadIdx.x - cw; d <= cw; d += blockDim.x) {
+      int lag = (tau + d) % P;
+      if (lag < 0) lag += P;
+      const int rho = lag % S, t = lag / S;
+      row[(size_t)rho * G::LC + G::row_pos(t % 31, t % 33, M == 1 ? 0 : t % M)] = -1.f;
+    }
+    __syncthreads();
+    float m = 0.f;
+    if ((P & 3) == 0) {
+      const float4* r4 = reinterpret_cast<const float4*>(row);
+      for (int i = threadIdx.x; i < P / 4; i += blockDim.x) {
+        const float4 v = __ldcs(r4 + i);
+        m = fmaxf(m, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+      }
+    } else {
+      for (int i = threadIdx.x; i < P; i += blockDim.x) m = fmaxf(m, __ldcs(row + i));
+    }
+    // non-negative floats order like their bit patterns
+    const unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(m));
+    if ((threadIdx.x & 31) == 0) atomicMax(&s_max, bits);
+    __syncthreads();
+    if (threadIdx.x == 0) best[w].p2 = __uint_as_float(s_max);
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_second_scan(const PolyClass& pc, const SearchDims& dims, float* d_rowbuf, BestRow* d_best,
+                               int chip_width, int num_sms, cudaStream_t st) {
+  const int n_items = dims.n_ant * dims.n_prn;
+  if (n_items == 0) return cudaSuccess;
+  if (2 * chip_width + 1 >= pc.P) return cudaErrorInvalidValue;
+  int grid = num_sms * 8;
+  if (grid > n_items) grid = n_items;
+  switch (pc.M) {
+    case 1: second_scan_kernel<1><<<grid, 256, 0, st>>>(d_rowbuf, d_best, n_items, pc.S, pc.P, chip_width); break;
+    case 4: second_scan_kernel<4><<<grid, 256, 0, st>>>(d_rowbuf, d_best, n_items, pc.S, pc.P, chip_width); break;
+    case 10: second_scan_kernel<10><<<grid, 256, 0, st>>>(d_rowbuf, d_best, n_items, pc.S, pc.P, chip_width); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return TGA_LAUNCHED();
 }
 
 // ---------------------------------------------------------------------------

@@ -84,8 +84,13 @@ cudaError_t launch_correlate(const PolyClass& pc, const SearchDims& dims, const 
                              const float2* d_D, unsigned long long* d_keys, int num_sms,
                              cudaStream_t st);
 // FP32 re-evaluation of each (antenna, PRN)'s selected row: rewrites best.p / best.tau.
+// With d_rowbuf (n_ant * n_prn * P floats) it also leaves each row's |y|^2 there.
 cudaError_t launch_refine(const PolyClass& pc, const SearchDims& dims, const float2* d_Z, const float2* d_D,
-                          BestRow* d_best, int num_sms, cudaStream_t st);
+                          BestRow* d_best, float* d_rowbuf, int num_sms, cudaStream_t st);
+// Second peak (best.p2) from the rows launch_refine left in d_rowbuf; the
+// result equals launch_second_peak's.
+cudaError_t launch_second_scan(const PolyClass& pc, const SearchDims& dims, float* d_rowbuf, BestRow* d_best,
+                               int chip_width, int num_sms, cudaStream_t st);
 // Tensor-core search: FP16 operands in the (31, R2, R3) frequency layout
 // (launch_tc_pack of Z and of the code spectra), then the three-stage tcgen05
 // correlator (FP32 accumulation in TMEM).  Keys hold |y|^2 scaled by 2^-2k

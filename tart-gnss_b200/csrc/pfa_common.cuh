@@ -31,6 +31,10 @@ struct Geo {
   }
   // digit-layout offset of (a, b, c): [a][c][b]
   __device__ static __forceinline__ int offset(int a, int b, int c) { return a * COLS + c * 33 + b; }
+  // position of output (a, b, c) in a row buffer of REFINE: the order in
+  // which consecutive threads emit it ([b][a] for M = 1, whose last stage
+  // runs per a; [a][c][b] otherwise)
+  __device__ static __forceinline__ int row_pos(int a, int b, int c) { return M == 1 ? b * 31 + a : offset(a, b, c); }
 };
 
 // REFINE re-evaluates the selected row of each (antenna, PRN) in FP32 and
@@ -47,6 +51,7 @@ struct PfaParams {
   int n_prn, S, P, chip_width;
   unsigned long long* keys;   // CORR output, one per row
   BestRow* best;              // SECOND in/out
+  float* rowbuf;              // REFINE (optional): |y|^2 of each item's row, [item][rho][row_pos]
 };
 
 }  // namespace tga

@@ -438,6 +438,7 @@ struct GroupBufs {
   void* z16 = nullptr;
   void* d16 = nullptr;
   void* bmat = nullptr;
+  float* rows = nullptr;  // tensor-core mode: |y|^2 of each (antenna, PRN)'s selected row
 };
 
 GroupBufs prepare_group(tga_ctx* ctx, const ClassGroup& grp, int n_ant, int nb, const std::string& tag) {
@@ -473,6 +474,7 @@ GroupBufs prepare_group(tga_ctx* ctx, const ClassGroup& grp, int n_ant, int nb, 
     const long long n_zseq = (long long)n_ab * 2 * pc.S;
     b.z16 = ctx->buf(tag + ".z16", tc_operand_bytes(pc, n_zseq, false));
     b.d16 = ctx->buf(tag + ".d16", tc_operand_bytes(pc, (long long)n_prn * 2, true));
+    b.rows = (float*)ctx->buf(tag + ".rows", (size_t)n_ant * n_prn * pc.P * sizeof(float));
     // DFT matrices of the class (they depend on Lc only), uploaded once per context
     const std::string mat_name = "tcmat." + std::to_string(pc.M);
     if (!ctx->uploaded.count(mat_name)) {
@@ -533,11 +535,17 @@ void enqueue_group(tga_ctx* ctx, const ClassGroup& grp, const GroupBufs& b, cons
           [&] { return launch_correlate(pc, dims, b.z, b.D, b.keys, ctx->num_sms, st); });
   }
   timed(ctx, ("reduce_bins" + cls).c_str(), 0.0, [&] { return launch_reduce_bins(dims, b.keys, b.best, st); });
-  if (ctx->precision == TGA_PRECISION_FP16_TC)
+  if (ctx->precision == TGA_PRECISION_FP16_TC) {
+    // the FP32 re-evaluation keeps the selected rows, and the second peak is
+    // read from them instead of transforming the rows again
     timed(ctx, ("refine" + cls).c_str(), (double)n_ant * n_prn * pc.P * (tf + 9.0),
-          [&] { return launch_refine(pc, dims, b.z, b.D, b.best, ctx->num_sms, st); });
-  timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * pc.P * (tf + 9.0),
-        [&] { return launch_second_peak(pc, dims, b.z, b.D, b.best, chip_width, ctx->num_sms, st); });
+          [&] { return launch_refine(pc, dims, b.z, b.D, b.best, b.rows, ctx->num_sms, st); });
+    timed(ctx, ("second_scan" + cls).c_str(), 0.0,
+          [&] { return launch_second_scan(pc, dims, b.rows, b.best, chip_width, ctx->num_sms, st); });
+  } else {
+    timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * pc.P * (tf + 9.0),
+          [&] { return launch_second_peak(pc, dims, b.z, b.D, b.best, chip_width, ctx->num_sms, st); });
+  }
   timed(ctx, ("finalize" + cls).c_str(), 0.0,
         [&] { return launch_finalize(pc, dims, b.best, center, b.tables, want_cn0, b.cells, st); });
   CK(cudaMemcpyAsync(host_out, b.cells, (size_t)n_ant * n_prn * sizeof(CellOut), cudaMemcpyDeviceToHost, st));
