@@ -23,7 +23,10 @@
 //
 // Generic path (any N): the reference algorithm on the GPU, with Bluestein
 // FFTs of length N built on a power-of-two Stockham FFT.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
+
+#include <vector>
 
 #include <cstdint>
 #include <cstdio>
@@ -254,6 +257,9 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
       auto epilogue = [&](int s, int a, int b, int c, float2 v) {
         if (MODE == FWD_Z) {
           p.z[(size_t)seq_of(s) * LC + G::offset(a, b, c)] = v;
+          // the last stage reads and writes the same positions of its
+          // thread: keep the output for the FP16 units below
+          if (p.z16) buf[s * LC + G::offset(a, b, c)] = v;
         } else if (MODE == FWD_D) {
           p.Dout[(size_t)seq_of(s) * LC + G::offset(a, b, c)] = make_float2(v.x, -v.y);
         } else {
@@ -349,6 +355,33 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
         }
       }
       __syncthreads();
+      // tensor-core operands: FP16 units straight from the transformed
+      // sequences in shared memory (the work of tc_pack_kernel, without
+      // reading the FP32 spectra back from memory)
+      if (MODE == FWD_Z && p.z16) {
+        using U = TcUnits<M>;
+        for (int e = tid; e < BC * U::PER_SEQ; e += NT) {
+          const int s = e / U::PER_SEQ, r = e - s * U::PER_SEQ;
+          const int q = seq_of(s);
+          if (q < 0) continue;
+          const uint2 m = __ldg(p.z16_map + r);
+          const unsigned off[4] = {m.x & 0xffffu, m.x >> 16, m.y & 0xffffu, m.y >> 16};
+          uint32_t h[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            float2 v = make_float2(0.f, 0.f);
+            if (off[i] != 0xffffu) {
+              v = buf[s * LC + (int)off[i]];
+              v.x *= p.z16_scale;
+              v.y *= p.z16_scale;
+            }
+            const __half2 hv = __floats2half2_rn(v.x, v.y);
+            h[i] = *reinterpret_cast<const uint32_t*>(&hv);
+          }
+          p.z16[(size_t)q * U::PER_SEQ + r] = make_uint4(h[0], h[1], h[2], h[3]);
+        }
+        __syncthreads();
+      }
     }
 
     if (ARGMAX) {
@@ -444,6 +477,40 @@ static cudaError_t dispatch_pfa(int M, const PfaParams& p, int n_work_slots, int
 cudaError_t launch_forward_z(const PolyClass& pc, int n_ab, float2* d_z, int num_sms, cudaStream_t st) {
   PfaParams p = {};
   p.z = d_z;
+  p.n_seq = n_ab * 2 * pc.S;
+  p.S = pc.S;
+  p.P = pc.P;
+  return dispatch_pfa<FWD_Z>(pc.M, p, p.n_seq, num_sms, st);
+}
+
+std::vector<uint16_t> tc_unit_map(int M) {
+  auto build = [](auto u) {
+    using U = decltype(u);
+    std::vector<uint16_t> t((size_t)U::PER_SEQ * 4);
+    for (int r = 0; r < U::PER_SEQ; ++r) {
+      const int j = r / U::ROWS1, row = r - j * U::ROWS1, kp = U::row_part(row);
+      for (int i = 0; i < 4; ++i) {
+        const int d1 = 4 * j + i;
+        t[(size_t)r * 4 + i] = d1 < 31 ? (uint16_t)U::src_offset(d1, kp) : (uint16_t)0xffffu;
+      }
+    }
+    return t;
+  };
+  switch (M) {
+    case 1: return build(TcUnits<1>());
+    case 4: return build(TcUnits<4>());
+    case 10: return build(TcUnits<10>());
+  }
+  return {};
+}
+
+cudaError_t launch_forward_z_tc(const PolyClass& pc, int n_ab, float2* d_z, void* d_z16, const void* d_map,
+                                float z16_scale, int num_sms, cudaStream_t st) {
+  PfaParams p = {};
+  p.z = d_z;
+  p.z16 = static_cast<uint4*>(d_z16);
+  p.z16_map = static_cast<const uint2*>(d_map);
+  p.z16_scale = z16_scale;
   p.n_seq = n_ab * 2 * pc.S;
   p.S = pc.S;
   p.P = pc.P;

@@ -236,6 +236,7 @@ struct T3 {
   static constexpr int LC = 1023 * M, OCOLS = 33 * M;
   static constexpr int NST = Tc3Cfg<M>::NST;
   static_assert(31 * R2 * R3 == LC, "factorisation");
+  static_assert(TcUnits<M>::R2 == R2 && TcUnits<M>::R3 == R3, "FP16 operand units of the forward transform");
   static_assert(NST == 2 ? R3 == 1 : R3 == 11, "the epilogue reads 22 TMEM columns per stage-3 transform");
   // With R2 even the stage-3 transforms (t1, 2j) and (t1, 2j + 1) share one
   // operand row: K entries [0, 2 R3) and [P3OFF, P3OFF + 2 R3), against a
@@ -1120,6 +1121,12 @@ std::vector<unsigned char> tc_dft_matrices(int M) {
     case 10: return build_matrices<10>();
   }
   return {};
+}
+
+float tc_z_scale(const PolyClass& pc) {
+  int kz = 0, kd = 0;
+  tc_scales(pc, &kz, &kd);
+  return (float)(1.0 / (double)(1ull << kz));
 }
 
 cudaError_t launch_tc_pack(const PolyClass& pc, const float2* d_src, long long n_seq, bool code, void* d_dst,

@@ -76,6 +76,15 @@ cudaError_t launch_antenna_means(const uint8_t* d_bits, int n_rows, size_t row_b
 cudaError_t launch_frontend(const SampleSource& src, const SearchDims& dims, const PolyClass& pc,
                             float2* d_z, cudaStream_t st);
 cudaError_t launch_forward_z(const PolyClass& pc, int n_ab, float2* d_z, int num_sms, cudaStream_t st);
+// launch_forward_z that also writes the tensor-core FP16 operands of Z
+// (launch_tc_pack's layout and scale, tc_z_scale) from shared memory
+cudaError_t launch_forward_z_tc(const PolyClass& pc, int n_ab, float2* d_z, void* d_z16, const void* d_map,
+                                float z16_scale, int num_sms, cudaStream_t st);
+// d_map of launch_forward_z_tc for chip count 1023 M: per FP16 unit four
+// 16-bit offsets into the transformed sequence (0xffff: zero), host-built
+std::vector<uint16_t> tc_unit_map(int M);
+// FP16 scale of Z in the tensor-core operands
+float tc_z_scale(const PolyClass& pc);
 // forward transform of n_seq Lc-point sequences in place (any count)
 cudaError_t launch_forward_seqs(const PolyClass& pc, long long n_seq, float2* d_z, int num_sms, cudaStream_t st);
 cudaError_t launch_code_spectra(const PolyClass& pc, const int8_t* d_chips, int n_prn, float2* d_D,

@@ -37,6 +37,36 @@ struct Geo {
   __device__ static __forceinline__ int row_pos(int a, int b, int c) { return M == 1 ? b * 31 + a : offset(a, b, c); }
 };
 
+// FP16 operands of the tensor-core search in its (31, R2, R3) frequency
+// layout (Lc = 31 R2 R3; (R2, R3) = (33, 1), (12, 11), (30, 11) for M = 1,
+// 4, 10).  Unit (seq, j, u), u = d3 R2 + d2, holds the spectrum at digits
+// (d1, d2, d3), d1 = 4j .. 4j + 3 (zero for d1 >= 31), as 4 half2 (16
+// bytes).  A frequency digit d of radix R stands for the natural
+// frequencies k = d (LC / R) (mod R); src_offset is where the FP32 engine's
+// digit layout [a][c][b] of the (31, 33, M) map holds the same frequency.
+template <int M>
+struct TcUnits {
+  static constexpr int R2 = M == 1 ? 33 : M == 4 ? 12 : 30, R3 = M == 1 ? 1 : 11;
+  static constexpr int LC = 1023 * M, ROWS1 = R2 * R3, PER_SEQ = 8 * ROWS1;
+  static constexpr int E1 = (LC / 31) * modinv_c((LC / 31) % 31, 31);
+  static constexpr int E2 = (LC / R2) * modinv_c((LC / R2) % R2, R2);
+  static constexpr int E3 = (LC / R3) * modinv_c((LC / R3) % R3, R3);
+  static constexpr int UB = modinv_c((LC / 33) % 33, 33);
+  static constexpr int UC = M == 1 ? 0 : modinv_c((LC / M) % M, M);
+  __host__ __device__ static constexpr int freq_part(int d, int R, int E) { return ((d * (LC / R)) % R) * E; }
+  // frequency contribution of the (d2, d3) digits of stage-1 row u
+  __host__ __device__ static __forceinline__ int row_part(int u) {
+    const int d3 = u / R2, d2 = u - d3 * R2;
+    return freq_part(d2, R2, E2) + freq_part(d3, R3, E3);
+  }
+  // digit-layout offset [a][c][b] of slot d1 (< 31) of a row with row_part kp
+  __host__ __device__ static __forceinline__ int src_offset(int d1, int kp) {
+    const int k = (freq_part(d1, 31, E1) + kp) % LC;
+    const int kb = (UB * k) % 33, kc = M == 1 ? 0 : (UC * k) % M;
+    return d1 * 33 * M + kc * 33 + kb;
+  }
+};
+
 // REFINE re-evaluates the selected row of each (antenna, PRN) in FP32 and
 // rewrites its peak value and lag (used after a reduced-precision search).
 enum PfaMode { FWD_Z = 0, FWD_D = 1, CORR = 2, SECOND = 3, REFINE = 4 };
@@ -52,6 +82,9 @@ struct PfaParams {
   unsigned long long* keys;   // CORR output, one per row
   BestRow* best;              // SECOND in/out
   float* rowbuf;              // REFINE (optional): |y|^2 of each item's row, [item][rho][row_pos]
+  uint4* z16;                 // FWD_Z (optional): the transformed sequences also as TcUnits, x z16_scale
+  const uint2* z16_map;       // per unit: the 4 src_offset values as 16-bit fields (0xffff: zero)
+  float z16_scale;
 };
 
 }  // namespace tga

@@ -438,6 +438,7 @@ struct GroupBufs {
   void* z16 = nullptr;
   void* d16 = nullptr;
   void* bmat = nullptr;
+  void* zmap = nullptr;   // tensor-core mode: FP16 unit offsets (tc_unit_map)
   float* rows = nullptr;  // tensor-core mode: |y|^2 of each (antenna, PRN)'s selected row
 };
 
@@ -485,6 +486,15 @@ GroupBufs prepare_group(tga_ctx* ctx, const ClassGroup& grp, int n_ant, int nb, 
     } else {
       b.bmat = ctx->buf(mat_name, 0);
     }
+    const std::string map_name = "tcmap." + std::to_string(pc.M);
+    if (!ctx->uploaded.count(map_name)) {
+      const std::vector<uint16_t> map = tc_unit_map(pc.M);
+      b.zmap = ctx->buf(map_name, map.size() * sizeof(uint16_t));
+      CK(cudaMemcpy(b.zmap, map.data(), map.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+      ctx->uploaded[map_name] = {};
+    } else {
+      b.zmap = ctx->buf(map_name, 0);
+    }
   }
   return b;
 }
@@ -512,15 +522,14 @@ void enqueue_group(tga_ctx* ctx, const ClassGroup& grp, const GroupBufs& b, cons
         [&] { return launch_code_spectra(pc, b.chips, n_prn, b.D, ctx->num_sms, st); });
   timed(ctx, ("frontend" + cls).c_str(), (double)n_ab * 2 * pc.P * pc.S * 4.0,
         [&] { return launch_frontend(src, dims, pc, b.z, st); });
-  timed(ctx, ("forward_z" + cls).c_str(), (double)n_ab * 2 * pc.P * tf,
-        [&] { return launch_forward_z(pc, n_ab, b.z, ctx->num_sms, st); });
   if (ctx->precision == TGA_PRECISION_FP16_TC) {
-    const long long n_zseq = (long long)n_ab * 2 * pc.S;
-    timed(ctx, ("tc_pack" + cls).c_str(), 0.0, [&] {
-      cudaError_t e = launch_tc_pack(pc, b.z, n_zseq, false, b.z16, ctx->num_sms, st);
-      if (e == cudaSuccess) e = launch_tc_pack(pc, b.D, (long long)n_prn * 2, true, b.d16, ctx->num_sms, st);
-      return e;
+    // the forward transform also writes Z's FP16 operands; the code spectra
+    // are packed apart
+    timed(ctx, ("forward_z" + cls).c_str(), (double)n_ab * 2 * pc.P * tf, [&] {
+      return launch_forward_z_tc(pc, n_ab, b.z, b.z16, b.zmap, tc_z_scale(pc), ctx->num_sms, st);
     });
+    timed(ctx, ("tc_pack" + cls).c_str(), 0.0,
+          [&] { return launch_tc_pack(pc, b.D, (long long)n_prn * 2, true, b.d16, ctx->num_sms, st); });
     CK(cudaMemsetAsync(b.err, 0, sizeof(int), st));
     CK(cudaMemsetAsync(b.keys, 0, (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long), st));
     // tensor-core FLOPs of the three DFT stages as dense real GEMMs
@@ -531,6 +540,8 @@ void enqueue_group(tga_ctx* ctx, const ClassGroup& grp, const GroupBufs& b, cons
           });
     ctx->tc_err_pending = b.err;
   } else {
+    timed(ctx, ("forward_z" + cls).c_str(), (double)n_ab * 2 * pc.P * tf,
+          [&] { return launch_forward_z(pc, n_ab, b.z, ctx->num_sms, st); });
     timed(ctx, ("correlate" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * (tf + 9.0),
           [&] { return launch_correlate(pc, dims, b.z, b.D, b.keys, ctx->num_sms, st); });
   }
