@@ -180,9 +180,9 @@ constexpr int cmax3(int a, int b, int c) { return a > b ? (a > c ? a : c) : (b >
 
 constexpr int kSimtWarps = 12;  // a multiple of the 4 TMEM lane quadrants
 constexpr int kSimtThreads = 32 * kSimtWarps;
-// and the warp that issues the tensor-core work, and the warp that fetches
-// the code blocks
-constexpr int kTcThreads = kSimtThreads + 64;
+// and the two warps that issue the tensor-core work (one per chain), and
+// the warp that fetches the code blocks
+constexpr int kTcThreads = kSimtThreads + 96;
 constexpr int kTcTmemCols = 512;
 constexpr long long kWaitPolls = 1LL << 22;
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per wait on the tensor cores
@@ -574,15 +574,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   // PRN of chain x in round r
   auto prn_of = [&](int r, int x) -> int { return 2 * r + x < p.n_prn ? 2 * r + x : p.n_prn - 1; };
 
-  if (warp == NW) {
-    // ---------------- MMA warp: one thread issues the tensor-core work ----------------
+  if (warp == NW || warp == NW + 1) {
+    // ---------------- MMA warps: one thread each issues one chain's tensor-core work ----------------
+    // A thread's barrier test queues behind its own MMAs still waiting for
+    // the tensor cores, so with one issuing thread the tensor cores idled
+    // between stages; with one per chain (on different SM sub-partitions)
+    // the other chain's stage is issued meanwhile.
+    const int x = warp - NW;
     if (lane == 0) {
       const uint32_t a_addr = smem_addr(A0);
       const uint64_t db1 = Lay<T::KB1>::desc(smem_addr(B1));
       const uint64_t db2 = Lay<T::KB2>::desc(smem_addr(B2));
       const uint64_t db3 = Lay<T::KB3>::desc(smem_addr(B3));
-      uint32_t ph_ready[2] = {0u, 0u};
-      int commits[2] = {0, 0};
+      uint32_t ph_ready = 0u;
+      int commits = 0;
       bool ok = true;
       for (int w = blockIdx.x; w < p.n_items && ok; w += gridDim.x) {
         for (int r = 0; r < n_rounds && ok; ++r) {
@@ -590,13 +595,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
          for (int b = 0; b < B && ok; ++b) {
 #pragma unroll 1
           for (int st = 0; st < T::NST && ok; ++st) {
-#pragma unroll 1
-            for (int x = 0; x < 2; ++x) {
-              if (!bounded_wait(&s_ready[x], ph_ready[x])) {
+            {
+              if (!bounded_wait(&s_ready[x], ph_ready)) {
                 ok = false;
                 break;
               }
-              ph_ready[x] ^= 1u;
+              ph_ready ^= 1u;
               tc_fence_after();
               const uint32_t tm = tmem_base + (uint32_t)(x * (kTcTmemCols / 2));
               const uint32_t ax = a_addr + (uint32_t)(x * T::A_BYTES);
@@ -634,21 +638,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
                               db3 + 2 * ks, idesc_f16(T::N3), ks > 0 ? 1u : 0u);
                 }
                 mma_commit(&s_done[x]);
-                ++commits[x];
+                ++commits;
               }
             }
           }
          }
         }
       }
-      // drain: the last commit of each chain (after a timeout it may still
-      // be in flight)
-      for (int x = 0; x < 2; ++x)
-        if (commits[x] > 0) bounded_wait(&s_done[x], (uint32_t)((commits[x] - 1) & 1));
+      // drain: the chain's last commit (after a timeout it may still be in
+      // flight)
+      if (commits > 0) bounded_wait(&s_done[x], (uint32_t)((commits - 1) & 1));
       if (!ok) atomicExch(p.err, 1);
     }
     __syncwarp();
-  } else if (warp == NW + 1) {
+  } else if (warp == NW + 2) {
     // ---------------- code warp: one thread fetches the code blocks ----------------
     if (lane == 0) code_warp<T, NCB>(p, s_p1, s_code, CODE0, n_rounds);
     __syncwarp();
