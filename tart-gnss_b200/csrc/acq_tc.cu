@@ -957,9 +957,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       load_z(0);
       // chain x: wait for its code block when a new PRN starts (the blocks of
       // one PRN share it), form the products, hand over
-      auto products = [&](int x, bool new_code) -> bool {
+      // code_ready: this lane's earlier test of the block (issued before the
+      // epilogue, so its latency overlaps that work); the warp waits only if
+      // a lane saw it incomplete
+      auto products = [&](int x, bool new_code, uint32_t code_ready = 0u) -> bool {
         if (new_code) {
-          if (!warp_wait(&s_code[x], ph_code[x])) return false;
+          if (!__all_sync(0xffffffffu, code_ready) && !warp_wait(&s_code[x], ph_code[x])) return false;
           ph_code[x] ^= 1u;
         }
         p1(zr, A0 + x * T::A_BYTES, CODE0 + x * T::CODE_REGION);
@@ -1009,6 +1012,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
           }
           ph_done[x] ^= 1u;
           tc_fence_after();
+          // test the chain's next code block now, use the answer after P4
+          const uint32_t code_ready = (more && b + 1 == B) ? mbar_try_wait(&s_code[x], ph_code[x]) : 0u;
           // non-negative floats order like their bit patterns
           float pmax;
           if constexpr (NCB)
@@ -1021,7 +1026,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
           // the next products are those of block b + 1, or of the next
           // round's block 0
           if (more) {
-            failed = !products(x, b + 1 == B);
+            failed = !products(x, b + 1 == B, code_ready);
             if (!failed && (NCB ? (b + 1 < B ? b + 1 : 0) == B - 1 : true)) released(x);
           }
         }
