@@ -517,6 +517,20 @@ cudaError_t launch_forward_z_tc(const PolyClass& pc, int n_ab, float2* d_z, void
   return dispatch_pfa<FWD_Z>(pc.M, p, p.n_seq, num_sms, st);
 }
 
+cudaError_t launch_forward_seqs_tc(const PolyClass& pc, long long n_seq, float2* d_z, void* d_z16, const void* d_map,
+                                   float z16_scale, int num_sms, cudaStream_t st) {
+  if (n_seq > 0x7fffffffLL) return cudaErrorInvalidValue;
+  PfaParams p = {};
+  p.z = d_z;
+  p.z16 = static_cast<uint4*>(d_z16);
+  p.z16_map = static_cast<const uint2*>(d_map);
+  p.z16_scale = z16_scale;
+  p.n_seq = (int)n_seq;
+  p.S = pc.S;
+  p.P = pc.P;
+  return dispatch_pfa<FWD_Z>(pc.M, p, p.n_seq, num_sms, st);
+}
+
 cudaError_t launch_forward_seqs(const PolyClass& pc, long long n_seq, float2* d_z, int num_sms, cudaStream_t st) {
   if (n_seq > 0x7fffffffLL) return cudaErrorInvalidValue;
   PfaParams p = {};

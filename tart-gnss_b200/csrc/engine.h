@@ -83,6 +83,9 @@ cudaError_t launch_forward_z_tc(const PolyClass& pc, int n_ab, float2* d_z, void
 // d_map of launch_forward_z_tc for chip count 1023 M: per FP16 unit four
 // 16-bit offsets into the transformed sequence (0xffff: zero), host-built
 std::vector<uint16_t> tc_unit_map(int M);
+// launch_forward_seqs that also writes the tensor-core FP16 operands
+cudaError_t launch_forward_seqs_tc(const PolyClass& pc, long long n_seq, float2* d_z, void* d_z16, const void* d_map,
+                                   float z16_scale, int num_sms, cudaStream_t st);
 // FP16 scale of Z in the tensor-core operands
 float tc_z_scale(const PolyClass& pc);
 // forward transform of n_seq Lc-point sequences in place (any count)

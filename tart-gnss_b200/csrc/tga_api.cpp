@@ -422,6 +422,17 @@ struct SearchOut {
   std::vector<CellOut> cells;  // [n_ant][n_prn] of the group
 };
 
+// The offset table of the FP16 Z units (tc_unit_map), uploaded once per context.
+void* tc_unit_map_buf(tga_ctx* ctx, int M) {
+  const std::string map_name = "tcmap." + std::to_string(M);
+  if (ctx->uploaded.count(map_name)) return ctx->buf(map_name, 0);
+  const std::vector<uint16_t> map = tc_unit_map(M);
+  void* d = ctx->buf(map_name, map.size() * sizeof(uint16_t));
+  CK(cudaMemcpy(d, map.data(), map.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+  ctx->uploaded[map_name] = {};
+  return d;
+}
+
 // Device buffers of one class group, allocated (and the code chips and DFT
 // matrices uploaded) by prepare_group before anything is launched, so that
 // enqueue_group is launches and stream-ordered copies only and can be
@@ -486,15 +497,7 @@ GroupBufs prepare_group(tga_ctx* ctx, const ClassGroup& grp, int n_ant, int nb, 
     } else {
       b.bmat = ctx->buf(mat_name, 0);
     }
-    const std::string map_name = "tcmap." + std::to_string(pc.M);
-    if (!ctx->uploaded.count(map_name)) {
-      const std::vector<uint16_t> map = tc_unit_map(pc.M);
-      b.zmap = ctx->buf(map_name, map.size() * sizeof(uint16_t));
-      CK(cudaMemcpy(b.zmap, map.data(), map.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
-      ctx->uploaded[map_name] = {};
-    } else {
-      b.zmap = ctx->buf(map_name, 0);
-    }
+    b.zmap = tc_unit_map_buf(ctx, pc.M);
   }
   return b;
 }
@@ -1785,14 +1788,18 @@ int tga_search_noncoherent(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant_tot
           [&] { return launch_code_spectra(pc, d_chips, n_prn, d_D, ctx->num_sms, st); });
     timed(ctx, "nc_frontend", 0.0,
           [&] { return launch_nc_frontend(src, dims, pc, opt->coherent_periods, B, opt->start, d_z, st); });
-    timed(ctx, "nc_forward_z", (double)n_seq * pc.Lc * tf,
-          [&] { return launch_forward_seqs(pc, n_seq, d_z, ctx->num_sms, st); });
     // the tensor-core path covers Lc = 1023 (GPS, SBAS, QZSS C/A); other code
     // lengths run the FP32 search whatever the precision
     const bool tc = ctx->precision == TGA_PRECISION_FP16_TC && pc.M == 1;
+    void* d_z16 = tc ? ctx->buf("nc.z16", tc_operand_bytes(pc, n_seq, false)) : nullptr;
+    void* d_zmap = tc ? tc_unit_map_buf(ctx, pc.M) : nullptr;
+    // in tensor-core mode the forward transform also writes Z's FP16 operands
+    timed(ctx, "nc_forward_z", (double)n_seq * pc.Lc * tf, [&] {
+      return tc ? launch_forward_seqs_tc(pc, n_seq, d_z, d_z16, d_zmap, tc_z_scale(pc), ctx->num_sms, st)
+                : launch_forward_seqs(pc, n_seq, d_z, ctx->num_sms, st);
+    });
     if (tc) {
       int* d_err = (int*)ctx->buf("tc.err", sizeof(int));
-      void* d_z16 = ctx->buf("nc.z16", tc_operand_bytes(pc, n_seq, false));
       void* d_d16 = ctx->buf("nc.d16", tc_operand_bytes(pc, (long long)n_prn * 2, true));
       const std::string mat_name = "tcmat." + std::to_string(pc.M);
       void* d_bmat = nullptr;
@@ -1804,11 +1811,8 @@ int tga_search_noncoherent(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant_tot
       } else {
         d_bmat = ctx->buf(mat_name, 0);
       }
-      timed(ctx, "nc_tc_pack", 0.0, [&] {
-        cudaError_t e = launch_tc_pack(pc, d_z, n_seq, false, d_z16, ctx->num_sms, st);
-        if (e == cudaSuccess) e = launch_tc_pack(pc, d_D, (long long)n_prn * 2, true, d_d16, ctx->num_sms, st);
-        return e;
-      });
+      timed(ctx, "nc_tc_pack", 0.0,
+            [&] { return launch_tc_pack(pc, d_D, (long long)n_prn * 2, true, d_d16, ctx->num_sms, st); });
       CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
       CK(cudaMemsetAsync(d_keys, 0, (size_t)n_ant * nb * n_prn * sizeof(unsigned long long), st));
       timed(ctx, "nc_correlate_tc", (double)n_ant * nb * n_prn * B * pc.P * tc_gemm_flops_per_point(pc.M), [&] {
