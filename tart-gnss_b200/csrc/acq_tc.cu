@@ -855,8 +855,41 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
           }
         }
         return best;
+      } else if constexpr (M == 4) {
+        // Lc = 4092.  The stage-3 accumulator of a tile is 48 columns: the transforms
+        // (t1, 2j) and (t1, 2j + 1) in columns [0, 22) and [24, 46), zeros
+        // (zero rows of the DFT matrix) in the rest, so the maximum may take
+        // whole 8-column chunks.  The LAST_TILES x 6 chunks of a lane
+        // quadrant are split evenly over its 3 warps: chunk q = (w / 4) CPW
+        // + i, tile q / 6, columns 8 (q % 6) .. + 8.
+        static_assert(T::N3 == 48 && NW == 12 && (T::LAST_TILES * 6) % 3 == 0, "P4 chunk map");
+        constexpr int CPW = T::LAST_TILES * 6 / 3, BATCH = CPW % 4 == 0 ? 4 : (CPW % 3 == 0 ? 3 : 2);
+        static_assert(CPW % BATCH == 0, "P4 batches");
+#pragma unroll
+        for (int i0 = 0; i0 < CPW; i0 += BATCH) {
+          uint32_t v[BATCH][8];
+#pragma unroll
+          for (int i = 0; i < BATCH; ++i) {
+            const int q = (warp >> 2) * CPW + i0 + i;
+            tmem_ld8(tb + (uint32_t)((q / 6) * T::N3 + 8 * (q % 6)), v[i]);
+          }
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < BATCH; ++i) {
+            const int q = (warp >> 2) * CPW + i0 + i;
+            const int r = (q / 6) * 128 + quad * 32 + lane;
+            if (r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S) {
+#pragma unroll
+              for (int h = 0; h < 4; ++h)
+                best = fmaxf(best, fmaf(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h]),
+                                        __uint_as_float(v[i][2 * h + 1]) * __uint_as_float(v[i][2 * h + 1])));
+            }
+          }
+        }
+        return best;
       } else {
-        // tasks in batches of LB4: all loads of a batch in flight, one wait
+        // Lc = 10230 (where the chunks above measured slower): tasks in
+        // batches of LB4, all loads of a batch in flight, one wait
 #pragma unroll
         for (int i0 = 0; i0 < TPW4; i0 += LB4) {
           uint32_t v[LB4][VW];
