@@ -646,6 +646,20 @@ def main():
             "delay_rms_samples": {"grid": rms(gt), "refined": rms(rt)},
             "doppler_rms_hz": {"grid": rms(gf), "refined": rms(rf)},
             "converged": int(sum(r["converged"] for r in res))}
+    if rank == 0:
+        # --benchmark (main.rs:482-694) through tga_benchmark: one PRN per
+        # constellation on antenna 0 of the benchmark observation, setup
+        # (host extraction of every antenna's window) and search timed apart
+        ctx.benchmark(bits_np, FS)  # warm-up
+        entries = ctx.benchmark(bits_np, FS)
+        names = {tga.GPS: "GPS", tga.GALILEO: "Galileo", tga.BEIDOU: "BeiDou", tga.SBAS: "SBAS", tga.QZSS: "QZSS",
+                 tga.L1C: "L1C"}
+        total_search = sum(e["search_s"] for e in entries)
+        line["benchmark_split"] = {
+            "per_constellation": [{"constellation": names[e["constellation"]], "prn": e["prn"],
+                                   "setup_s": e["setup_s"], "search_s": e["search_s"]} for e in entries],
+            "setup_s": sum(e["setup_s"] for e in entries), "search_s": total_search,
+            "acq_per_s": len(entries) / total_search, "arithmetic": dtype[args.precision]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, desc = cpu_sample_baseline(os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": "cells/s", "cores": os.cpu_count(), "kind": "port",
