@@ -31,8 +31,8 @@
 //
 // One CTA per SM (all 512 TMEM columns) runs two PRN chains over the Z of a
 // (row, group of BC code-phase residues) work item, so that the tensor cores
-// work on one chain while the warps transpose the other; a dedicated warp
-// issues the MMAs.  Every wait is bounded (1 s): on expiry the kernel sets
+// work on one chain while the warps transpose the other; one dedicated warp
+// per chain issues its MMAs.  Every wait is bounded (1 s): on expiry the kernel sets
 // *err, drains (again bounded), frees its TMEM and returns.
 //
 // The same kernel (NCB) runs the non-coherent search at Lc = 1023: every PRN
@@ -458,16 +458,16 @@ __device__ __forceinline__ void tmem_ld_stage3(uint32_t taddr, int half, uint32_
 // Each chain has its own code block in shared memory, fetched for its next
 // PRN with one bulk copy as soon as the chain's products are formed, by a
 // warp of its own (s_p1[x]: the 12 SIMT warps have read the block for the
-// last time), so that the MMA warp does nothing but wait, issue and commit.  Per
-// PRN pair:
+// last time), so that the MMA warps do nothing but wait, issue and commit.
+// Per PRN pair:
 //   SIMT warps:  P1(a) P1(b) P2(a) P2(b) P3(a) P3(b) P4(a) P4(b)
-//   MMA warp:          M1(a) M1(b) M2(a) M2(b) M3(a) M3(b)
+//   MMA warps:         M1(a) M1(b) M2(a) M2(b) M3(a) M3(b)
 // where Mi(x) runs while the SIMT warps work on the other chain.  Hand-offs:
 // s_ready[x] (arrivals of the 12 SIMT warps: chain x's operands are in
 // shared memory and its accumulator has been read), s_done[x]
 // (tcgen05.commit) and s_code[x] (bulk copy).  A tcgen05.mma holds its
-// thread until the tensor cores take it, so the issuing has a warp of its
-// own.  Every wait is bounded.
+// thread until the tensor cores take it, so issuing has warps of its own,
+// one per chain.  Every wait is bounded.
 //
 // NCB (non-coherent search, Lc = 1023): the row is an (antenna, bin) and
 // every PRN pair runs through B coherent blocks; each thread keeps the |y|^2
