@@ -704,10 +704,11 @@ int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, si
   if (generic_consts.empty()) {
     // the plan: everything the launches take by value or by address
     std::string key;
-    char kb[160];
-    std::snprintf(kb, sizeof kb, "%p/%zu/%zu/%a/%a/%d/%d/%d/%d/%d/%d|", (const void*)d_bits, n_ant_total, row_bytes,
-                  fs, opt->center_freq, nb, opt->cn0, ctx->precision, ctx->test_flags, pfa_variant(10),
-                  chip_width_of(fs));
+    char kb[512];
+    const int kn = std::snprintf(kb, sizeof kb, "%p/%zu/%zu/%a/%a/%d/%d/%d/%d/%d/%d|", (const void*)d_bits,
+                                 n_ant_total, row_bytes, fs, opt->center_freq, nb, opt->cn0, ctx->precision,
+                                 ctx->test_flags, pfa_variant(10), chip_width_of(fs));
+    if (kn < 0 || kn >= (int)sizeof kb) throw std::runtime_error("search plan key does not fit");
     key = kb;
     for (int32_t a : ants) key += std::to_string(a) + ",";
     key += "|";
