@@ -45,6 +45,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "engine.h"
@@ -709,8 +710,29 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       }
     };
     // P2 and P3 read the accumulators in chunks of 16 columns (8 complex
-    // outputs) through two register buffers: the load of chunk q + 1 is in
-    // flight while chunk q is rounded and stored
+    // outputs).  At Lc = 10230 every chunk of the phase is loaded before one
+    // wait (measured fastest there); otherwise through two register buffers,
+    // the load of chunk q + 1 in flight while chunk q is rounded and stored.
+    constexpr bool ONE_WAIT = M == 10;
+    auto run_chunks = [&](auto nq, auto&& load, auto&& store) {
+      constexpr int NQ = decltype(nq)::value;
+      if constexpr (ONE_WAIT) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) load(q);
+        tmem_wait_ld();
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) store(q);
+      } else {
+        load(0);
+        tmem_wait_ld();
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+          if (q + 1 < NQ) load(q + 1);
+          store(q);
+          if (q + 1 < NQ) tmem_wait_ld();
+        }
+      }
+    };
     // ---- P2: stage-1 accumulators -> stage-2 rows (t1, d3), K = d2 ----
     auto p2 = [&](int x) {
       unsigned char* A = A0 + x * T::A_BYTES;
@@ -719,10 +741,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       // column halves: task i is tile w / 4 + 3 (i / CS1), half i % CS1,
       // known at compile time but for the tile
       constexpr int NQ = TPW2 * 2;  // a task is 32 columns
-      uint32_t buf[2][16];
+      uint32_t buf[ONE_WAIT ? NQ : 2][16];
       auto load = [&](int q) {
         const int i = q >> 1, t = (warp >> 2) + 3 * (i / CS1), half = i % CS1;
-        tmem_ld16(tb + (uint32_t)(t * T::N1 + 32 * half + 16 * (q & 1)), buf[q & 1]);
+        tmem_ld16(tb + (uint32_t)(t * T::N1 + 32 * half + 16 * (q & 1)), buf[ONE_WAIT ? q : q & 1]);
       };
       auto store = [&](int q) {
         const int i = q >> 1, t = (warp >> 2) + 3 * (i / CS1), half = i % CS1;
@@ -750,18 +772,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
         for (int h = 0; h < 8; ++h) {
           const int t1 = 16 * half + 8 * (q & 1) + h;
           if (valid && t1 < 31)
-            st_shared_u32(dst + t1 * T1_STRIDE,
-                          pack_h2_sat(__uint_as_float(buf[q & 1][2 * h]), __uint_as_float(buf[q & 1][2 * h + 1])));
+            st_shared_u32(dst + t1 * T1_STRIDE, pack_h2_sat(__uint_as_float(buf[ONE_WAIT ? q : q & 1][2 * h]),
+                                                            __uint_as_float(buf[ONE_WAIT ? q : q & 1][2 * h + 1])));
         }
       };
-      load(0);
-      tmem_wait_ld();
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        if (q + 1 < NQ) load(q + 1);
-        store(q);
-        if (q + 1 < NQ) tmem_wait_ld();
-      }
+      run_chunks(std::integral_constant<int, NQ>(), load, store);
     };
     // ---- P3: stage-2 accumulators -> stage-3 rows (t1, t2), K = d3 ----
     auto p3 = [&](int x) {
@@ -770,10 +785,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       // tasks as in P2: tile w / 4 + 3 (i / CS2), half i % CS2
       constexpr int CPT = W2 / 16;  // chunks per task
       constexpr int NQ = TPW3 * CPT;
-      uint32_t buf[2][16];
+      uint32_t buf[ONE_WAIT ? NQ : 2][16];
       auto load = [&](int q) {
         const int i = q / CPT, t = (warp >> 2) + 3 * (i / CS2), half = i % CS2;
-        tmem_ld16(tb + (uint32_t)(t * T::N2 + W2 * half + 16 * (q % CPT)), buf[q & 1]);
+        tmem_ld16(tb + (uint32_t)(t * T::N2 + W2 * half + 16 * (q % CPT)), buf[ONE_WAIT ? q : q & 1]);
       };
       auto store = [&](int q) {
         const int i = q / CPT, t = (warp >> 2) + 3 * (i / CS2), half = i % CS2;
@@ -782,7 +797,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
         const int t1 = T::S2O ? (qq & 127) >> 2 : qq / R3;
         const int d3 = T::S2O ? 4 * (qq >> 7) + (qq & 3) : qq - t1 * R3;
         const bool valid = r < T::NR2 && (!T::S2O || (d3 < R3 && t1 < 31));
-        const uint32_t* v = buf[q & 1];
+        const uint32_t* v = buf[ONE_WAIT ? q : q & 1];
         if (T::PAIR3) {
           // paired stage-3 row (t1, t2 / 2) = s ROWS3P + t1 R2 / 2 + t2 / 2
           // (T1F3: s ROWS3P + (t2 / 2) 31 + t1), K entry d3 (t2 even) or
@@ -809,14 +824,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
           }
         }
       };
-      load(0);
-      tmem_wait_ld();
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        if (q + 1 < NQ) load(q + 1);
-        store(q);
-        if (q + 1 < NQ) tmem_wait_ld();
-      }
+      run_chunks(std::integral_constant<int, NQ>(), load, store);
     };
     // ---- P4: |y|^2 maximum over the stage-3 outputs of chain x ----
     // Only the row maximum is kept: the bin / hypothesis reduction compares
