@@ -298,6 +298,7 @@ def main():
     ap.add_argument("--no-weak", action="store_true",
                     help="skip the weak-signal non-coherent search (10 ms coherent x 10, 201 x 50 Hz bins)")
     ap.add_argument("--no-fine", action="store_true", help="skip the fine-acquisition measurement")
+    ap.add_argument("--no-split", action="store_true", help="skip the --benchmark-style setup/search split")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -646,7 +647,7 @@ def main():
             "delay_rms_samples": {"grid": rms(gt), "refined": rms(rt)},
             "doppler_rms_hz": {"grid": rms(gf), "refined": rms(rf)},
             "converged": int(sum(r["converged"] for r in res))}
-    if rank == 0:
+    if rank == 0 and not args.no_split:
         # --benchmark (main.rs:482-694) through tga_benchmark: one PRN per
         # constellation on antenna 0 of the benchmark observation, setup
         # (host extraction of every antenna's window) and search timed apart
