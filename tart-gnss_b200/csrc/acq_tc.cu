@@ -430,10 +430,21 @@ struct Tc3Params {
   int* err;
   int n_items;  // n_ab * groups: (row, residue group) work items
   int groups;   // ceil(S / BC)
+  // work units: item u / split, its PRN pairs [r0, r1) of part u % split
+  // (split > 1 only when the items are fewer than the SMs)
+  int split;
   int n_prn, S;
   int B;        // coherent blocks summed non-coherently (1: the drop-in search)
   int skip_commit;  // test hook: see TGA_TEST_TC_SKIP_COMMIT
 };
+
+// PRN pairs [first, end) of work unit u, of n_rounds pairs per item
+__device__ __forceinline__ int unit_round0(const Tc3Params& p, int u, int n_rounds) {
+  return (u % p.split) * n_rounds / p.split;
+}
+__device__ __forceinline__ int unit_round1(const Tc3Params& p, int u, int n_rounds) {
+  return (u % p.split + 1) * n_rounds / p.split;
+}
 
 // Reads the 22 accumulator columns of stage-3 transform `half` of this warp's
 // lane quadrant at column taddr into v[0..21] (v[22], v[23] are padding).
@@ -494,14 +505,16 @@ __device__ __noinline__ void code_warp(const Tc3Params& p, uint64_t* s_p1, uint6
     bulk_g2s(smem_addr(CODE0 + x * T::CODE_REGION), src, (uint32_t)T::CODE_BYTES, &s_code[x]);
     ++fetches[x];
   };
-  if ((int)blockIdx.x < p.n_items && n_rounds > 0) {
-    fetch(0, blockIdx.x, 0);
-    fetch(1, blockIdx.x, 0);
+  const int n_units = p.n_items * p.split;
+  if ((int)blockIdx.x < n_units && n_rounds > 0) {
+    fetch(0, blockIdx.x / p.split, unit_round0(p, blockIdx.x, n_rounds));
+    fetch(1, blockIdx.x / p.split, unit_round0(p, blockIdx.x, n_rounds));
   }
 #pragma unroll 1
-  for (int w = blockIdx.x; w < p.n_items && ok; w += gridDim.x)
+  for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
+    const int w = u / p.split, r1 = unit_round1(p, u, n_rounds), un = u + (int)gridDim.x;
 #pragma unroll 1
-    for (int r = 0; r < n_rounds && ok; ++r)
+    for (int r = unit_round0(p, u, n_rounds); r < r1 && ok; ++r)
 #pragma unroll 1
       for (int x = 0; x < 2 && ok; ++x) {
         if (!bounded_wait(&s_p1[x], ph_p1[x])) {
@@ -509,11 +522,12 @@ __device__ __noinline__ void code_warp(const Tc3Params& p, uint64_t* s_p1, uint6
           break;
         }
         ph_p1[x] ^= 1u;
-        if (r + 1 < n_rounds)
+        if (r + 1 < r1)
           fetch(x, w, r + 1);
-        else if (w + (int)gridDim.x < p.n_items)
-          fetch(x, w + gridDim.x, 0);
+        else if (un < n_units)
+          fetch(x, un / p.split, unit_round0(p, un, n_rounds));
       }
+  }
   // drain: the last bulk copy of each chain
   for (int x = 0; x < 2; ++x)
     if (fetches[x] > 0) bounded_wait(&s_code[x], (uint32_t)((fetches[x] - 1) & 1));
@@ -590,8 +604,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       uint32_t ph_ready = 0u;
       int commits = 0;
       bool ok = true;
-      for (int w = blockIdx.x; w < p.n_items && ok; w += gridDim.x) {
-        for (int r = 0; r < n_rounds && ok; ++r) {
+      for (int u = blockIdx.x; u < p.n_items * p.split && ok; u += gridDim.x) {
+        const int r1 = unit_round1(p, u, n_rounds);
+        for (int r = unit_round0(p, u, n_rounds); r < r1 && ok; ++r) {
 #pragma unroll 1
          for (int b = 0; b < B && ok; ++b) {
 #pragma unroll 1
@@ -977,8 +992,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       return best;
     };
 
-    for (int w = blockIdx.x; w < p.n_items && !failed; w += gridDim.x) {
-      const int ab_h = w / p.groups, g = w - ab_h * p.groups;
+    for (int u = blockIdx.x; u < p.n_items * p.split && !failed; u += gridDim.x) {
+      const int w = u / p.split, ab_h = w / p.groups, g = w - ab_h * p.groups;
+      const int r0 = unit_round0(p, u, n_rounds), r1 = unit_round1(p, u, n_rounds);
       // this item's Z units of block blk, in registers
       uint4 zr[U];
       auto load_z = [&](int blk) {
@@ -1019,9 +1035,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
         failed = !products(x, true);
         if (!failed && B == 1) released(x);
       }
-      for (int r = 0; r < n_rounds && !failed; ++r)
+      for (int r = r0; r < r1 && !failed; ++r)
        for (int b = 0; b < B && !failed; ++b) {
-        const bool more = b + 1 < B || r + 1 < n_rounds;  // a next block of this item follows
+        const bool more = b + 1 < B || r + 1 < r1;  // a next block of this unit follows
         // both chains have formed this block's products: bring the next
         // block's Z into the registers while the transforms run
         if (NCB && more) load_z(b + 1 < B ? b + 1 : 0);
@@ -1099,13 +1115,20 @@ cudaError_t run_tc3(const PolyClass& pc, const SearchDims& dims, int B, const vo
   p.groups = (pc.S + T::BC - 1) / T::BC;
   p.B = NCB ? B : 1;
   p.n_items = dims.n_ant * dims.nb * (NCB ? 1 : 2) * p.groups;
+  // too few items to fill the SMs: split each item's PRN pairs over CTAs
+  const int n_rounds = (dims.n_prn + 1) / 2;
+  p.split = 1;
+  if (p.n_items > 0 && p.n_items < num_sms && n_rounds > 1) {
+    p.split = (num_sms + p.n_items - 1) / p.n_items;
+    if (p.split > n_rounds) p.split = n_rounds;
+  }
   auto kern = pfa_tc3_kernel<M, NCB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, T::SMEM);
   if (e != cudaSuccess) return e;
   // one CTA per SM: T::SMEM is above half of the SM's shared memory, so the
   // 512-column TMEM allocation never meets another one
   int grid = num_sms;
-  if (grid > p.n_items) grid = p.n_items;
+  if (grid > p.n_items * p.split) grid = p.n_items * p.split;
   if (grid < 1) return cudaSuccess;
   kern<<<grid, kTcThreads, T::SMEM, st>>>(p);
   kernel_launch_add(1);
