@@ -438,12 +438,11 @@ struct Tc3Params {
   int skip_commit;  // test hook: see TGA_TEST_TC_SKIP_COMMIT
 };
 
-// PRN pairs [first, end) of work unit u, of n_rounds pairs per item
-__device__ __forceinline__ int unit_round0(const Tc3Params& p, int u, int n_rounds) {
-  return (u % p.split) * n_rounds / p.split;
-}
-__device__ __forceinline__ int unit_round1(const Tc3Params& p, int u, int n_rounds) {
-  return (u % p.split + 1) * n_rounds / p.split;
+// PRN pairs [first, end) of work unit u, of n_rounds pairs per item, with
+// `split` units per item
+__device__ __forceinline__ int unit_round0(int split, int u, int n_rounds) { return (u % split) * n_rounds / split; }
+__device__ __forceinline__ int unit_round1(int split, int u, int n_rounds) {
+  return (u % split + 1) * n_rounds / split;
 }
 
 // Reads the 22 accumulator columns of stage-3 transform `half` of this warp's
@@ -505,16 +504,17 @@ __device__ __noinline__ void code_warp(const Tc3Params& p, uint64_t* s_p1, uint6
     bulk_g2s(smem_addr(CODE0 + x * T::CODE_REGION), src, (uint32_t)T::CODE_BYTES, &s_code[x]);
     ++fetches[x];
   };
-  const int n_units = p.n_items * p.split;
+  const int split = NCB ? p.split : 1;  // the drop-in search always has enough items
+  const int n_units = p.n_items * split;
   if ((int)blockIdx.x < n_units && n_rounds > 0) {
-    fetch(0, blockIdx.x / p.split, unit_round0(p, blockIdx.x, n_rounds));
-    fetch(1, blockIdx.x / p.split, unit_round0(p, blockIdx.x, n_rounds));
+    fetch(0, blockIdx.x / split, unit_round0(split, blockIdx.x, n_rounds));
+    fetch(1, blockIdx.x / split, unit_round0(split, blockIdx.x, n_rounds));
   }
 #pragma unroll 1
   for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
-    const int w = u / p.split, r1 = unit_round1(p, u, n_rounds), un = u + (int)gridDim.x;
+    const int w = u / split, r1 = unit_round1(split, u, n_rounds), un = u + (int)gridDim.x;
 #pragma unroll 1
-    for (int r = unit_round0(p, u, n_rounds); r < r1 && ok; ++r)
+    for (int r = unit_round0(split, u, n_rounds); r < r1 && ok; ++r)
 #pragma unroll 1
       for (int x = 0; x < 2 && ok; ++x) {
         if (!bounded_wait(&s_p1[x], ph_p1[x])) {
@@ -525,7 +525,7 @@ __device__ __noinline__ void code_warp(const Tc3Params& p, uint64_t* s_p1, uint6
         if (r + 1 < r1)
           fetch(x, w, r + 1);
         else if (un < n_units)
-          fetch(x, un / p.split, unit_round0(p, un, n_rounds));
+          fetch(x, un / split, unit_round0(split, un, n_rounds));
       }
   }
   // drain: the last bulk copy of each chain
@@ -563,6 +563,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   float* ACC = reinterpret_cast<float*>(CODE0 + 2 * T::CODE_REGION);  // [2 chains][33][ACC_ROWS] (NCB)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quad = warp & 3;
   const int S = p.S, n_rounds = (p.n_prn + 1) / 2, B = NCB ? p.B : 1;
+  const int split = NCB ? p.split : 1;  // the drop-in search always has enough items
 
   if (warp == 0) {
     tmem_alloc(&s_tmem, kTcTmemCols);
@@ -604,9 +605,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       uint32_t ph_ready = 0u;
       int commits = 0;
       bool ok = true;
-      for (int u = blockIdx.x; u < p.n_items * p.split && ok; u += gridDim.x) {
-        const int r1 = unit_round1(p, u, n_rounds);
-        for (int r = unit_round0(p, u, n_rounds); r < r1 && ok; ++r) {
+      for (int u = blockIdx.x; u < p.n_items * split && ok; u += gridDim.x) {
+        const int r1 = unit_round1(split, u, n_rounds);
+        for (int r = unit_round0(split, u, n_rounds); r < r1 && ok; ++r) {
 #pragma unroll 1
          for (int b = 0; b < B && ok; ++b) {
 #pragma unroll 1
@@ -992,9 +993,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       return best;
     };
 
-    for (int u = blockIdx.x; u < p.n_items * p.split && !failed; u += gridDim.x) {
-      const int w = u / p.split, ab_h = w / p.groups, g = w - ab_h * p.groups;
-      const int r0 = unit_round0(p, u, n_rounds), r1 = unit_round1(p, u, n_rounds);
+    for (int u = blockIdx.x; u < p.n_items * split && !failed; u += gridDim.x) {
+      const int w = u / split, ab_h = w / p.groups, g = w - ab_h * p.groups;
+      const int r0 = unit_round0(split, u, n_rounds), r1 = unit_round1(split, u, n_rounds);
       // this item's Z units of block blk, in registers
       uint4 zr[U];
       auto load_z = [&](int blk) {
@@ -1115,10 +1116,11 @@ cudaError_t run_tc3(const PolyClass& pc, const SearchDims& dims, int B, const vo
   p.groups = (pc.S + T::BC - 1) / T::BC;
   p.B = NCB ? B : 1;
   p.n_items = dims.n_ant * dims.nb * (NCB ? 1 : 2) * p.groups;
-  // too few items to fill the SMs: split each item's PRN pairs over CTAs
+  // too few items to fill the SMs (the non-coherent search on a few rows):
+  // split each item's PRN pairs over CTAs
   const int n_rounds = (dims.n_prn + 1) / 2;
   p.split = 1;
-  if (p.n_items > 0 && p.n_items < num_sms && n_rounds > 1) {
+  if (NCB && p.n_items > 0 && p.n_items < num_sms && n_rounds > 1) {
     p.split = (num_sms + p.n_items - 1) / p.n_items;
     if (p.split > n_rounds) p.split = n_rounds;
   }
