@@ -111,3 +111,27 @@ def test_profiling_and_generic_plans_run_eagerly():
         for _ in range(3):
             ctx.acquire_cells(short, 16.0e6, mask=1 << tga.GPS, prn_filter=[5])
             assert ctx.last_graph() == tga.GRAPH_NONE
+
+
+def test_timeout_reported_through_captured_and_replayed_graphs():
+    """The tensor-core wait-expiry hook (no MMA issued, every wait bounded to
+    1 s, nothing faults) under graph capture and replay: each call fails with
+    TGA_ERR_TIMEOUT, and with the hook off the next plan runs normally."""
+    bits = _obs(95, n_ant=1)
+    mask = 1 << tga.GPS
+    with tga.Context(0) as ctx:
+        ctx.set_precision(tga.PRECISION_FP16_TC)
+        ctx.set_test_flags(tga.TEST_TC_SKIP_COMMIT)
+        states = []
+        for _ in range(3):
+            with pytest.raises(tga.TgaError) as ei:
+                ctx.acquire_cells(bits, FS, mask=mask, prn_filter=[5])
+            assert ei.value.code == 6  # TGA_ERR_TIMEOUT
+            states.append(ctx.last_graph())
+        assert states == [tga.GRAPH_NONE, tga.GRAPH_CAPTURED, tga.GRAPH_REPLAYED]
+        ctx.set_test_flags(0)
+        got = ctx.acquire_cells(bits, FS, mask=mask, prn_filter=[5])
+    with tga.Context(0) as ref:
+        ref.set_graphs(False)
+        ref.set_precision(tga.PRECISION_FP16_TC)
+        _same(got, ref.acquire_cells(bits, FS, mask=mask, prn_filter=[5]))
