@@ -969,25 +969,34 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
         const int r = t * 128 + quad * 32 + lane;
         const bool valid = r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S;
         float* a = acc + (size_t)(11 * c) * T::ACC_ROWS + r;
+        // all loads of the sums first, then the arithmetic, then the
+        // stores: one shared-memory latency per task instead of one per
+        // output (the compiler kept each load behind the previous store)
+        float sum[11];
 #pragma unroll
-        for (int h = 0; h < 11; ++h) {
-          // the chunk starts 22 c - s0 = 0, 6 or 4 words into v
-          float re, im;
-          if (c == 0) {
-            re = __uint_as_float(v[2 * h]);
-            im = __uint_as_float(v[2 * h + 1]);
-          } else if (c == 1) {
-            re = __uint_as_float(v[6 + 2 * h]);
-            im = __uint_as_float(v[6 + 2 * h + 1]);
-          } else {
-            re = __uint_as_float(v[4 + 2 * h]);
-            im = __uint_as_float(v[4 + 2 * h + 1]);
+        for (int h = 0; h < 11; ++h) sum[h] = b > 0 ? a[h * T::ACC_ROWS] : 0.f;
+        // the chunk starts 22 c - s0 = 0, 6 or 4 words into v (c is
+        // uniform over the warp; constant indices keep v in registers)
+        auto add = [&](auto o) {
+#pragma unroll
+          for (int h = 0; h < 11; ++h) {
+            const float re = __uint_as_float(v[decltype(o)::value + 2 * h]);
+            const float im = __uint_as_float(v[decltype(o)::value + 2 * h + 1]);
+            sum[h] = fmaf(re, re, im * im) + sum[h];
           }
-          const float pw = fmaf(re, re, im * im) + (b > 0 ? a[h * T::ACC_ROWS] : 0.f);
-          if (b + 1 < B)
-            a[h * T::ACC_ROWS] = pw;
-          else if (valid)
-            best = fmaxf(best, pw);
+        };
+        if (c == 0)
+          add(std::integral_constant<int, 0>());
+        else if (c == 1)
+          add(std::integral_constant<int, 6>());
+        else
+          add(std::integral_constant<int, 4>());
+        if (b + 1 < B) {
+#pragma unroll
+          for (int h = 0; h < 11; ++h) a[h * T::ACC_ROWS] = sum[h];
+        } else if (valid) {
+#pragma unroll
+          for (int h = 0; h < 11; ++h) best = fmaxf(best, sum[h]);
         }
       }
       return best;
