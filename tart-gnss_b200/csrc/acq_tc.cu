@@ -932,10 +932,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
             if (i0 + i < TPW4 && task < NT4) {
               const int r = (task / (4 * HALVES3)) * 128 + quad * 32 + lane;
               if (r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S) {
+                // the task's powers, then their maximum as a pairwise tree
+                // (a serial fmaxf chain left the warps waiting on latency)
+                float pw[T::LAST_OUT];
 #pragma unroll
                 for (int h = 0; h < T::LAST_OUT; ++h)
-                  best = fmaxf(best, fmaf(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h]),
-                                          __uint_as_float(v[i][2 * h + 1]) * __uint_as_float(v[i][2 * h + 1])));
+                  pw[h] = fmaf(__uint_as_float(v[i][2 * h]), __uint_as_float(v[i][2 * h]),
+                               __uint_as_float(v[i][2 * h + 1]) * __uint_as_float(v[i][2 * h + 1]));
+#pragma unroll
+                for (int w2 = 1; w2 < T::LAST_OUT; w2 *= 2)
+#pragma unroll
+                  for (int h = 0; h + w2 < T::LAST_OUT; h += 2 * w2) pw[h] = fmaxf(pw[h], pw[h + w2]);
+                best = fmaxf(best, pw[0]);
               }
             }
           }
