@@ -93,6 +93,10 @@ struct FrontParams {
   const double* fc;
   int nb, P, S, Lc;
   float pulse[kMaxPulse];
+  // pulse shape: 0 any, 1 constant w0, 2 w0 for the first S / 2 samples and
+  // -w0 for the rest (BOC(1, 1)); 1 and 2 let the polyphase sums run
+  int pulse_kind;
+  float pulse_w0;
   float2* z;
 };
 
@@ -153,6 +157,54 @@ __global__ void __launch_bounds__(256) frontend_kernel(FrontParams p) {
   }
   __syncthreads();
   const size_t seqA = ((size_t)ab * 2 + 0) * S, seqB = ((size_t)ab * 2 + 1) * S;
+  if (p.pulse_kind != 0 && S >= 4) {
+    // runs of L = S / 4 residues per thread: the first sum directly, each
+    // next one from the previous (2 or 3 samples instead of S):
+    //   constant w0:   z(rho + 1) = z(rho) + w0 (f[a + S] - f[a])
+    //   w0 / -w0:      z(rho + 1) = z(rho) + w0 (2 f[a + S/2] - f[a] - f[a + S])
+    // with a = jj S + rho; sample i sits at padded index i + i / S
+    const int L = (S + 3) / 4;
+    const float w0 = p.pulse_w0;
+    const bool boc = p.pulse_kind == 2;
+    const int H = S / 2;
+    for (int o = threadIdx.x; o < 4 * nj; o += blockDim.x) {
+      const int k = o / nj, jj = o - k * nj;
+      const int rho0 = k * L, rho1 = min(rho0 + L, S);
+      if (rho0 >= S) continue;
+      float2 za = make_float2(0.f, 0.f), zb = make_float2(0.f, 0.f);
+      const int base = jj * S + rho0 + jj;
+      for (int s = 0; s < S; ++s) {
+        const int pi = base + s + (rho0 + s >= S ? 1 : 0);
+        const float w = p.pulse[s];
+        za.x = fmaf(w, fsh[pi].x, za.x);
+        za.y = fmaf(w, fsh[pi].y, za.y);
+        zb.x = fmaf(w, gsh[pi].x, zb.x);
+        zb.y = fmaf(w, gsh[pi].y, zb.y);
+      }
+      const int j = j0 + jj;
+      p.z[(seqA + rho0) * Lc + j] = za;
+      p.z[(seqB + rho0) * Lc + j] = cmul(zb, tw[jj]);
+      for (int rho = rho0; rho + 1 < rho1; ++rho) {
+        const int a = jj * S + rho;
+        const int pa = a + jj, pe = a + S + jj + 1;
+        if (boc) {
+          const int pm = a + H + jj + (rho + H >= S ? 1 : 0);
+          za.x += w0 * (2.f * fsh[pm].x - fsh[pa].x - fsh[pe].x);
+          za.y += w0 * (2.f * fsh[pm].y - fsh[pa].y - fsh[pe].y);
+          zb.x += w0 * (2.f * gsh[pm].x - gsh[pa].x - gsh[pe].x);
+          zb.y += w0 * (2.f * gsh[pm].y - gsh[pa].y - gsh[pe].y);
+        } else {
+          za.x += w0 * (fsh[pe].x - fsh[pa].x);
+          za.y += w0 * (fsh[pe].y - fsh[pa].y);
+          zb.x += w0 * (gsh[pe].x - gsh[pa].x);
+          zb.y += w0 * (gsh[pe].y - gsh[pa].y);
+        }
+        p.z[(seqA + rho + 1) * Lc + j] = za;
+        p.z[(seqB + rho + 1) * Lc + j] = cmul(zb, tw[jj]);
+      }
+    }
+    return;
+  }
   for (int o = threadIdx.x; o < S * nj; o += blockDim.x) {
     const int rho = o / nj, jj = o - rho * nj;
     float2 za = make_float2(0.f, 0.f), zb = make_float2(0.f, 0.f);
@@ -183,6 +235,14 @@ cudaError_t launch_frontend(const SampleSource& src, const SearchDims& dims, con
   p.S = pc.S;
   p.Lc = pc.Lc;
   for (int i = 0; i < kMaxPulse; ++i) p.pulse[i] = pc.pulse[i];
+  // the pulse's shape (see FrontParams)
+  p.pulse_w0 = pc.pulse[0];
+  bool constant = true, boc = pc.S % 2 == 0;
+  for (int i = 0; i < pc.S; ++i) {
+    constant = constant && pc.pulse[i] == pc.pulse[0];
+    boc = boc && pc.pulse[i] == (i < pc.S / 2 ? pc.pulse[0] : -pc.pulse[0]);
+  }
+  p.pulse_kind = constant ? 1 : (boc ? 2 : 0);
   p.z = d_z;
   const int span = kFrontJ * pc.S + pc.S;
   const size_t smem = (size_t)(2 * (span + span / pc.S + 1) + kFrontJ) * sizeof(float2);
