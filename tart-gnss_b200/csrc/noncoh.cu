@@ -30,6 +30,10 @@ struct NcFrontParams {
   int nb, P, S, Lc, K, B;
   long long start;
   float pulse[kMaxPulse];
+  // pulse shape: 0 any, 1 constant w0, 2 w0 for the first S / 2 samples and
+  // -w0 for the rest; 1 and 2 let the polyphase sums run
+  int pulse_kind;
+  float pulse_w0;
   float2* z;
 };
 
@@ -122,6 +126,43 @@ __global__ void __launch_bounds__(256) nc_frontend_kernel(NcFrontParams p) {
   }
   __syncthreads();
   const size_t seq0 = ((size_t)ab * p.B + blk) * S;
+  if (p.pulse_kind != 0 && S >= 4) {
+    // runs of S / 4 residues per thread, each sum from the previous one
+    // (the drop-in front end's rule): with a = jj S + rho,
+    //   constant w0:   z(rho + 1) = z(rho) + w0 (f[a + S] - f[a])
+    //   w0 / -w0:      z(rho + 1) = z(rho) + w0 (2 f[a + S/2] - f[a] - f[a + S])
+    const int L = (S + 3) / 4, H = S / 2;
+    const float w0 = p.pulse_w0;
+    const bool boc = p.pulse_kind == 2;
+    for (int o = threadIdx.x; o < 4 * nj; o += blockDim.x) {
+      const int k = o / nj, jj = o - k * nj;
+      const int rho0 = k * L, rho1 = min(rho0 + L, S);
+      if (rho0 >= S) continue;
+      float2 z = make_float2(0.f, 0.f);
+      const int base = jj * S + rho0 + jj;
+      for (int s = 0; s < S; ++s) {
+        const float2 v = fsm[base + s + (rho0 + s >= S ? 1 : 0)];
+        const float w = p.pulse[s];
+        z.x = fmaf(w, v.x, z.x);
+        z.y = fmaf(w, v.y, z.y);
+      }
+      p.z[(seq0 + rho0) * Lc + j0 + jj] = z;
+      for (int rho = rho0; rho + 1 < rho1; ++rho) {
+        const int a = jj * S + rho;
+        const float2 fa = fsm[a + jj], fe = fsm[a + S + jj + 1];
+        if (boc) {
+          const float2 fm = fsm[a + H + jj + (rho + H >= S ? 1 : 0)];
+          z.x += w0 * (2.f * fm.x - fa.x - fe.x);
+          z.y += w0 * (2.f * fm.y - fa.y - fe.y);
+        } else {
+          z.x += w0 * (fe.x - fa.x);
+          z.y += w0 * (fe.y - fa.y);
+        }
+        p.z[(seq0 + rho + 1) * Lc + j0 + jj] = z;
+      }
+    }
+    return;
+  }
   for (int o = threadIdx.x; o < S * nj; o += blockDim.x) {
     const int rho = o / nj, jj = o - rho * nj;
     float2 z = make_float2(0.f, 0.f);
@@ -367,6 +408,14 @@ cudaError_t launch_nc_frontend(const SampleSource& src, const SearchDims& dims, 
   p.B = B;
   p.start = start;
   for (int i = 0; i < kMaxPulse; ++i) p.pulse[i] = pc.pulse[i];
+  // the pulse's shape (see NcFrontParams)
+  p.pulse_w0 = pc.pulse[0];
+  bool constant = true, boc = pc.S % 2 == 0;
+  for (int i = 0; i < pc.S; ++i) {
+    constant = constant && pc.pulse[i] == pc.pulse[0];
+    boc = boc && pc.pulse[i] == (i < pc.S / 2 ? pc.pulse[0] : -pc.pulse[0]);
+  }
+  p.pulse_kind = constant ? 1 : (boc ? 2 : 0);
   p.z = d_z;
   const int span = kNcJ * pc.S + pc.S;
   const size_t smem = (size_t)(span + span / pc.S + 1 + K + 8) * sizeof(float2);
