@@ -1024,8 +1024,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
             const int j = e / T::NR1, r = e - j * T::NR1;
             const int s = r / T::ROWS1, u = r - s * T::ROWS1;
             const int rho = g * BC + s;
-            if (rho < S)
-              zr[k] = __ldcs(p.z16 + ((((size_t)ab_h * B + blk) * S + rho) * 8 + j) * T::ROWS1 + u);
+            // the drop-in search reads its Z once (evict first); the
+            // non-coherent search reads each block again for every PRN
+            // pair, so it keeps the blocks in L2
+            if (rho < S) {
+              const uint4* src = p.z16 + ((((size_t)ab_h * B + blk) * S + rho) * 8 + j) * T::ROWS1 + u;
+              zr[k] = NCB ? __ldcg(src) : __ldcs(src);
+            }
           }
         }
       };
