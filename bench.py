@@ -211,8 +211,9 @@ def fp64_peak_errors(bits, runs, threads):
     """Peak-metric error of the GPU searches against the oracle in float64 on
     a bounded sample of the benchmark recording (antenna 0, the PRNs of the
     CPU baseline sample, all 41 bins): per constellation, the largest
-    relative error of signal_strength and whether code phase, bin and
-    hypothesis equal the FP64 result.  runs: {arithmetic: cells}."""
+    relative error of signal_strength, the largest C/N0 (ACR, dB-Hz) error
+    and whether code phase, bin, hypothesis and C/N0 validity equal the FP64
+    result.  runs: {arithmetic: cells}."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import acq_oracle as O
     names = {O.GPS: "GPS L1 C/A", O.SBAS: "SBAS", O.QZSS: "QZSS", O.GALILEO: "Galileo E1-C",
@@ -222,18 +223,22 @@ def fp64_peak_errors(bits, runs, threads):
     ub = np.unpackbits(bits[:1], axis=1)
     out = {}
     for c, prns in sample.items():
-        ref = O.acquire_all(ub, FS, c, prn_filter=prns, precision="f64", threads=threads)
+        ref = O.acquire_all(ub, FS, c, prn_filter=prns, cn0=True, precision="f64", threads=threads)
         per = {}
         for arith, cells in runs.items():
-            worst, same = 0.0, True
+            worst, worst_cn0, same = 0.0, 0.0, True
             for r in ref["results"]:
                 rc = r["cells"][0]
                 g = cells[(cells["constellation"] == c) & (cells["prn"] == rc["prn"]) & (cells["antenna"] == 0)][0]
                 worst = max(worst, abs(g["signal_strength"] - rc["signal_strength"]) / rc["signal_strength"])
+                rcn0 = (r.get("cn0_acr") or [None])[0]
                 same &= (int(g["best_codephase"]) == int(rc["best_codephase"]) and
                          int(g["best_freq_idx"]) == int(rc["best_freq_idx"]) and
-                         int(g["hypothesis"]) == int(rc["hypothesis"]))
-            per[arith] = {"max_rel_peak_error": worst, "same_cell": bool(same)}
+                         int(g["hypothesis"]) == int(rc["hypothesis"]) and
+                         bool(g["cn0_valid"]) == (rcn0 is not None))
+                if rcn0 is not None and g["cn0_valid"]:
+                    worst_cn0 = max(worst_cn0, abs(float(g["cn0_acr"]) - rcn0))
+            per[arith] = {"max_rel_peak_error": worst, "max_cn0_error_db": worst_cn0, "same_cell": bool(same)}
         out[names[c]] = per
     return out
 
