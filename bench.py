@@ -292,7 +292,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--n-ant", type=int, default=N_ANT, help="antennas per GPU (profiling runs use fewer)")
-    ap.add_argument("--variant10", type=int, default=None, help="launch-shape variant of the Lc=10230 kernels")
+    ap.add_argument("--variant10", type=int, default=None, help="launch-shape variant of the Lc=10230 kernels "
+                    "(skips the autotuner)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--precision", default="fp16tc", choices=["fp32", "fp16tc"],
                     help="search arithmetic of the headline: FP16 tensor-core transform with FP32 refinement "
                          "(default), or FP32 CUDA cores")
@@ -352,11 +354,16 @@ def main():
         lib.tga_kernel_times(ctx._h, cap, names, ms, la, fl, ctypes.byref(n))
         return {names[i].decode(): (ms[i], la[i], fl[i]) for i in range(min(n.value, cap))}
 
+    tuned = {}
+
     def measure(precision):
         """W warm-up and K timed device steps of one arithmetic; every rank
         takes the same collective steps.  Returns ms/step (max over ranks),
         cells, per-kernel times, launches and the last step's cells."""
         ctx.set_precision(prec_id[precision])
+        if args.variant10 is None and not args.no_autotune:
+            # launch shapes picked on this workload, before the warm-up
+            tuned[precision] = ctx.autotune(d_bits.data_ptr(), n_ant, row_bytes, FS, mask=tga.ALL, cn0=True, reps=3)
         for _ in range(args.warmup):
             step_device()
         torch.cuda.synchronize()
@@ -596,6 +603,13 @@ def main():
             "roofline": roofline(agg, args.precision, sm_mhz),
             "kernels": kernels(agg),
             "clocks": clocks}
+    if tuned:
+        # tga_autotune on this workload before each arithmetic's warm-up: the
+        # launch shape kept per code length and the step time of each variant
+        line["autotune"] = {dtype[p]: [{"lc": e["lc"], "variant": e["variant"],
+                                        "ms_per_variant": [round(m, 3) for m in e["ms"]],
+                                        "same_results": e["same_results"]} for e in v]
+                            for p, v in tuned.items()}
     if other is not None:
         oprec, oms, ocells, oagg, olaunch, oout = other
         da, ka = detections(out)

@@ -252,10 +252,32 @@ int tga_set_test_flags(tga_ctx* ctx, int flags);
 #define TGA_PRECISION_FP32 0
 #define TGA_PRECISION_FP16_TC 1
 int tga_set_precision(tga_ctx* ctx, int precision);
-/* Launch-shape variant of the transform kernels for chip count lc (1023,
- * 4092, 10230): 0 = default; 1 (10230 only) = two polyphase branches per
- * CTA sharing the code spectrum.  Results are identical; only speed varies. */
+/* Launch-shape variant of this context's FP32 correlation kernels, for its
+ * current precision (each precision keeps its own), for chip
+ * count lc (1023, 4092, 10230): 0 = default; 1 = twice the polyphase
+ * branches per CTA (16, 4, 2) at one CTA per SM, sharing the code spectrum
+ * in L1.  Results are identical; only speed varies.  (The tensor-core
+ * search takes the variant in its FP32 re-evaluation of the selected row.) */
 int tga_set_variant(tga_ctx* ctx, int lc, int variant);
+
+/* One code length tuned by tga_autotune. */
+typedef struct {
+  int32_t lc;            /* chip count: 1023, 4092 or 10230 */
+  int32_t variant;       /* the variant kept (now set on the context) */
+  double ms[2];          /* median device time of the whole search per variant */
+  int32_t same_results[2]; /* 1 if that variant's cells equal variant 0's */
+} tga_tune_entry;
+
+/* Autotuner of the launch shapes: runs the search tga_acquire_all_device
+ * would run (packed bits on the device) once untimed and `reps` times timed
+ * per candidate variant of each code length in the search, one length at a
+ * time with the others fixed, and keeps on the context (for its current
+ * precision) the fastest variant whose cells equal variant 0's.  The search's code lengths come out in
+ * out[0..*n_out), ascending.  Graphs are off while it runs; later searches
+ * build their graphs with the kept variants.  reps: 1-100. */
+int tga_autotune(tga_ctx* ctx, const uint8_t* d_packed_bits, size_t n_ant, size_t row_bytes,
+                 double sampling_freq, const tga_all_options* opt, int reps, tga_tune_entry out[3],
+                 size_t* n_out);
 /* CUDA graphs for tga_acquire_all / tga_acquire_all_device (enabled by
  * default).  A search plan (bits buffer, shapes, options, precision,
  * variant) runs eagerly on its first call, is captured into a CUDA graph on

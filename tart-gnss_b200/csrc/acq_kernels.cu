@@ -474,8 +474,11 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
 }
 
 // Launch configurations: (third digit M, slots per CTA, threads, min CTAs/SM).
-// Variant 0 is the default; the other variants are alternatives kept for
-// tuning (selected with tga_set_variant).
+// Variant 0 is the default; variant 1 doubles the polyphase branches (slots)
+// and threads of a CTA at one CTA per SM, so more branches of one (row, PRN)
+// item share the code spectrum in L1.  The correlation modes take the
+// variant of the class (PolyClass::variant, set by tga_set_variant or
+// tga_autotune); the forward transforms always run variant 0.
 template <int M, int V>
 struct PfaCfg;
 template <>
@@ -483,8 +486,16 @@ struct PfaCfg<1, 0> {
   static constexpr int BC = 8, NT = 288, MINB = 2;  // 8 x 33 DFT-31 columns
 };
 template <>
+struct PfaCfg<1, 1> {
+  static constexpr int BC = 16, NT = 576, MINB = 1;
+};
+template <>
 struct PfaCfg<4, 0> {
   static constexpr int BC = 2, NT = 288, MINB = 2;  // 2 x 132 columns
+};
+template <>
+struct PfaCfg<4, 1> {
+  static constexpr int BC = 4, NT = 576, MINB = 1;
 };
 template <>
 struct PfaCfg<10, 0> {
@@ -494,12 +505,6 @@ template <>
 struct PfaCfg<10, 1> {
   static constexpr int BC = 2, NT = 704, MINB = 1;  // two rho slots share D in L1
 };
-
-static int g_variant10 = 0;
-void set_pfa_variant(int M, int v) {
-  if (M == 10) g_variant10 = v;
-}
-int pfa_variant(int M) { return M == 10 ? g_variant10 : 0; }
 
 template <int M, int V, int MODE>
 static cudaError_t run_pfa(const PfaParams& p, int n_work_slots, int num_sms, cudaStream_t st) {
@@ -522,14 +527,22 @@ static cudaError_t run_pfa(const PfaParams& p, int n_work_slots, int num_sms, cu
 }
 
 template <int MODE>
-static cudaError_t dispatch_pfa(int M, const PfaParams& p, int n_work_slots, int num_sms, cudaStream_t st) {
-  switch (M) {
+static cudaError_t dispatch_pfa(const PolyClass& pc, const PfaParams& p, int n_work_slots, int num_sms,
+                                cudaStream_t st) {
+  if constexpr (MODE == CORR || MODE == SECOND || MODE == REFINE) {
+    if (pc.variant == 1) {
+      switch (pc.M) {
+        case 1: return run_pfa<1, 1, MODE>(p, n_work_slots, num_sms, st);
+        case 4: return run_pfa<4, 1, MODE>(p, n_work_slots, num_sms, st);
+        case 10: return run_pfa<10, 1, MODE>(p, n_work_slots, num_sms, st);
+      }
+      return cudaErrorInvalidValue;
+    }
+  }
+  switch (pc.M) {
     case 1: return run_pfa<1, 0, MODE>(p, n_work_slots, num_sms, st);
     case 4: return run_pfa<4, 0, MODE>(p, n_work_slots, num_sms, st);
-    case 10:
-      if (g_variant10 == 1 && (MODE == CORR || MODE == SECOND || MODE == REFINE))
-        return run_pfa<10, 1, MODE>(p, n_work_slots, num_sms, st);
-      return run_pfa<10, 0, MODE>(p, n_work_slots, num_sms, st);
+    case 10: return run_pfa<10, 0, MODE>(p, n_work_slots, num_sms, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -540,7 +553,7 @@ cudaError_t launch_forward_z(const PolyClass& pc, int n_ab, float2* d_z, int num
   p.n_seq = n_ab * 2 * pc.S;
   p.S = pc.S;
   p.P = pc.P;
-  return dispatch_pfa<FWD_Z>(pc.M, p, p.n_seq, num_sms, st);
+  return dispatch_pfa<FWD_Z>(pc, p, p.n_seq, num_sms, st);
 }
 
 std::vector<uint16_t> tc_unit_map(int M) {
@@ -574,7 +587,7 @@ cudaError_t launch_forward_z_tc(const PolyClass& pc, int n_ab, float2* d_z, void
   p.n_seq = n_ab * 2 * pc.S;
   p.S = pc.S;
   p.P = pc.P;
-  return dispatch_pfa<FWD_Z>(pc.M, p, p.n_seq, num_sms, st);
+  return dispatch_pfa<FWD_Z>(pc, p, p.n_seq, num_sms, st);
 }
 
 cudaError_t launch_forward_seqs_tc(const PolyClass& pc, long long n_seq, float2* d_z, void* d_z16, const void* d_map,
@@ -588,7 +601,7 @@ cudaError_t launch_forward_seqs_tc(const PolyClass& pc, long long n_seq, float2*
   p.n_seq = (int)n_seq;
   p.S = pc.S;
   p.P = pc.P;
-  return dispatch_pfa<FWD_Z>(pc.M, p, p.n_seq, num_sms, st);
+  return dispatch_pfa<FWD_Z>(pc, p, p.n_seq, num_sms, st);
 }
 
 cudaError_t launch_forward_seqs(const PolyClass& pc, long long n_seq, float2* d_z, int num_sms, cudaStream_t st) {
@@ -598,7 +611,7 @@ cudaError_t launch_forward_seqs(const PolyClass& pc, long long n_seq, float2* d_
   p.n_seq = (int)n_seq;
   p.S = pc.S;
   p.P = pc.P;
-  return dispatch_pfa<FWD_Z>(pc.M, p, p.n_seq, num_sms, st);
+  return dispatch_pfa<FWD_Z>(pc, p, p.n_seq, num_sms, st);
 }
 
 cudaError_t launch_code_spectra(const PolyClass& pc, const int8_t* d_chips, int n_prn, float2* d_D,
@@ -609,7 +622,7 @@ cudaError_t launch_code_spectra(const PolyClass& pc, const int8_t* d_chips, int 
   p.n_seq = n_prn * 2;
   p.S = pc.S;
   p.P = pc.P;
-  return dispatch_pfa<FWD_D>(pc.M, p, p.n_seq, num_sms, st);
+  return dispatch_pfa<FWD_D>(pc, p, p.n_seq, num_sms, st);
 }
 
 cudaError_t launch_correlate(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
@@ -623,7 +636,7 @@ cudaError_t launch_correlate(const PolyClass& pc, const SearchDims& dims, const 
   p.S = pc.S;
   p.P = pc.P;
   p.n_items = dims.n_ant * dims.nb * 2 * dims.n_prn;
-  return dispatch_pfa<CORR>(pc.M, p, p.n_items, num_sms, st);
+  return dispatch_pfa<CORR>(pc, p, p.n_items, num_sms, st);
 }
 
 cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
@@ -638,7 +651,7 @@ cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, cons
   p.P = pc.P;
   p.chip_width = chip_width;
   p.n_items = dims.n_ant * dims.n_prn;
-  return dispatch_pfa<SECOND>(pc.M, p, p.n_items, num_sms, st);
+  return dispatch_pfa<SECOND>(pc, p, p.n_items, num_sms, st);
 }
 
 cudaError_t launch_refine(const PolyClass& pc, const SearchDims& dims, const float2* d_Z, const float2* d_D,
@@ -652,7 +665,7 @@ cudaError_t launch_refine(const PolyClass& pc, const SearchDims& dims, const flo
   p.S = pc.S;
   p.P = pc.P;
   p.n_items = dims.n_ant * dims.n_prn;
-  return dispatch_pfa<REFINE>(pc.M, p, p.n_items, num_sms, st);
+  return dispatch_pfa<REFINE>(pc, p, p.n_items, num_sms, st);
 }
 
 // Second peak from the rows REFINE left in rowbuf (correlate.rs:157-175, the

@@ -19,6 +19,9 @@ constexpr int kMaxBins = 4096;
 struct PolyClass {
   int P = 0, S = 0, Lc = 0, M = 0;  // M = Lc / 1023
   float pulse[kMaxPulse] = {};
+  // launch shape of the FP32 correlation kernels (0 = default, 1 = twice the
+  // polyphase branches per CTA at one CTA per SM); results do not depend on it
+  int variant = 0;
 };
 
 // Sample source of the front end.
@@ -154,11 +157,6 @@ cudaError_t launch_generic(const GenericPlan& gp, const float* d_sig, const doub
 size_t generic_work_elems(const GenericPlan& gp, int nb);
 cudaError_t launch_bits_to_signal(const uint8_t* d_bits, size_t row_bytes, int row, const double* d_mean, int n,
                                   double pc, float* d_sig, double* d_pp, cudaStream_t st);
-
-// Selects an alternative launch configuration of the transform kernels for
-// third digit M (tuning; 0 = default).
-void set_pfa_variant(int M, int v);
-int pfa_variant(int M);
 
 // fine acquisition: per (task, antenna) the complex sums R, dR/dtau, dR/df,
 // d2R/dtau2, d2R/df2, d2R/dtau df (un-normalised), zeroed and accumulated

@@ -53,6 +53,8 @@ struct tga_ctx {
   double last_ms = 0.0;
   uint64_t h2d = 0, d2h = 0;
   int precision = 0;  // TGA_PRECISION_*
+  // FP32 correlation launch shape per precision for Lc = 1023, 4092, 10230
+  int variant[2][3] = {{0, 0, 0}, {0, 0, 0}};
   // per-kernel event timing
   bool profiling = false;
   struct Pending {
@@ -359,6 +361,8 @@ const std::vector<int8_t>& cached_chips(tga_ctx* ctx, int c, int prn) {
 // chip count has no fused kernel.  The check is exact (every sample of every
 // PRN is compared with the reference's resampling rule) and cached per
 // context, since it depends only on (constellation, rate, period, PRN).
+int variant_slot(int M) { return M == 1 ? 0 : M == 4 ? 1 : 2; }
+
 bool poly_class_for(tga_ctx* ctx, int c, double samples_per_code, size_t P, size_t N,
                     const std::vector<int>& prns, PolyClass* out) {
   const ConstellationInfo& ci = info(c);
@@ -401,6 +405,7 @@ bool poly_class_for(tga_ctx* ctx, int c, double samples_per_code, size_t P, size
   }
   if (!cc.structure_ok) return false;
   *out = cc.pc;
+  out->variant = ctx->variant[ctx->precision][variant_slot(out->M)];
   return true;
 }
 
@@ -705,9 +710,11 @@ int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, si
     // the plan: everything the launches take by value or by address
     std::string key;
     char kb[512];
-    const int kn = std::snprintf(kb, sizeof kb, "%p/%zu/%zu/%a/%a/%d/%d/%d/%d/%d/%d|", (const void*)d_bits,
+    const int kn = std::snprintf(kb, sizeof kb, "%p/%zu/%zu/%a/%a/%d/%d/%d/%d/%d%d%d/%d|", (const void*)d_bits,
                                  n_ant_total, row_bytes, fs, opt->center_freq, nb, opt->cn0, ctx->precision,
-                                 ctx->test_flags, pfa_variant(10), chip_width_of(fs));
+                                 ctx->test_flags, ctx->variant[ctx->precision][0],
+                                 ctx->variant[ctx->precision][1], ctx->variant[ctx->precision][2],
+                                 chip_width_of(fs));
     if (kn < 0 || kn >= (int)sizeof kb) throw std::runtime_error("search plan key does not fit");
     key = kb;
     for (int32_t a : ants) key += std::to_string(a) + ",";
@@ -1163,8 +1170,70 @@ int tga_set_precision(tga_ctx* ctx, int precision) {
 
 int tga_set_variant(tga_ctx* ctx, int lc, int variant) {
   if (!ctx || (lc != 1023 && lc != 4092 && lc != 10230) || variant < 0 || variant > 1) return TGA_ERR_INVALID_ARG;
-  set_pfa_variant(lc / 1023, variant);
+  ctx->variant[ctx->precision][variant_slot(lc / 1023)] = variant;
   return TGA_OK;
+}
+
+int tga_autotune(tga_ctx* ctx, const uint8_t* d_packed_bits, size_t n_ant, size_t row_bytes, double fs,
+                 const tga_all_options* opt, int reps, tga_tune_entry out[3], size_t* n_out) {
+  return guarded(ctx, [&] {
+    if (!d_packed_bits || !opt || !out || !n_out) throw InvalidArg("null argument");
+    if (reps < 1 || reps > 100) throw InvalidArg("reps must be 1-100");
+    size_t n_cells = 0;
+    if (tga_all_cell_count(n_ant, opt, &n_cells) != TGA_OK) throw InvalidArg("invalid options");
+    bool has[3] = {false, false, false};
+    for (int c = 0; c < N_CONST; ++c)
+      if (opt->constellation_mask & (1u << c)) has[variant_slot(info(c).primary_chips / 1023)] = true;
+    // every candidate runs eagerly, so no graph is kept for a rejected one
+    struct GraphsOff {
+      tga_ctx* c;
+      bool was;
+      ~GraphsOff() { c->graphs_enabled = was; }
+    } graphs_off{ctx, ctx->graphs_enabled};
+    ctx->graphs_enabled = false;
+    int* var = ctx->variant[ctx->precision];
+    std::vector<tga_cell> ref(n_cells), cur(n_cells);
+    // one untimed run, then the median device time of `reps` runs
+    auto measure = [&](std::vector<tga_cell>& cells, double* ms) -> int {
+      std::vector<double> t;
+      for (int r = 0; r <= reps; ++r) {
+        size_t n = 0;
+        begin_call(ctx);
+        const int rc = acquire_all_impl(ctx, d_packed_bits, n_ant, row_bytes, fs, opt, cells.data(),
+                                        cells.size(), &n);
+        if (rc != TGA_OK) return rc;
+        if (r > 0) t.push_back(ctx->last_ms);
+      }
+      std::sort(t.begin(), t.end());
+      *ms = t[t.size() / 2];
+      return TGA_OK;
+    };
+    auto same = [](const std::vector<tga_cell>& a, const std::vector<tga_cell>& b) {
+      return a.size() == b.size() && std::memcmp(a.data(), b.data(), a.size() * sizeof(tga_cell)) == 0;
+    };
+    static const int kLc[3] = {1023, 4092, 10230};
+    size_t k = 0;
+    for (int slot = 0; slot < 3; ++slot) {
+      if (!has[slot]) continue;
+      tga_tune_entry& e = out[k++];
+      e.lc = kLc[slot];
+      int best = 0;
+      for (int v = 0; v < 2; ++v) {
+        var[slot] = v;
+        const int rc = measure(v == 0 ? ref : cur, &e.ms[v]);
+        if (rc != TGA_OK) {
+          var[slot] = 0;
+          return rc;
+        }
+        e.same_results[v] = v == 0 ? 1 : same(ref, cur);
+        if (e.same_results[v] && e.ms[v] < e.ms[best]) best = v;
+      }
+      var[slot] = best;
+      e.variant = best;
+    }
+    *n_out = k;
+    return TGA_OK;
+  });
 }
 
 int tga_set_graphs(tga_ctx* ctx, int enable) {

@@ -58,6 +58,12 @@ class BenchEntry(ctypes.Structure):
                 ("search_s", ctypes.c_double), ("result", Result)]
 
 
+class TuneEntry(ctypes.Structure):
+    """tga_tune_entry: one code length tuned by tga_autotune."""
+    _fields_ = [("lc", ctypes.c_int32), ("variant", ctypes.c_int32), ("ms", ctypes.c_double * 2),
+                ("same_results", ctypes.c_int32 * 2)]
+
+
 class Cell(ctypes.Structure):
     _fields_ = [("constellation", ctypes.c_int32), ("prn", ctypes.c_int32), ("antenna", ctypes.c_int32),
                 ("best_freq_idx", ctypes.c_int32), ("best_codephase", ctypes.c_int64),
@@ -163,6 +169,7 @@ def lib():
     L.tga_set_profiling.argtypes = [_P, i32]
     L.tga_set_graphs.argtypes = [_P, i32]
     L.tga_benchmark.argtypes = [_P, _P, sz, sz, dbl, _P]
+    L.tga_autotune.argtypes = [_P, _P, sz, sz, dbl, _P, i32, _P, _P]
     L.tga_last_graph.argtypes = [_P, ctypes.POINTER(ctypes.c_int)]
     L.tga_set_variant.argtypes = [_P, i32, i32]
     L.tga_set_precision.argtypes = [_P, i32]
@@ -410,6 +417,25 @@ class Context:
                                         out))
         return [{"constellation": e.constellation, "prn": e.prn, "setup_s": e.setup_s, "search_s": e.search_s,
                  "result": e.result} for e in out]
+
+    def autotune(self, device_bits, n_ant, row_bytes, sampling_freq, mask=ALL, ant_filter=None,
+                 prn_filter=None, center_freq=GPS_IF, search_band=GPS_SEARCH_BAND, cn0=False, reps=3):
+        """tga_autotune: time each launch-shape variant on this search (bits
+        on the device, an integer pointer) and keep the fastest per code
+        length on the context.  Returns one dict per code length searched:
+        lc, variant (kept), ms [variant 0, variant 1], same_results."""
+        o, keep = self._options(mask, ant_filter, prn_filter, center_freq, search_band, cn0, False)
+        out = (TuneEntry * 3)()
+        n = ctypes.c_size_t()
+        self._check(lib().tga_autotune(self._h, ctypes.c_void_p(device_bits), n_ant, row_bytes,
+                                       float(sampling_freq), ctypes.byref(o), int(reps), out, ctypes.byref(n)))
+        del keep
+        return [{"lc": e.lc, "variant": e.variant, "ms": list(e.ms), "same_results": [bool(x) for x in e.same_results]}
+                for e in out[:n.value]]
+
+    def set_variant(self, lc, variant):
+        """Launch-shape variant (0 or 1) of the FP32 correlation kernels for chip count lc."""
+        self._check(lib().tga_set_variant(self._h, int(lc), int(variant)))
 
     def set_profiling(self, enable):
         """Per-kernel CUDA-event timing of later calls (tga_kernel_times)."""
