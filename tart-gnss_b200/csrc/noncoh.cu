@@ -37,7 +37,7 @@ struct NcFrontParams {
   float2* z;
 };
 
-constexpr int kNcJ = 64;  // chips per CTA
+constexpr int kNcJ = 128;  // chips per CTA: at S = 16, eight folded samples for each of 256 threads
 
 // bit n of the row (1 for a + sample)
 __device__ __forceinline__ int sample_bit(const uint8_t* __restrict__ row_bits, long long n) {
@@ -91,6 +91,7 @@ __global__ void __launch_bounds__(256) nc_frontend_kernel(NcFrontParams p) {
       float2 acc[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) acc[j] = make_float2(0.f, 0.f);
+#pragma unroll 5
       for (int k = 0; k < p.K; ++k) {
         const long long n = n0 + (long long)k * P + m0;
         const long long byte = n >> 3;
