@@ -37,7 +37,7 @@ struct NcFrontParams {
   float2* z;
 };
 
-constexpr int kNcJ = 128;  // chips per CTA: at S = 16, eight folded samples for each of 256 threads
+constexpr int kNcJ = 256;  // chips per CTA: at S = 16, two groups of eight folded samples per thread
 
 // bit n of the row (1 for a + sample)
 __device__ __forceinline__ int sample_bit(const uint8_t* __restrict__ row_bits, long long n) {
