@@ -183,7 +183,10 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_sample_baseline(threads, repeats=1):
+CPU_SAMPLE_REPEATS = 16  # ~10 s of oracle work per sample on a 16-core host
+
+
+def cpu_sample_baseline(threads, repeats=CPU_SAMPLE_REPEATS):
     """CPU restatement of the reference algorithm (oracle) on a bounded sample
     of the same workload: antenna 0, a PRN subset of every constellation, all
     41 bins.  Returns (cells/s, seconds, sample description)."""
