@@ -41,21 +41,48 @@ FS = 16.368e6
 N_ANT = 24
 SAMPLES = 1636800  # 100 ms
 SEED = 0x5EED2026 + 1
-METRIC = "acq cells/s, --all x 24 ant"
+METRIC = "acq cells/s, --all x 24 ant: BF16-TC vs FP32 fused on B200, same detections"
 WORKLOAD = ("--all x 24 ant, 16.368 MHz 1-bit, 100 ms synthetic, 276 PRNs x 41 bins x 300 Hz, "
             "2-period coherent dual-hypothesis, --cn0")
+# PRNs of each code length in the --all search (GPS 38 + SBAS 39 + QZSS 23;
+# Galileo 50; BeiDou 63 + L1C 63) and the samples per chip at 16.368 MHz
+GROUP_PRNS = {1023: 100, 4092: 50, 10230: 126}
+SAMPLES_PER_CHIP = 16
 
 
-def synth_observation(seed, n_ant=N_ANT, n_samples=SAMPLES, chunk=163680):
-    """Seeded synthetic 1-bit recording (see module docstring)."""
+def workload_config(n_ant):
+    """The `config` object of both arms: the workload only, nothing of the
+    arithmetic or the implementation that runs it."""
+    cells = sum(n_ant * 41 * n * SAMPLES_PER_CHIP * lc for lc, n in GROUP_PRNS.items())
+    return {"workload": WORKLOAD, "n_ant": n_ant, "cells_per_step_per_gpu": float(cells),
+            "l2": "256 MB buffer written between timed steps; 3.9 GB intermediate per step",
+            "parallelism": "replicas (weak scaling: one 24-antenna observation per GPU)"}
+
+
+def tga_codes(c, prn, period):
+    """One period of a PRN's resampled code from the library (GPU arm)."""
     import tga
+    return tga.code_resampled(c, int(prn), float(period), period).astype(np.float32)
+
+
+def oracle_codes(c, prn, period):
+    """The same code from the oracle's C restatement (reference arm, so that
+    arm never loads the library; tests/test_lib_cpu.py pins the two equal)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import acq_oracle as O
+    return O.resampled_code(c, int(prn), float(period), period).astype(np.float32)
+
+
+def synth_observation(seed, n_ant=N_ANT, n_samples=SAMPLES, chunk=163680, codes=tga_codes):
+    """Seeded synthetic 1-bit recording (see module docstring).  `codes`
+    makes one period of a PRN's code; both generators give identical bits."""
     rng = np.random.default_rng(seed)
     sats = []
     for c in range(6):
         lo, hi = {0: (1, 38), 1: (1, 50), 2: (1, 63), 3: (120, 158), 4: (1, 63), 5: (184, 206)}[c]
         P = int(FS / 1000.0) if c in (0, 3, 5) else int(FS * (0.004 if c == 1 else 0.010))
         for prn in rng.choice(np.arange(lo, hi + 1), size=10, replace=False):
-            code = tga.code_resampled(c, int(prn), float(P), P).astype(np.float32)
+            code = codes(c, prn, P)
             n_ep = n_samples // P + 2
             sats.append(dict(c=c, prn=int(prn), P=P, code=code, delay=int(rng.integers(0, P)),
                              dop=float(rng.uniform(-4000, 4000)), cn0=float(rng.uniform(38, 50)),
@@ -192,7 +219,7 @@ def cpu_sample_baseline(threads, repeats=CPU_SAMPLE_REPEATS):
     41 bins.  Returns (cells/s, seconds, sample description)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import acq_oracle as O
-    bits, _ = synth_observation(SEED, n_ant=1)
+    bits, _ = synth_observation(SEED, n_ant=1, codes=oracle_codes)
     ub = np.unpackbits(bits, axis=1)
     sample = {O.GPS: [1, 2, 3, 4], O.SBAS: [120, 121], O.QZSS: [184], O.GALILEO: [1, 2], O.BEIDOU: [1, 2],
               O.L1C: [1, 2]}
@@ -246,6 +273,12 @@ def fp64_peak_errors(bits, runs, threads):
     return out
 
 
+# tensor-core MMA FLOPs per complex output point of the inverse transform,
+# by code length: the Good-Thomas stages 31 x 33 (Lc = 1023), 31 x 12 x 11
+# (4092) and 31 x 30 x 11 (10230) as real 2R x 2R GEMMs, 8 R per stage
+TC_MMA_FLOPS_PER_POINT = {1023: 8 * (31 + 33), 4092: 8 * (31 + 12 + 11), 10230: 8 * (31 + 30 + 11)}
+
+
 def fp32_peak_tflops(sm_mhz, n_sm=148):
     return n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
 
@@ -264,8 +297,9 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "sample": "bounded CPU sample"},
-            "cpu_baseline": {"value": value, "unit": "cells/s", "cores": threads, "kind": "port", "sample": desc},
+            "data": "synthetic", "config": workload_config(N_ANT),
+            "cpu_baseline": {"value": value, "unit": "cells/s", "cores": threads, "kind": "port",
+                             "sample": "bounded sample of the workload: " + desc},
             "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -403,34 +437,46 @@ def main():
         return ms_step, cells, agg, launches, out
 
     def roofline(agg, precision, sm_mhz):
-        """Dominant kernel of a run against its roofline: the tensor-core
-        correlator against the measured sustained dense FP16/BF16 rate (it is
-        timed inside a long step), the FP32 kernels against the FP32 pipe."""
+        """Dominant kernel of a run against its roofline.  `achieved` counts
+        the algorithmic FLOPs the library reports per launch (5 P log2 P + 9 P
+        per correlation row of P lags: product, inverse FFT, power; the
+        executed arithmetic is larger).  The tensor-core correlator is held
+        against the measured sustained dense FP16/BF16 rate (it is timed
+        inside a long step), the FP32 kernels against the FP32 pipe.  For the
+        tensor-core kernel `tensor_pipe_util` is the fraction of that rate its
+        executed MMAs take (the DFT stages as dense real 2R x 2R GEMMs)."""
         dname, (dms, dl, dfl) = max(agg.items(), key=lambda kv: kv[1][0])
         avg_launch_s = dms / dl / 1e3
         achieved = dfl / dl / avg_launch_s / 1e12
         peaks = load_peaks()
+        extra = {}
         if precision == "fp16tc" and dname.startswith("correlate_tc"):
             if peaks and peaks.get("bf16_tflops_sustained"):
                 peak, src = float(peaks["bf16_tflops_sustained"]), "of measured: MEASURED_PEAKS.json bf16_tflops_sustained"
             else:
                 peak, src = 1400.0, "of fallback: sustained dense bf16 figure of the profiling recipe"
             bound = "tensor"
-            note = ("algorithmic FLOPs: the DFT stages as dense real 2R x 2R GEMMs, 8 x (sum of the radices) "
-                    "per complex output point")
+            lc = int(dname.split("Lc=")[1].rstrip("]"))
+            rows = n_ant * 41 * 2 * GROUP_PRNS[lc]
+            executed = rows * SAMPLES_PER_CHIP * lc * TC_MMA_FLOPS_PER_POINT[lc]
+            extra = {"tensor_pipe_util": executed / avg_launch_s / 1e12 / peak,
+                     "executed_tflops": executed / avg_launch_s / 1e12,
+                     "executed_flops": "the DFT stages as dense real 2R x 2R GEMMs, 8 x (sum of the radices) per "
+                                       "complex output point (%d at Lc = %d)" % (TC_MMA_FLOPS_PER_POINT[lc], lc)}
         else:
             peak = fp32_peak_tflops(sm_mhz)
             src = ("148 SM x 128 FP32 lanes x 2 flop x median SM clock under load (%.0f MHz); "
                    "MEASURED_PEAKS.json has no FP32 SIMT figure" % sm_mhz)
             bound = "fp32"
-            note = "algorithmic FLOPs of the prime-factor transform as executed (FMA = 2)"
         traffic = None
         tp = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tp):
             traffic = json.load(open(tp)).get(dname.split("[")[0], {}).get("bytes_per_launch")
-        return {"bound": bound, "kernel": dname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": traffic, "peak_source": src, "flops": note,
-                "flops_per_launch": dfl / dl, "avg_launch_ms": dms / dl}
+        return dict({"bound": bound, "kernel": dname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": src,
+                     "flops": "algorithmic: 5 P log2 P + 9 P per correlation row of P lags (two hypotheses per "
+                              "(antenna, bin, PRN))",
+                     "flops_per_launch": dfl / dl, "avg_launch_ms": dms / dl}, **extra)
 
     def kernels(agg):
         tot = sum(x[0] for x in agg.values())
@@ -594,12 +640,9 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": dtype[args.precision], "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_ant": n_ant, "cells_per_step_per_gpu": cells,
-                       "arithmetic": ("FP16 tensor-core (tcgen05) transform, FP32 accumulation, selected row "
-                                      "re-evaluated in FP32" if args.precision == "fp16tc"
-                                      else "FP32 CUDA-core transform"),
-                       "l2": "256 MB buffer written between timed steps; 3.9 GB intermediate per step",
-                       "parallelism": "replicas (weak scaling: one 24-antenna observation per GPU)"},
+            "config": workload_config(n_ant),
+            "arithmetic": ("FP16 tensor-core (tcgen05) transform, FP32 accumulation, selected rows "
+                           "re-evaluated in FP32" if args.precision == "fp16tc" else "FP32 CUDA-core transform"),
             "e2e": {"value": cells * world / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": h2d.value,
                     "d2h_bytes_per_step": d2h.value, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": launches,

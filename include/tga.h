@@ -161,16 +161,23 @@ int tga_acquire_l1c_single(tga_ctx* ctx, const float* h_signal_f32, const double
  *
  * Scratch comes from one fixed 16 MiB array in the library's device memory
  * (held on every GPU that loads the library until the process exits).  A
- * search needs n_bins * 2 * samples_per_chunk * 8 bytes plus ~0.2 MB: for
- * example GPS / SBAS / QZSS at 16.368 MHz with up to 61 bins (the
- * reference's +-6 kHz / 300 Hz grid has 41), or any constellation at the
- * reference's 1.023-2.046 MHz test rates.  Larger searches return
- * TGA_ERR_CAPACITY; windows other than two periods with a whole number of
- * samples per chip return TGA_ERR_UNSUPPORTED.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress) and uploads
- * constant tables: make it before any stream capture.  Every call shares the
- * array and leaves its contents behind (each call writes every part it
- * reads first); calls that overlap on the GPU race on it, so serialise them. */
+ * search fits when, with every term rounded up to a multiple of 256 bytes,
+ *   n_bins * 2 * samples_per_chunk * 8  +  2 * chips * 8  +  n_bins * 16
+ *   + n_bins * 8  +  (chips + 1)  +  about 800 bytes
+ * is at most 16 MiB (chips = 1023, 4092 or 10230): for example GPS / SBAS /
+ * QZSS at 16.368 MHz with up to 63 bins (the reference's +-6 kHz / 300 Hz
+ * grid has 41), Galileo at 4.092 MHz, or BeiDou / L1C at 2.046 MHz.  Larger
+ * searches return TGA_ERR_CAPACITY.  Only the fused polyphase search is
+ * built in: a window of exactly two periods with a whole number of samples
+ * per chip (samples_per_chunk a multiple of the chip count).  There is no
+ * generic fallback, so inputs that tga_acquire_single serves through its
+ * generic path (e.g. 16 MHz sampling) return TGA_ERR_UNSUPPORTED here.  The
+ * first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and uploads constant tables: make it before any
+ * stream capture.  Host threads may make their first calls at once (the
+ * set-up is serialised).  Every call shares the array and leaves its
+ * contents behind (each call writes every part it reads first); calls that
+ * overlap on the GPU race on it, so serialise them. */
 int tga_acquire_single_static(int constellation, const float* d_signal_f32,
                               const double* d_phasepoints, size_t num_samples,
                               double sampling_freq, double center_freq, double search_band,
@@ -233,7 +240,10 @@ int tga_last_transfer_bytes(const tga_ctx* ctx, uint64_t* h2d_bytes, uint64_t* d
 void* tga_stream(tga_ctx* ctx);
 /* Per-kernel device timing of later calls (CUDA events around each launch,
  * on the context stream).  tga_kernel_times returns, for the last call, up
- * to cap entries of (kernel name, total ms, launches, algorithmic FLOPs). */
+ * to cap entries of (kernel name, total ms, launches, algorithmic FLOPs).
+ * Algorithmic FLOPs count 5 N log2 N per complex FFT of N points, 6 per
+ * complex product, 3 per |y|^2 and 10 per wiped-off sample, whatever the
+ * kernel executes. */
 int tga_set_profiling(tga_ctx* ctx, int enable);
 /* Arithmetic of the correlation search.
  *  TGA_PRECISION_FP32 (default): every transform stage in FP32 on the CUDA

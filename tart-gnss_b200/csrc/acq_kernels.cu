@@ -28,8 +28,10 @@
 
 #include <vector>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 
 #include "dft.cuh"
 #include "engine.h"
@@ -38,7 +40,10 @@
 
 namespace tga {
 
-static int g_launches = 0;
+// Launches of the calling host thread: a search runs on the thread that
+// called the entry point, so a per-thread count is that call's count even
+// when several contexts run on several threads at once.
+static thread_local int g_launches = 0;
 int kernel_launch_count_reset() {
   int v = g_launches;
   g_launches = 0;
@@ -775,17 +780,26 @@ __constant__ double kAcrGps[59][2];
 __constant__ double kAcrGal[71][2];
 __constant__ double kAcrBds[79][2];
 __constant__ double kAcrL1c[79][2];
-static bool g_acr_uploaded[64] = {};
+// The tables are uploaded once per device, on the first call that needs them
+// (with that device current).  Host threads making their first calls at
+// once are serialised by the mutex; later calls only read the flag.
+constexpr int kAcrMaxDevices = 64;
+static std::atomic<bool> g_acr_uploaded[kAcrMaxDevices];
+static std::mutex g_acr_mutex;
 
 static cudaError_t upload_acr_tables() {
   int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && g_acr_uploaded[dev]) return cudaSuccess;
-  cudaError_t e = cudaMemcpyToSymbol(kAcrGps, TGA_GPS_L1_CA_ACR_TABLE, sizeof(kAcrGps));
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const bool cached = dev >= 0 && dev < kAcrMaxDevices;
+  if (cached && g_acr_uploaded[dev].load(std::memory_order_acquire)) return cudaSuccess;
+  std::lock_guard<std::mutex> lock(g_acr_mutex);
+  if (cached && g_acr_uploaded[dev].load(std::memory_order_relaxed)) return cudaSuccess;
+  e = cudaMemcpyToSymbol(kAcrGps, TGA_GPS_L1_CA_ACR_TABLE, sizeof(kAcrGps));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(kAcrGal, TGA_GALILEO_E1C_ACR_TABLE, sizeof(kAcrGal));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(kAcrBds, TGA_BEIDOU_B1C_ACR_TABLE, sizeof(kAcrBds));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(kAcrL1c, TGA_GPS_L1C_ACR_TABLE, sizeof(kAcrL1c));
-  if (e == cudaSuccess && dev >= 0 && dev < 64) g_acr_uploaded[dev] = true;
+  if (e == cudaSuccess && cached) g_acr_uploaded[dev].store(true, std::memory_order_release);
   return e;
 }
 

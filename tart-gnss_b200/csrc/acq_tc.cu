@@ -1200,16 +1200,6 @@ size_t tc_operand_bytes(const PolyClass& pc, long long n_seq, bool code) {
   return (size_t)n_seq * 8 * rows1 * 16;
 }
 
-double tc_gemm_flops_per_point(int M) {
-  // real-embedded DFT-R as a dense 2R x 2R GEMM: 8 R FLOPs per complex point and stage
-  switch (M) {
-    case 1: return 8.0 * (31 + Tc3Cfg<1>::R2);  // two stages
-    case 4: return 8.0 * (31 + Tc3Cfg<4>::R2 + Tc3Cfg<4>::R3);
-    case 10: return 8.0 * (31 + Tc3Cfg<10>::R2 + Tc3Cfg<10>::R3);
-  }
-  return 0.0;
-}
-
 std::vector<unsigned char> tc_dft_matrices(int M) {
   switch (M) {
     case 1: return build_matrices<1>();

@@ -112,7 +112,6 @@ cudaError_t launch_second_scan(const PolyClass& pc, const SearchDims& dims, floa
 // (comparisons only) and must be zeroed before the launch; *d_err is set
 // non-zero when a bounded wait on the tensor cores expired.
 size_t tc_operand_bytes(const PolyClass& pc, long long n_seq, bool code);
-double tc_gemm_flops_per_point(int M);
 // the three inverse-DFT matrices of class M in the correlator's shared-memory
 // layouts (FP16), to be uploaded once and passed as d_bmat
 std::vector<unsigned char> tc_dft_matrices(int M);

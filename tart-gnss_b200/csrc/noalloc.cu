@@ -19,9 +19,11 @@
 // on the GPU (concurrent streams or host threads) race on it.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 
 #include "../../include/tga.h"
 #include "engine.h"
@@ -35,7 +37,11 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 namespace {
 
 constexpr int kMaxDevices = 64;
-unsigned char* g_scratch_ptr[kMaxDevices] = {};
+// Per-device address of the scratch array.  Set once per device under the
+// mutex (host threads making their first calls at once wait for each
+// other), then only read.
+std::atomic<unsigned char*> g_scratch_ptr[kMaxDevices];
+std::mutex g_scratch_mutex;
 
 // Device address of the scratch array on the current device (set-up once).
 cudaError_t scratch_for_current_device(unsigned char** out) {
@@ -43,13 +49,19 @@ cudaError_t scratch_for_current_device(unsigned char** out) {
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch_ptr[dev] = (unsigned char*)p;
+  unsigned char* ptr = g_scratch_ptr[dev].load(std::memory_order_acquire);
+  if (!ptr) {
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    ptr = g_scratch_ptr[dev].load(std::memory_order_relaxed);
+    if (!ptr) {
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess) return e;
+      ptr = static_cast<unsigned char*>(p);
+      g_scratch_ptr[dev].store(ptr, std::memory_order_release);
+    }
   }
-  *out = g_scratch_ptr[dev];
+  *out = ptr;
   return cudaSuccess;
 }
 

@@ -338,16 +338,14 @@ void run_planned(tga_ctx* ctx, const std::string& key, F&& enqueue) {
   ctx->last_graph = TGA_GRAPH_CAPTURED;
 }
 
-// FP32 operations per transform point of one length-Lc inverse transform as
-// implemented (DFT-31 1950 flops per 31 points, DFT-33 948 per 33, DFT-4 16
-// per 4, DFT-10 124 per 10; FMA = 2), excluding the input product (6) and
-// the output power (3).
-double transform_flops_per_point(int M) {
-  double f = 1950.0 / 31.0 + 948.0 / 33.0;
-  if (M == 4) f += 4.0;
-  if (M == 10) f += 12.4;
-  return f;
-}
+// Algorithmic FLOPs reported per kernel (tga_kernel_times) and used by the
+// roofline: 5 N log2 N per complex FFT of N points, 6 per complex product,
+// 3 per |y|^2 and 10 per sample of carrier wipe-off, whatever a kernel
+// executes (the prime-factor transforms execute more per point, the
+// tensor-core stages far more).  One correlation row of P lags is a
+// product, an inverse transform and the power of every lag.
+double fft_flops(double n) { return n > 1.0 ? 5.0 * n * std::log2(n) : 0.0; }
+double corr_row_flops(int P) { return fft_flops((double)P) + 9.0 * (double)P; }
 
 const std::vector<int8_t>& cached_chips(tga_ctx* ctx, int c, int prn) {
   auto key = std::make_pair(c, prn);
@@ -524,45 +522,42 @@ void enqueue_group(tga_ctx* ctx, const ClassGroup& grp, const GroupBufs& b, cons
   dims.n_prn = n_prn;
   dims.fc = d_fc;
 
-  const double tf = transform_flops_per_point(pc.M);
+  const double row = corr_row_flops(pc.P);
   const std::string cls = "[Lc=" + std::to_string(pc.Lc) + "]";
-  timed(ctx, ("code_spectra" + cls).c_str(), (double)n_prn * 2 * pc.Lc * tf,
+  timed(ctx, ("code_spectra" + cls).c_str(), (double)n_prn * 2 * fft_flops(pc.Lc),
         [&] { return launch_code_spectra(pc, b.chips, n_prn, b.D, ctx->num_sms, st); });
-  timed(ctx, ("frontend" + cls).c_str(), (double)n_ab * 2 * pc.P * pc.S * 4.0,
+  timed(ctx, ("frontend" + cls).c_str(), (double)n_ab * 10.0 * pc.P,
         [&] { return launch_frontend(src, dims, pc, b.z, st); });
   if (ctx->precision == TGA_PRECISION_FP16_TC) {
     // the forward transform also writes Z's FP16 operands; the code spectra
     // are packed apart
-    timed(ctx, ("forward_z" + cls).c_str(), (double)n_ab * 2 * pc.P * tf, [&] {
+    timed(ctx, ("forward_z" + cls).c_str(), (double)n_ab * 2 * fft_flops(pc.P), [&] {
       return launch_forward_z_tc(pc, n_ab, b.z, b.z16, b.zmap, tc_z_scale(pc), ctx->num_sms, st);
     });
     timed(ctx, ("tc_pack" + cls).c_str(), 0.0,
           [&] { return launch_tc_pack(pc, b.D, (long long)n_prn * 2, true, b.d16, ctx->num_sms, st); });
     CK(cudaMemsetAsync(b.err, 0, sizeof(int), st));
     CK(cudaMemsetAsync(b.keys, 0, (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long), st));
-    // tensor-core FLOPs of the three DFT stages as dense real GEMMs
-    timed(ctx, ("correlate_tc" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * tc_gemm_flops_per_point(pc.M),
-          [&] {
-            return launch_correlate_tc(pc, dims, b.bmat, b.z16, b.d16, b.keys, b.err, ctx->test_flags, ctx->num_sms,
-                                       st);
-          });
+    timed(ctx, ("correlate_tc" + cls).c_str(), (double)n_ab * 2 * n_prn * row, [&] {
+      return launch_correlate_tc(pc, dims, b.bmat, b.z16, b.d16, b.keys, b.err, ctx->test_flags, ctx->num_sms, st);
+    });
     ctx->tc_err_pending = b.err;
   } else {
-    timed(ctx, ("forward_z" + cls).c_str(), (double)n_ab * 2 * pc.P * tf,
+    timed(ctx, ("forward_z" + cls).c_str(), (double)n_ab * 2 * fft_flops(pc.P),
           [&] { return launch_forward_z(pc, n_ab, b.z, ctx->num_sms, st); });
-    timed(ctx, ("correlate" + cls).c_str(), (double)n_ab * 2 * n_prn * pc.P * (tf + 9.0),
+    timed(ctx, ("correlate" + cls).c_str(), (double)n_ab * 2 * n_prn * row,
           [&] { return launch_correlate(pc, dims, b.z, b.D, b.keys, ctx->num_sms, st); });
   }
   timed(ctx, ("reduce_bins" + cls).c_str(), 0.0, [&] { return launch_reduce_bins(dims, b.keys, b.best, st); });
   if (ctx->precision == TGA_PRECISION_FP16_TC) {
     // the FP32 re-evaluation keeps the selected rows, and the second peak is
     // read from them instead of transforming the rows again
-    timed(ctx, ("refine" + cls).c_str(), (double)n_ant * n_prn * pc.P * (tf + 9.0),
+    timed(ctx, ("refine" + cls).c_str(), (double)n_ant * n_prn * row,
           [&] { return launch_refine(pc, dims, b.z, b.D, b.best, b.rows, ctx->num_sms, st); });
     timed(ctx, ("second_scan" + cls).c_str(), 0.0,
           [&] { return launch_second_scan(pc, dims, b.rows, b.best, chip_width, ctx->num_sms, st); });
   } else {
-    timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * pc.P * (tf + 9.0),
+    timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * row,
           [&] { return launch_second_peak(pc, dims, b.z, b.D, b.best, chip_width, ctx->num_sms, st); });
   }
   timed(ctx, ("finalize" + cls).c_str(), 0.0,
@@ -1853,10 +1848,10 @@ int tga_search_noncoherent(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant_tot
     unsigned long long* d_keys =
         (unsigned long long*)ctx->buf("nc.keys", (size_t)n_ant * nb * n_prn * sizeof(unsigned long long));
     BestRow* d_best = (BestRow*)ctx->buf("nc.best", (size_t)n_ant * n_prn * sizeof(BestRow));
-    const double tf = transform_flops_per_point(pc.M);
-    timed(ctx, "nc_code_spectra", (double)n_prn * 2 * pc.Lc * tf,
+    const double row = corr_row_flops(pc.P);
+    timed(ctx, "nc_code_spectra", (double)n_prn * 2 * fft_flops(pc.Lc),
           [&] { return launch_code_spectra(pc, d_chips, n_prn, d_D, ctx->num_sms, st); });
-    timed(ctx, "nc_frontend", 0.0,
+    timed(ctx, "nc_frontend", (double)n_ant * nb * B * 10.0 * pc.P * opt->coherent_periods,
           [&] { return launch_nc_frontend(src, dims, pc, opt->coherent_periods, B, opt->start, d_z, st); });
     // the tensor-core path covers Lc = 1023 (GPS, SBAS, QZSS C/A); other code
     // lengths run the FP32 search whatever the precision
@@ -1864,7 +1859,7 @@ int tga_search_noncoherent(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant_tot
     void* d_z16 = tc ? ctx->buf("nc.z16", tc_operand_bytes(pc, n_seq, false)) : nullptr;
     void* d_zmap = tc ? tc_unit_map_buf(ctx, pc.M) : nullptr;
     // in tensor-core mode the forward transform also writes Z's FP16 operands
-    timed(ctx, "nc_forward_z", (double)n_seq * pc.Lc * tf, [&] {
+    timed(ctx, "nc_forward_z", (double)n_ant * nb * B * fft_flops(pc.P), [&] {
       return tc ? launch_forward_seqs_tc(pc, n_seq, d_z, d_z16, d_zmap, tc_z_scale(pc), ctx->num_sms, st)
                 : launch_forward_seqs(pc, n_seq, d_z, ctx->num_sms, st);
     });
@@ -1885,20 +1880,20 @@ int tga_search_noncoherent(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant_tot
             [&] { return launch_tc_pack(pc, d_D, (long long)n_prn * 2, true, d_d16, ctx->num_sms, st); });
       CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
       CK(cudaMemsetAsync(d_keys, 0, (size_t)n_ant * nb * n_prn * sizeof(unsigned long long), st));
-      timed(ctx, "nc_correlate_tc", (double)n_ant * nb * n_prn * B * pc.P * tc_gemm_flops_per_point(pc.M), [&] {
+      timed(ctx, "nc_correlate_tc", (double)n_ant * nb * n_prn * B * row, [&] {
         return launch_correlate_tc_nc(pc, dims, B, d_bmat, d_z16, d_d16, d_keys, d_err, ctx->test_flags,
                                       ctx->num_sms, st);
       });
       ctx->tc_err_pending = d_err;
     } else {
-      timed(ctx, "nc_correlate", (double)n_ant * nb * n_prn * B * pc.P * (tf + 9.0),
+      timed(ctx, "nc_correlate", (double)n_ant * nb * n_prn * B * row,
             [&] { return launch_nc_correlate(pc, dims, B, d_z, d_D, d_keys, ctx->num_sms, st); });
     }
     timed(ctx, "nc_reduce", 0.0, [&] { return launch_nc_reduce(dims, d_keys, d_best, st); });
     if (tc)
-      timed(ctx, "nc_refine", (double)n_ant * n_prn * B * pc.P * (tf + 9.0),
+      timed(ctx, "nc_refine", (double)n_ant * n_prn * B * row,
             [&] { return launch_nc_refine(pc, dims, B, d_z, d_D, d_best, ctx->num_sms, st); });
-    timed(ctx, "nc_second", (double)n_ant * n_prn * B * pc.P * (tf + 9.0), [&] {
+    timed(ctx, "nc_second", (double)n_ant * n_prn * B * row, [&] {
       return launch_nc_second(pc, dims, B, d_z, d_D, d_best, chip_width_of(fs), ctx->num_sms, st);
     });
     std::vector<BestRow> best((size_t)n_ant * n_prn);
