@@ -279,6 +279,54 @@ def fp64_peak_errors(bits, runs, threads):
 TC_MMA_FLOPS_PER_POINT = {1023: 8 * (31 + 33), 4092: 8 * (31 + 12 + 11), 10230: 8 * (31 + 30 + 11)}
 
 
+# index of a constellation's PRN inside its code-length group's row-peak
+# array (the group's constellations in mask order)
+GROUP_OF = {0: (1023, 0, 1), 3: (1023, 38, 120), 5: (1023, 77, 184), 1: (4092, 0, 1), 2: (10230, 0, 1),
+            4: (10230, 63, 1)}
+
+
+def fp64_key_errors(bits, tc_rows, threads):
+    """Error of the tensor-core search's FP16 row keys against the oracle in
+    float64 on the bounded sample (antenna 0, the PRNs of the CPU baseline
+    sample, all 41 bins x 2 hypotheses): per constellation, the largest
+    |FP16 row peak - FP64 row peak| relative to the largest FP64 row peak of
+    the (antenna, PRN) (the normalisation of the library's candidate bound,
+    2^-6), and the largest relative error of the best row's peak.
+    tc_rows: {chips: array [n_ant, 82, n_prn]} from Context.row_peaks."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import acq_oracle as O
+    import concurrent.futures as cf
+    names = {O.GPS: "GPS L1 C/A", O.SBAS: "SBAS", O.QZSS: "QZSS", O.GALILEO: "Galileo E1-C",
+             O.BEIDOU: "BeiDou B1C", O.L1C: "GPS L1C"}
+    sample = {O.GPS: [1, 2, 3, 4], O.SBAS: [120, 121], O.QZSS: [184], O.GALILEO: [1, 2], O.BEIDOU: [1, 2],
+              O.L1C: [1, 2]}
+    ub = np.unpackbits(bits[:1], axis=1)[0]
+    fc = O.freq_grid(4.092e6, 6000.0)
+    out = {}
+    for c, prns in sample.items():
+        P = O.period_samples(c, FS)
+        sig, pp = O.antenna_prep(ub, 2 * P, FS)
+        chips, off, first = GROUP_OF[c]
+        worst_rows, worst_best = 0.0, 0.0
+        for prn in prns:
+            code = O.resampled_code(c, prn, float(P), 2 * P)
+            cc, ca = O.code_spectra(code, P, "f64")
+
+            def rowmax(f):
+                r = O._bin_work(sig, pp, f, cc, ca, np.float64, np.complex128)
+                m = [0.0, 0.0]
+                m[r[3]], m[1 - r[3]] = float(r[2].max()), float(r[4].max())
+                return m
+            with cf.ThreadPoolExecutor(threads) as ex:
+                ref = np.array(list(ex.map(rowmax, fc))).reshape(-1)  # [bin * 2 + hyp]
+            got = tc_rows[chips][0, :, off + prn - first]
+            worst_rows = max(worst_rows, float(np.abs(got - ref).max() / ref.max()))
+            b = int(np.argmax(ref))
+            worst_best = max(worst_best, abs(got[b] - ref[b]) / ref[b])
+        out[names[c]] = {"max_row_error_of_row_max": worst_rows, "max_rel_error_best_row": worst_best}
+    return out
+
+
 def fp32_peak_tflops(sm_mhz, n_sm=148):
     return n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
 
@@ -302,6 +350,99 @@ def run_reference(args, rank, world):
                              "sample": "bounded sample of the workload: " + desc},
             "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# The --all search non-coherently over the whole 100 ms: one code period per
+# coherent block and bins of 1 / (2 T) per code length over +-5 kHz
+CONFIG2 = [  # (constellation, PRN range, blocks, bins, bin step Hz)
+    (0, (1, 38), 100, 21, 500.0), (3, (120, 158), 100, 21, 500.0), (5, (184, 206), 100, 21, 500.0),
+    (1, (1, 50), 25, 81, 125.0), (2, (1, 63), 10, 201, 50.0), (4, (1, 63), 10, 201, 50.0)]
+
+
+def run_config2(ctx, bits, sats, args, world, stream, flush, kernel_times, prec_id):
+    """Every constellation of the --all search over the full 100 ms of the
+    benchmark recording, non-coherently: coherent blocks of one code period
+    (1 / 4 / 10 ms), |y|^2 summed over the 100 / 25 / 10 blocks, Doppler
+    +-5 kHz in 500 / 125 / 50 Hz bins, 24 antennas.  Both arithmetics end to
+    end through tga_search_noncoherent_multi from pinned host bits (GPS /
+    SBAS / QZSS and BeiDou / L1C share their front ends); cell-blocks count
+    (antenna, PRN, bin, lag, block).  Detection against the injected
+    satellites: summed peak > 1.5 x second peak, code phase within one
+    sample, frequency within one bin."""
+    import torch
+    import tga
+    if world > 1:
+        import torch.distributed as dist
+    searches = [dict(constellation=c, prns=list(range(lo, hi + 1)), center_freq=4.092e6, bin_step_hz=step,
+                     n_bins=nb, coherent_periods=1, blocks=B) for c, (lo, hi), B, nb, step in CONFIG2]
+    n_ant = bits.shape[0]
+    period = {0: 16368, 3: 16368, 5: 16368, 1: 65472, 2: 163680, 4: 163680}
+    cells = float(sum(n_ant * (hi - lo + 1) * nb * period[c] * B for c, (lo, hi), B, nb, _ in CONFIG2))
+    host = torch.from_numpy(bits).pin_memory().numpy()
+    steps, warm = min(args.steps, 3), min(args.warmup, 1)
+    runs = {}
+    for prec in ("fp16tc", "fp32"):
+        ctx.set_precision(prec_id[prec])
+        for _ in range(warm):
+            out = ctx.search_noncoherent_multi(host, FS, searches)
+        if world > 1:
+            dist.barrier()
+        times = []
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = ctx.search_noncoherent_multi(host, FS, searches)
+            times.append(time.perf_counter() - t0)
+        t = statistics.mean(times)
+        if world > 1:
+            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        refined = sum(ctx.row_peaks(lc)[1] for lc in (1023, 4092, 10230)) if prec == "fp16tc" else 0
+        # one more, untimed call with per-kernel events for the breakdown
+        tga.lib().tga_set_profiling(ctx._h, 1)
+        ctx.search_noncoherent_multi(host, FS, searches)
+        kt = {k: round(v[0], 3) for k, v in kernel_times().items()}
+        tga.lib().tga_set_profiling(ctx._h, 0)
+        runs[prec] = (t, out, kt, refined)
+    truth = {}
+    for sv in sats:
+        truth[(sv["c"], sv["prn"])] = sv
+
+    def detect(outs):
+        det_all, stats = [], {}
+        for (c, (lo, hi), B, nb, step), o in zip(CONFIG2, outs):
+            P = period[c]
+            det = o["power"] > 1.5 * o["second_power"]
+            present = np.array([(c, int(x["prn"])) in truth for x in o])
+            hit = np.zeros(len(o), bool)
+            for i, x in enumerate(o):
+                sv = truth.get((c, int(x["prn"])))
+                if sv is not None:
+                    d = abs(int(x["best_codephase"]) - (P - sv["delay"]) % P)
+                    hit[i] = min(d, P - d) <= 1 and abs(x["frequency"] - sv["dop"]) <= step
+            stats[tga.NAMES[c]] = {"p_detect": float(np.mean(det[present] & hit[present])),
+                                   "p_false_alarm": float(np.mean(det[~present])) if (~present).any() else None}
+            det_all.append(det)
+        return det_all, stats
+    fields = ("best_freq_idx", "best_codephase", "power", "second_power")
+    identical = all(np.array_equal(a[k], b[k]) for a, b in zip(runs["fp16tc"][1], runs["fp32"][1]) for k in fields)
+    _, st16 = detect(runs["fp16tc"][1])
+    _, st32 = detect(runs["fp32"][1])
+    t16, t32 = runs["fp16tc"][0], runs["fp32"][0]
+    return {"workload": "--all x %d ant, 100 ms, non-coherent: one code period per coherent block (GPS/SBAS/QZSS "
+                        "1 ms x 100, Galileo 4 ms x 25, BeiDou/L1C 10 ms x 10), Doppler +-5 kHz in 500 / 125 / 50 Hz "
+                        "bins (1 / 2T), 276 PRNs; the benchmark recording (10 satellites per constellation, "
+                        "38-50 dB-Hz, random sign per code epoch); tga_search_noncoherent_multi from pinned host "
+                        "bits (end to end)" % n_ant,
+            "unit": "cell-blocks/s", "cells_per_step_per_gpu": cells, "steps": steps, "warmup": warm,
+            "fp16tc": {"value": cells * world / t16, "ms_per_step": t16 * 1e3, "kernels_ms": runs["fp16tc"][2],
+                       "rows_reevaluated_fp32": runs["fp16tc"][3], "detection": st16},
+            "fp32": {"value": cells * world / t32, "ms_per_step": t32 * 1e3, "kernels_ms": runs["fp32"][2],
+                     "detection": st32},
+            "speedup_fp16tc_over_fp32": t32 / t16, "identical_cells": bool(identical)}
 
 
 def load_peaks():
@@ -342,6 +483,8 @@ def main():
     ap.add_argument("--no-weak", action="store_true",
                     help="skip the weak-signal non-coherent search (10 ms coherent x 10, 201 x 50 Hz bins)")
     ap.add_argument("--no-fine", action="store_true", help="skip the fine-acquisition measurement")
+    ap.add_argument("--no-config2", action="store_true",
+                    help="skip the non-coherent --all search (per-code-length bins over 100 ms)")
     ap.add_argument("--no-split", action="store_true", help="skip the --benchmark-style setup/search split")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -361,7 +504,7 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    bits_np, _ = synth_observation(SEED + rank, n_ant=args.n_ant)
+    bits_np, sats_np = synth_observation(SEED + rank, n_ant=args.n_ant)
     n_ant, row_bytes = bits_np.shape
     pinned = torch.empty((n_ant, row_bytes), dtype=torch.uint8, pin_memory=True)
     pinned.numpy()[:] = bits_np
@@ -486,6 +629,13 @@ def main():
     clk = Clocks(local)
     clk.start()
     ms_step, cells, agg, launches, out = measure(args.precision)
+    # the last timed step's row keys and, in tensor-core mode, how many rows
+    # the FP16 key bound sent to the FP32 re-evaluation
+    head_rows, refined_rows = {}, {}
+    for chips in GROUP_PRNS:
+        r, nref = ctx.row_peaks(chips)
+        head_rows[chips] = r.reshape(n_ant, 82, -1)
+        refined_rows[chips] = nref
     other = None
     if not args.no_compare:
         oprec = "fp32" if args.precision == "fp16tc" else "fp16tc"
@@ -611,6 +761,10 @@ def main():
                             "ms_per_step": w_other * 1e3, "speedup_of_weak": w_other / w_head,
                             "detection": stats_o,
                             "same_detections": bool(np.array_equal(det_h, det_o)) and same_rows}}
+    config2 = None
+    if not args.no_config2:
+        config2 = run_config2(ctx, bits_np, sats_np, args, world, stream, flush, kernel_times, prec_id)
+        ctx.set_precision(prec_id[args.precision])
     clocks = clk.stop()
     sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
     value = cells * world / (ms_step / 1e3)
@@ -661,9 +815,14 @@ def main():
         da, ka = detections(out)
         db, kb = detections(oout)
         same = bool(np.array_equal(da, db) and np.array_equal(ka[da], kb[db]))
+        # every field of every cell, detected or not
+        identical = all(np.array_equal(out[k], oout[k]) for k in
+                        ("best_codephase", "best_freq_idx", "hypothesis", "signal_strength", "second_peak",
+                         "cn0_valid", "cn0_acr"))
         ovalue = ocells * world / (oms / 1e3)
         line["compare"] = {"arithmetic": dtype[oprec], "value": ovalue, "ms_per_step": oms,
                            "speedup_of_headline": value / ovalue, "same_detections": same,
+                           "identical_cells": bool(identical),
                            "detected_cells": int(da.sum()), "cells": int(len(da)),
                            "roofline": roofline(oagg, oprec, sm_mhz), "gpu_launches": olaunch}
     if rank == 0 and world == 1 and other is not None and not args.no_cpu_baseline:
@@ -672,6 +831,18 @@ def main():
                       "oracle (reference algorithm) in float64",
             "per_constellation": fp64_peak_errors(bits_np, {dtype[args.precision]: out, dtype[other[0]]: other[5]},
                                                   os.cpu_count() or 1)}
+    if args.precision == "fp16tc":
+        line["rows_reevaluated_fp32"] = {
+            str(chips): {"rows": refined_rows[chips], "of_rows": int(head_rows[chips].size),
+                         "per_cell": refined_rows[chips] / (head_rows[chips].size / 82)} for chips in GROUP_PRNS}
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            line["fp16_key_error_vs_fp64"] = {
+                "sample": "antenna 0, PRNs GPS 1-4, SBAS 120-121, QZSS 184, Galileo 1-2, BeiDou 1-2, L1C 1-2, "
+                          "41 bins x 2 hypotheses; oracle (reference algorithm) in float64",
+                "bound": 2.0 ** -6,
+                "per_constellation": fp64_key_errors(bits_np, head_rows, os.cpu_count() or 1)}
+    if config2 is not None:
+        line["config2"] = config2
     if plain is not None:
         line["plain_gps"] = plain
     if weak is not None:

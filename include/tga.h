@@ -297,6 +297,22 @@ int tga_autotune(tga_ctx* ctx, const uint8_t* d_packed_bits, size_t n_ant, size_
  * generic path, run eagerly.  No counterpart in the reference (a CPU
  * library); it serves the batched search's launch path. */
 int tga_set_graphs(tga_ctx* ctx, int enable);
+/* Row peaks of the last search call.  After tga_acquire_all*, for its fused
+ * group of `chips`-chip codes (1023: GPS, SBAS, QZSS; 4092: Galileo; 10230:
+ * BeiDou, L1C): out[((ant * n_bins + bin) * 2 + hyp) * n_prn + i] is the
+ * largest |IFFT_2P| / sqrt(2P) of that (bin, hypothesis) row -- the
+ * reference's signal_strength units.  After tga_search_noncoherent (chips =
+ * its code length): out[(ant * n_bins + bin) * n_prn + i] is the row's
+ * largest summed power in tga_nc_cell.power units.  Values are as the
+ * search's own arithmetic computed them: the FP16 tensor-core row maxima in
+ * TGA_PRECISION_FP16_TC, FP32 otherwise.  ant and i index the call's antenna
+ * list and the group's PRNs (its constellations in mask order).  *n_out =
+ * the row count; out may be NULL to query it (TGA_ERR_CAPACITY if cap is
+ * smaller).  *n_rows_refined (may be NULL) = rows the tensor-core search
+ * re-evaluated in FP32 (0 in FP32 mode).  No counterpart in the reference;
+ * it serves the measurement of the reduced-precision keys' error. */
+int tga_last_row_peaks(tga_ctx* ctx, int chips, double* out, size_t cap, size_t* n_out,
+                       int64_t* n_rows_refined);
 /* How the last tga_acquire_all* call ran: eagerly, captured then launched,
  * or replayed from a graph captured earlier. */
 #define TGA_GRAPH_NONE 0
@@ -409,6 +425,16 @@ typedef struct tga_nc_cell {
 /* Cells in (PRN, antenna) order; cap counts cells. */
 int tga_search_noncoherent(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, size_t row_bytes, double fs,
                            const tga_nc_options* opt, tga_nc_cell* out, size_t cap, size_t* n_out);
+/* Several non-coherent searches of one recording in one call, e.g. every
+ * constellation of an --all search with its own blocks and Doppler grid:
+ * opts[i] as for tga_search_noncoherent; the cells of opts[0], then those
+ * of opts[1], ..., each in (PRN, antenna) order.  Searches with the same
+ * code length and pulse (GPS / SBAS / QZSS; BeiDou / L1C), blocks, Doppler
+ * grid and antennas share one front end and forward transform.  No
+ * counterpart in the reference (an extension, like tga_search_noncoherent). */
+int tga_search_noncoherent_multi(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, size_t row_bytes,
+                                 double fs, const tga_nc_options* opts, size_t n_opts, tga_nc_cell* out, size_t cap,
+                                 size_t* n_out);
 
 /* ---- ACR table Monte Carlo (examples/gen_acr_tables.rs) ---------------------------
  * Regenerates a C/N0 lookup table for one constellation: for every C/N0 from

@@ -269,26 +269,31 @@ template <int M, int BC, int NT, int MINB, int MODE>
 __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
   using G = Geo<M>;
   constexpr int COLS = G::COLS, LC = G::LC, NC = G::NC;
-  constexpr bool INV = (MODE == CORR || MODE == SECOND || MODE == REFINE);
-  constexpr bool ARGMAX = (MODE == CORR || MODE == REFINE);
+  constexpr bool INV = (MODE == CORR || MODE == SECOND || MODE == CAND);
+  constexpr bool ARGMAX = (MODE == CORR || MODE == CAND);
   extern __shared__ float2 buf[];
   __shared__ unsigned long long s_key;
   __shared__ unsigned int s_p2;
   const int tid = threadIdx.x;
   const int S = p.S;
   const int groups = INV ? (S + BC - 1) / BC : 1;
-  const int n_work = INV ? p.n_items : (p.n_seq + BC - 1) / BC;
+  int n_work = INV ? p.n_items : (p.n_seq + BC - 1) / BC;
+  if (MODE == CAND) n_work = min(n_work, *p.cand_count);
 
   for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
     int ab_h = 0, prn = 0, tau_star = 0;
     if (MODE == CORR) {
       ab_h = w / p.n_prn;
       prn = w - ab_h * p.n_prn;
-    } else if (MODE == SECOND || MODE == REFINE) {
+    } else if (MODE == SECOND) {
       const BestRow b = p.best[w];
       ab_h = b.ab * 2 + b.hyp;
       prn = w % p.n_prn;
       tau_star = b.tau;
+    } else if (MODE == CAND) {
+      const int2 c = p.cand[w];
+      ab_h = c.x;
+      prn = c.y;
     }
     const int hyp = ab_h & 1;
     // CORR: running maximum of |y|^2 and a compact code of its position
@@ -329,8 +334,6 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
           p.Dout[(size_t)seq_of(s) * LC + G::offset(a, b, c)] = make_float2(v.x, -v.y);
         } else {
           const float pw = fmaf(v.x, v.x, v.y * v.y);
-          if (MODE == REFINE && p.rowbuf)
-            p.rowbuf[((size_t)w * S + seq_of(s)) * LC + G::row_pos(a, b, c)] = pw;
           if (ARGMAX) {
             const int code = ((seq_of(s) * 31 + a) * 33 + b) * 16 + c;
             if (pw == pmax) {
@@ -459,14 +462,8 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
       }
       if ((tid & 31) == 0) atomicMax(&s_key, kbest);
       __syncthreads();
-      if (tid == 0) {
-        if (MODE == CORR) {
-          p.keys[w] = s_key;
-        } else {
-          p.best[w].tau = (int)(unsigned)(s_key & 0xffffffffull);
-          p.best[w].p = __uint_as_float((unsigned)(s_key >> 32));
-        }
-      }
+      // CORR's item w is the row ab_h * n_prn + prn
+      if (tid == 0) p.keys[(size_t)ab_h * p.n_prn + prn] = s_key;
     } else if (MODE == SECOND) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) pbest = fmaxf(pbest, __shfl_xor_sync(0xffffffffu, pbest, o));
@@ -534,7 +531,7 @@ static cudaError_t run_pfa(const PfaParams& p, int n_work_slots, int num_sms, cu
 template <int MODE>
 static cudaError_t dispatch_pfa(const PolyClass& pc, const PfaParams& p, int n_work_slots, int num_sms,
                                 cudaStream_t st) {
-  if constexpr (MODE == CORR || MODE == SECOND || MODE == REFINE) {
+  if constexpr (MODE == CORR || MODE == SECOND || MODE == CAND) {
     if (pc.variant == 1) {
       switch (pc.M) {
         case 1: return run_pfa<1, 1, MODE>(p, n_work_slots, num_sms, st);
@@ -659,73 +656,53 @@ cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, cons
   return dispatch_pfa<SECOND>(pc, p, p.n_items, num_sms, st);
 }
 
-cudaError_t launch_refine(const PolyClass& pc, const SearchDims& dims, const float2* d_Z, const float2* d_D,
-                          BestRow* d_best, float* d_rowbuf, int num_sms, cudaStream_t st) {
+cudaError_t launch_correlate_listed(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
+                                    const float2* d_D, const int2* d_cand, const int* d_count, int capacity,
+                                    unsigned long long* d_keys, int num_sms, cudaStream_t st) {
   PfaParams p = {};
   p.z = const_cast<float2*>(d_Z);
   p.D = d_D;
-  p.best = d_best;
-  p.rowbuf = d_rowbuf;
+  p.keys = d_keys;
+  p.cand = d_cand;
+  p.cand_count = d_count;
   p.n_prn = dims.n_prn;
   p.S = pc.S;
   p.P = pc.P;
-  p.n_items = dims.n_ant * dims.n_prn;
-  return dispatch_pfa<REFINE>(pc, p, p.n_items, num_sms, st);
+  p.n_items = capacity;
+  return dispatch_pfa<CAND>(pc, p, p.n_items, num_sms, st);
 }
 
-// Second peak from the rows REFINE left in rowbuf (correlate.rs:157-175, the
-// rule of pfa_kernel mode SECOND): the 2 cw + 1 lags within cw of the peak
-// lag are overwritten with -1, then the row maximum, at least 0.  The lags
-// near the peak are located through their CRT digits (a, b, c) =
-// (t mod 31, t mod 33, t mod M) of t = lag / S in residue lag mod S.
-template <int M>
-__global__ void __launch_bounds__(256) second_scan_kernel(float* __restrict__ rowbuf, BestRow* __restrict__ best,
-                                                          int n_items, int S, int P, int cw) {
-  using G = Geo<M>;
-  __shared__ unsigned s_max;
-  for (int w = blockIdx.x; w < n_items; w += gridDim.x) {
-    float* row = rowbuf + (size_t)w * P;
-    if (threadIdx.x == 0) s_max = 0u;
-    const int tau = best[w].tau;
-    for (int d = (int)threadIdx.x - cw; d <= cw; d += blockDim.x) {
-      int lag = (tau + d) % P;
-      if (lag < 0) lag += P;
-      const int rho = lag % S, t = lag / S;
-      row[(size_t)rho * G::LC + G::row_pos(t % 31, t % 33, M == 1 ? 0 : t % M)] = -1.f;
-    }
-    __syncthreads();
-    float m = 0.f;
-    if ((P & 3) == 0) {
-      const float4* r4 = reinterpret_cast<const float4*>(row);
-      for (int i = threadIdx.x; i < P / 4; i += blockDim.x) {
-        const float4 v = __ldcs(r4 + i);
-        m = fmaxf(m, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
-      }
-    } else {
-      for (int i = threadIdx.x; i < P; i += blockDim.x) m = fmaxf(m, __ldcs(row + i));
-    }
-    // non-negative floats order like their bit patterns
-    const unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(m));
-    if ((threadIdx.x & 31) == 0) atomicMax(&s_max, bits);
-    __syncthreads();
-    if (threadIdx.x == 0) best[w].p2 = __uint_as_float(s_max);
-    __syncthreads();
-  }
+// Rows of a reduced-precision search to re-evaluate in FP32.  Per (antenna,
+// PRN), with K the largest reduced-precision key of its 2 nb rows, every row
+// whose key is at least keep * K is listed (keep * K = 0 lists all rows).
+// If every row's amplitude error is at most e and keep = (1 - 2 e / sqrt(K))^2
+// or less, the row holding the FP32 maximum is always listed: its key is at
+// least (sqrt(V) - e)^2 with V the FP32 maximum, and sqrt(K) <= sqrt(V) + e.
+// Rows not listed hold FP32 values below V, so the FP32 keys of the listed
+// rows alone give the FP32 search's choice under the same tie rules.
+// Rows are [ant][bin][hyp] with n_hyp hypotheses (2 in the drop-in search,
+// 1 in the non-coherent one); a listed row is (its row index, prn).
+__global__ void tc_candidates_kernel(int n_ant, int n_rows, int n_prn, const unsigned long long* __restrict__ keys,
+                                     float keep, int2* __restrict__ cand, int* __restrict__ count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_ant * n_prn) return;
+  const int ant = i / n_prn, prn = i - ant * n_prn;
+  const size_t row0 = (size_t)ant * n_rows;
+  float kmax = 0.f;
+  for (int r = 0; r < n_rows; ++r)
+    kmax = fmaxf(kmax, __uint_as_float((unsigned)(keys[(row0 + r) * n_prn + prn] >> 32)));
+  const float t = kmax * keep;
+  for (int r = 0; r < n_rows; ++r)
+    if (__uint_as_float((unsigned)(keys[(row0 + r) * n_prn + prn] >> 32)) >= t)
+      cand[atomicAdd(count, 1)] = make_int2((int)(row0 + r), prn);
 }
 
-cudaError_t launch_second_scan(const PolyClass& pc, const SearchDims& dims, float* d_rowbuf, BestRow* d_best,
-                               int chip_width, int num_sms, cudaStream_t st) {
-  const int n_items = dims.n_ant * dims.n_prn;
-  if (n_items == 0) return cudaSuccess;
-  if (2 * chip_width + 1 >= pc.P) return cudaErrorInvalidValue;
-  int grid = num_sms * 8;
-  if (grid > n_items) grid = n_items;
-  switch (pc.M) {
-    case 1: second_scan_kernel<1><<<grid, 256, 0, st>>>(d_rowbuf, d_best, n_items, pc.S, pc.P, chip_width); break;
-    case 4: second_scan_kernel<4><<<grid, 256, 0, st>>>(d_rowbuf, d_best, n_items, pc.S, pc.P, chip_width); break;
-    case 10: second_scan_kernel<10><<<grid, 256, 0, st>>>(d_rowbuf, d_best, n_items, pc.S, pc.P, chip_width); break;
-    default: return cudaErrorInvalidValue;
-  }
+cudaError_t launch_tc_candidates(const SearchDims& dims, int n_hyp, const unsigned long long* d_keys, float keep,
+                                 int2* d_cand, int* d_count, cudaStream_t st) {
+  const int n = dims.n_ant * dims.n_prn;
+  if (n <= 0) return cudaSuccess;
+  tc_candidates_kernel<<<(n + 127) / 128, 128, 0, st>>>(dims.n_ant, dims.nb * n_hyp, dims.n_prn, d_keys, keep,
+                                                        d_cand, d_count);
   return TGA_LAUNCHED();
 }
 

@@ -25,9 +25,10 @@
 // |C 2^-kd| <= Lc 2^-kd stay inside FP16, every product is below 32768 and so
 // is every correlation value; stage outputs are rounded with satfinite.
 // Keys carry the row maximum of |y|^2 2^-2k (the lag bits are zero) and are
-// only compared; the selected row of every (antenna, PRN) is re-evaluated in
-// FP32 afterwards (launch_refine), so the reported peak, lag and second peak
-// are FP32 values.
+// only compared: every row of an (antenna, PRN) whose key lies within the
+// FP16 error bound of its best is re-evaluated in FP32 afterwards
+// (launch_tc_candidates, launch_correlate_listed), so the chosen row, and
+// the reported peak, lag and second peak, are those of the FP32 search.
 //
 // One CTA per SM (all 512 TMEM columns) runs two PRN chains over the Z of a
 // (row, group of BC code-phase residues) work item, so that the tensor cores
@@ -35,10 +36,12 @@
 // per chain issues its MMAs.  Every wait is bounded (1 s): on expiry the kernel sets
 // *err, drains (again bounded), frees its TMEM and returns.
 //
-// The same kernel (NCB) runs the non-coherent search at Lc = 1023: every PRN
-// pair goes through B coherent blocks, the Z of each block is loaded into the
-// registers in turn, and the |y|^2 of the blocks are summed in shared memory
-// before the row maximum.
+// The same kernel (NCB) runs the non-coherent search: every PRN pair goes
+// through B coherent blocks, the Z of each block is loaded into the registers
+// in turn, and the |y|^2 of the blocks are summed in shared memory before the
+// row maximum.  At Lc = 10230, where two chains' sums and code blocks do not
+// fit the shared memory, the two chains instead take consecutive blocks of
+// one PRN and share its code block and sums (BLKCH).
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -296,12 +299,21 @@ struct T3 {
   static constexpr int LAST_TILES = NST == 3 ? TILES3 : TILES2;
   static constexpr int LAST_ROWS = NST == 3 ? ROWS3P : ROWS2, LAST_NR = NST == 3 ? NR3 : NR2;
   static constexpr int LAST_OUT = NST == 3 ? R3 : R2;
-  // non-coherent search: per chain, |y|^2 sums over the blocks of the 33
-  // stage-2 outputs of every row, as [33][LAST_TILES * 128] floats (rows
-  // fastest: a warp's 32 lanes touch 32 banks)
-  static_assert(!NCB || (M == 1 && NST == 2 && LAST_OUT == 33), "non-coherent search: Lc = 1023");
+  // non-coherent search: |y|^2 sums over the blocks of the ACC_OUT outputs
+  // of every last-stage row (33 stage-2 outputs, or the 2 x 11 outputs of a
+  // paired stage-3 row), as [ACC_OUT][LAST_TILES * 128] floats (rows
+  // fastest: a warp's 32 lanes touch 32 banks).  The two chains run two
+  // PRNs, each with its own code block and sums, except with BLKCH (Lc =
+  // 10230, where two sets of sums and code blocks do not fit the shared
+  // memory): there the chains run consecutive blocks of one PRN and share
+  // its code block and one set of sums.
+  static constexpr bool BLKCH = NCB && M == 10;
+  static_assert(!NCB || (NST == 2 && LAST_OUT == 33) || (NST == 3 && PAIR3 && LAST_OUT == 11),
+                "non-coherent epilogue layouts");
+  static constexpr int ACC_OUT = NST == 2 ? 33 : 2 * R3;
   static constexpr int ACC_ROWS = LAST_TILES * 128;
-  static constexpr int ACC_BYTES = NCB ? (33 * ACC_ROWS * 4 + 1023) / 1024 * 1024 : 0;
+  static constexpr int ACC_BYTES = NCB ? (ACC_OUT * ACC_ROWS * 4 + 1023) / 1024 * 1024 : 0;
+  static constexpr int N_ACC = NCB ? (BLKCH ? 1 : 2) : 0, N_CODE = BLKCH ? 1 : 2;
   // data operand regions: rows padded to whole tiles, K chunks lbo apart
   static constexpr int LBO1 = TILES1 * 128 * 16 + 16, LBO2 = TILES2 * 128 * 16 + 16 * Tc3Cfg<M>::PAD2,
                        LBO3 = TILES3 * 128 * 16 + 16 * Tc3Cfg<M>::PAD3;
@@ -316,7 +328,8 @@ struct T3 {
   static constexpr int UNITS = NR1 * 8;
   static constexpr int U = (UNITS + kSimtThreads - 1) / kSimtThreads;
   static_assert(8 * ROWS1 < 65536 && 8 * LBO1 < 65536, "packed unit offsets");
-  static constexpr int SMEM_RAW = 2 * A_BYTES + B1_BYTES + B2_BYTES + B3_BYTES + 2 * CODE_REGION + 2 * ACC_BYTES + 1024;
+  static constexpr int SMEM_RAW =
+      2 * A_BYTES + B1_BYTES + B2_BYTES + B3_BYTES + N_CODE * CODE_REGION + N_ACC * ACC_BYTES + 1024;
   // more than half of the SM's shared memory: one CTA, and so one 512-column
   // TMEM allocation, per SM
   static constexpr int SMEM = SMEM_RAW > 120 * 1024 ? SMEM_RAW : 120 * 1024;
@@ -480,11 +493,14 @@ __device__ __forceinline__ void tmem_ld_stage3(uint32_t taddr, int half, uint32_
 // thread until the tensor cores take it, so issuing has warps of its own,
 // one per chain.  Every wait is bounded.
 //
-// NCB (non-coherent search, Lc = 1023): the row is an (antenna, bin) and
-// every PRN pair runs through B coherent blocks; each thread keeps the |y|^2
-// sums of its epilogue outputs in shared memory and takes the row maximum
-// after the last block.  The Z of the next block is loaded into the
-// registers while the current block's transform runs.
+// NCB (non-coherent search): the row is an (antenna, bin) and every PRN pair
+// runs through B coherent blocks; each thread keeps the |y|^2 sums of its
+// epilogue outputs in shared memory and takes the row maximum after the last
+// block.  The Z of the next block is loaded into the registers while the
+// current block's transform runs.  BLKCH (Lc = 10230): a round is one PRN,
+// whose blocks 2 i and 2 i + 1 run on chains a and b; one code block and one
+// set of sums serve both chains, and chain b's Z is loaded after chain a has
+// formed its products.
 // The code warp's thread: after the 12 SIMT warps have formed chain x's
 // products of a PRN's last block (s_p1[x]), bulk-copy the chain's next code
 // block into its slot (s_code[x]).  Its own function, so that its registers
@@ -492,44 +508,62 @@ __device__ __forceinline__ void tmem_ld_stage3(uint32_t taddr, int half, uint32_
 template <class T, bool NCB>
 __device__ __noinline__ void code_warp(const Tc3Params& p, uint64_t* s_p1, uint64_t* s_code, unsigned char* CODE0,
                                        int n_rounds) {
-  auto prn_of = [&](int r, int x) -> int { return 2 * r + x < p.n_prn ? 2 * r + x : p.n_prn - 1; };
+  // the PRN of chain x in round r: PRN pairs, or with BLKCH one PRN per round
+  auto prn_of = [&](int r, int x) -> int {
+    if (T::BLKCH) return r;
+    return 2 * r + x < p.n_prn ? 2 * r + x : p.n_prn - 1;
+  };
   uint32_t ph_p1[2] = {0u, 0u};
   int fetches[2] = {0, 0};
   bool ok = true;
-  // code block of chain x for round r of work item w
-  auto fetch = [&](int x, int w, int r) {
+  // code block of chain x for round r of work item w, into slot `slot`
+  auto fetch = [&](int slot, int x, int w, int r) {
     const int hyp = NCB ? 0 : (w / p.groups) & 1;
     const uint4* src = p.d16 + ((size_t)prn_of(r, x) * 2 + hyp) * 8 * T::ROWS1;
-    mbar_arrive_expect_tx(&s_code[x], (uint32_t)T::CODE_BYTES);
-    bulk_g2s(smem_addr(CODE0 + x * T::CODE_REGION), src, (uint32_t)T::CODE_BYTES, &s_code[x]);
-    ++fetches[x];
+    mbar_arrive_expect_tx(&s_code[slot], (uint32_t)T::CODE_BYTES);
+    bulk_g2s(smem_addr(CODE0 + slot * T::CODE_REGION), src, (uint32_t)T::CODE_BYTES, &s_code[slot]);
+    ++fetches[slot];
   };
   const int split = NCB ? p.split : 1;  // the drop-in search always has enough items
   const int n_units = p.n_items * split;
-  if ((int)blockIdx.x < n_units && n_rounds > 0) {
-    fetch(0, blockIdx.x / split, unit_round0(split, blockIdx.x, n_rounds));
-    fetch(1, blockIdx.x / split, unit_round0(split, blockIdx.x, n_rounds));
-  }
+  constexpr int NSLOT = T::BLKCH ? 1 : 2;
+  if ((int)blockIdx.x < n_units && n_rounds > 0)
+    for (int x = 0; x < NSLOT; ++x) fetch(x, x, blockIdx.x / split, unit_round0(split, blockIdx.x, n_rounds));
 #pragma unroll 1
   for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
     const int w = u / split, r1 = unit_round1(split, u, n_rounds), un = u + (int)gridDim.x;
 #pragma unroll 1
-    for (int r = unit_round0(split, u, n_rounds); r < r1 && ok; ++r)
-#pragma unroll 1
-      for (int x = 0; x < 2 && ok; ++x) {
-        if (!bounded_wait(&s_p1[x], ph_p1[x])) {
-          ok = false;
-          break;
+    for (int r = unit_round0(split, u, n_rounds); r < r1 && ok; ++r) {
+      // BLKCH: the one slot is refilled once both chains have formed the
+      // products of the PRN's last blocks
+      if constexpr (T::BLKCH) {
+        for (int x = 0; x < 2 && ok; ++x) {
+          ok = bounded_wait(&s_p1[x], ph_p1[x]) != 0;
+          ph_p1[x] ^= 1u;
         }
-        ph_p1[x] ^= 1u;
+        if (!ok) break;
         if (r + 1 < r1)
-          fetch(x, w, r + 1);
+          fetch(0, 0, w, r + 1);
         else if (un < n_units)
-          fetch(x, un / split, unit_round0(split, un, n_rounds));
+          fetch(0, 0, un / split, unit_round0(split, un, n_rounds));
+      } else {
+#pragma unroll 1
+        for (int x = 0; x < 2 && ok; ++x) {
+          if (!bounded_wait(&s_p1[x], ph_p1[x])) {
+            ok = false;
+            break;
+          }
+          ph_p1[x] ^= 1u;
+          if (r + 1 < r1)
+            fetch(x, x, w, r + 1);
+          else if (un < n_units)
+            fetch(x, x, un / split, unit_round0(split, un, n_rounds));
+        }
       }
+    }
   }
-  // drain: the last bulk copy of each chain
-  for (int x = 0; x < 2; ++x)
+  // drain: the last bulk copy of each slot
+  for (int x = 0; x < NSLOT; ++x)
     if (fetches[x] > 0) bounded_wait(&s_code[x], (uint32_t)((fetches[x] - 1) & 1));
   if (!ok) atomicExch(p.err, 1);
 }
@@ -560,9 +594,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   unsigned char* B2 = B1 + T::B1_BYTES;
   unsigned char* B3 = B2 + T::B2_BYTES;
   unsigned char* CODE0 = B3 + T::B3_BYTES;
-  float* ACC = reinterpret_cast<float*>(CODE0 + 2 * T::CODE_REGION);  // [2 chains][33][ACC_ROWS] (NCB)
+  // NCB: the sums, [N_ACC][ACC_OUT][ACC_ROWS]
+  float* ACC = reinterpret_cast<float*>(CODE0 + T::N_CODE * T::CODE_REGION);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quad = warp & 3;
-  const int S = p.S, n_rounds = (p.n_prn + 1) / 2, B = NCB ? p.B : 1;
+  // rounds: PRN pairs, or with BLKCH single PRNs; steps of a round: one per
+  // coherent block, or with BLKCH one per pair of blocks (chain x takes
+  // block 2 i + x; a block index >= B, when B is odd, stands for zero data)
+  const int S = p.S, n_rounds = T::BLKCH ? p.n_prn : (p.n_prn + 1) / 2, B = NCB ? p.B : 1;
+  const int NI = T::BLKCH ? (B + 1) / 2 : B;
   const int split = NCB ? p.split : 1;  // the drop-in search always has enough items
 
   if (warp == 0) {
@@ -588,7 +627,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   tc_fence_after();
   const uint32_t tmem_base = s_tmem;
   // PRN of chain x in round r
-  auto prn_of = [&](int r, int x) -> int { return 2 * r + x < p.n_prn ? 2 * r + x : p.n_prn - 1; };
+  auto prn_of = [&](int r, int x) -> int {
+    if (T::BLKCH) return r;
+    return 2 * r + x < p.n_prn ? 2 * r + x : p.n_prn - 1;
+  };
 
   if (warp == NW || warp == NW + 1) {
     // ---------------- MMA warps: one thread each issues one chain's tensor-core work ----------------
@@ -609,7 +651,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
         const int r1 = unit_round1(split, u, n_rounds);
         for (int r = unit_round0(split, u, n_rounds); r < r1 && ok; ++r) {
 #pragma unroll 1
-         for (int b = 0; b < B && ok; ++b) {
+         for (int b = 0; b < NI && ok; ++b) {
 #pragma unroll 1
           for (int st = 0; st < T::NST && ok; ++st) {
             {
@@ -843,10 +885,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       run_chunks(std::integral_constant<int, NQ>(), load, store);
     };
     // ---- P4: |y|^2 maximum over the stage-3 outputs of chain x ----
-    // Only the row maximum is kept: the bin / hypothesis reduction compares
-    // powers alone, and the selected row of every (antenna, PRN) is searched
-    // again in FP32 (launch_refine), which finds its lag with the
-    // reference's tie rule.  Padding rows and residues >= S are skipped.
+    // Only the row maximum is kept: rows near the best of their (antenna,
+    // PRN) are searched again in FP32 (launch_correlate_listed), which finds
+    // the lag with the reference's tie rule.  Padding rows and residues >= S are skipped.
     auto p4 = [&](int x, int g) -> float {
       const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
       // accumulator words read per task: 24 for a stage-3 transform (22 used)
@@ -952,59 +993,79 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       }
     };
 
-    // ---- P4 of the non-coherent search: add block b's |y|^2 to the chain's
-    // sums in shared memory; after the last block, the row maximum of the
-    // sums ----  Tasks are (stage-2 tile, lane quadrant, outputs
-    // [11 c, 11 c + 11)), task = warp + i NW.
-    auto p4_nc = [&](int x, int g, int b) -> float {
-      constexpr int NTN = T::LAST_TILES * 4 * 3, TPWN = (NTN + NW - 1) / NW;
+    // ---- P4 of the non-coherent search: add the block's |y|^2 to the
+    // chain's sums in shared memory (first: the sums start at it); after the
+    // last block (last), the row maximum of the sums ----
+    // Two-stage split: tasks are (stage-2 tile, lane quadrant, outputs
+    // [11 c, 11 c + 11)).  Three-stage paired split: tasks are (stage-3
+    // tile, lane quadrant, half h: the 11 outputs of accumulator columns
+    // [24 h, 24 h + 22)).  task = warp + i NW keeps the warp's quadrant.
+    auto p4_nc = [&](int x, int g, bool first, bool last) -> float {
       const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
-      float* acc = ACC + (size_t)x * (T::ACC_BYTES / 4);
+      float* acc = ACC + (size_t)(T::BLKCH ? 0 : x) * (T::ACC_BYTES / 4);
       float best = 0.f;
-#pragma unroll
-      for (int i = 0; i < TPWN; ++i) {
-        const int task = warp + i * NW;
-        if (task >= NTN) break;
-        const int t = task / 12, c = (task >> 2) % 3;
-        const int s0 = c == 0 ? 0 : (c == 1 ? 16 : 40);  // 8-column aligned start covering [22 c, 22 c + 22)
-        uint32_t v[32];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          uint32_t(&q)[8] = *reinterpret_cast<uint32_t(*)[8]>(&v[8 * k]);
-          tmem_ld8(tb + (uint32_t)(t * T::N2 + s0 + 8 * k), q);
-        }
-        tmem_wait_ld();
-        const int r = t * 128 + quad * 32 + lane;
-        const bool valid = r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S;
-        float* a = acc + (size_t)(11 * c) * T::ACC_ROWS + r;
-        // all loads of the sums first, then the arithmetic, then the
-        // stores: one shared-memory latency per task instead of one per
-        // output (the compiler kept each load behind the previous store)
+      // adds the powers of 11 complex outputs (words v[o + 2 h], v[o + 2 h + 1])
+      // to the 11 sums a[h ACC_ROWS]: all loads of the sums first, then the
+      // arithmetic, then the stores -- one shared-memory latency per task
+      // instead of one per output (the compiler kept each load behind the
+      // previous store)
+      auto add11 = [&](const uint32_t* v, float* a, bool valid) {
         float sum[11];
 #pragma unroll
-        for (int h = 0; h < 11; ++h) sum[h] = b > 0 ? a[h * T::ACC_ROWS] : 0.f;
-        // the chunk starts 22 c - s0 = 0, 6 or 4 words into v (c is
-        // uniform over the warp; constant indices keep v in registers)
-        auto add = [&](auto o) {
+        for (int h = 0; h < 11; ++h) sum[h] = first ? 0.f : a[h * T::ACC_ROWS];
 #pragma unroll
-          for (int h = 0; h < 11; ++h) {
-            const float re = __uint_as_float(v[decltype(o)::value + 2 * h]);
-            const float im = __uint_as_float(v[decltype(o)::value + 2 * h + 1]);
-            sum[h] = fmaf(re, re, im * im) + sum[h];
-          }
-        };
-        if (c == 0)
-          add(std::integral_constant<int, 0>());
-        else if (c == 1)
-          add(std::integral_constant<int, 6>());
-        else
-          add(std::integral_constant<int, 4>());
-        if (b + 1 < B) {
+        for (int h = 0; h < 11; ++h) {
+          const float re = __uint_as_float(v[2 * h]), im = __uint_as_float(v[2 * h + 1]);
+          sum[h] = fmaf(re, re, im * im) + sum[h];
+        }
+        if (!last) {
 #pragma unroll
           for (int h = 0; h < 11; ++h) a[h * T::ACC_ROWS] = sum[h];
         } else if (valid) {
 #pragma unroll
           for (int h = 0; h < 11; ++h) best = fmaxf(best, sum[h]);
+        }
+      };
+      if constexpr (T::NST == 2) {
+        constexpr int NTN = T::LAST_TILES * 4 * 3, TPWN = (NTN + NW - 1) / NW;
+#pragma unroll
+        for (int i = 0; i < TPWN; ++i) {
+          const int task = warp + i * NW;
+          if (task >= NTN) break;
+          const int t = task / 12, c = (task >> 2) % 3;
+          const int s0 = c == 0 ? 0 : (c == 1 ? 16 : 40);  // 8-column aligned start covering [22 c, 22 c + 22)
+          uint32_t v[32];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            uint32_t(&q)[8] = *reinterpret_cast<uint32_t(*)[8]>(&v[8 * k]);
+            tmem_ld8(tb + (uint32_t)(t * T::N2 + s0 + 8 * k), q);
+          }
+          tmem_wait_ld();
+          const int r = t * 128 + quad * 32 + lane;
+          const bool valid = r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S;
+          float* a = acc + (size_t)(11 * c) * T::ACC_ROWS + r;
+          // the chunk starts 22 c - s0 = 0, 6 or 4 words into v (c is
+          // uniform over the warp; constant offsets keep v in registers)
+          if (c == 0)
+            add11(v, a, valid);
+          else if (c == 1)
+            add11(v + 6, a, valid);
+          else
+            add11(v + 4, a, valid);
+        }
+      } else {
+        constexpr int NTN = T::LAST_TILES * 4 * 2, TPWN = (NTN + NW - 1) / NW;
+#pragma unroll
+        for (int i = 0; i < TPWN; ++i) {
+          const int task = warp + i * NW;
+          if (task >= NTN) break;
+          const int t = task / 8, half = (task >> 2) & 1;
+          uint32_t v[24];
+          tmem_ld_stage3<T::PAIR3>(tb + (uint32_t)(t * T::N3), half, v);
+          tmem_wait_ld();
+          const int r = t * 128 + quad * 32 + lane;
+          const bool valid = r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S;
+          add11(v, acc + (size_t)(11 * half) * T::ACC_ROWS + r, valid);
         }
       }
       return best;
@@ -1026,26 +1087,29 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
             const int rho = g * BC + s;
             // the drop-in search reads its Z once (evict first); the
             // non-coherent search reads each block again for every PRN
-            // pair, so it keeps the blocks in L2
-            if (rho < S) {
+            // (pair), so it keeps the blocks in L2.  blk >= B (BLKCH, B
+            // odd) stands for zero data, which adds nothing to the sums.
+            if (rho < S && blk < B) {
               const uint4* src = p.z16 + ((((size_t)ab_h * B + blk) * S + rho) * 8 + j) * T::ROWS1 + u;
               zr[k] = NCB ? __ldcg(src) : __ldcs(src);
             }
           }
         }
       };
-      load_z(0);
+      // the code slot of chain x (BLKCH: one slot for both)
+      auto slot = [](int x) -> int { return T::BLKCH ? 0 : x; };
       // chain x: wait for its code block when a new PRN starts (the blocks of
       // one PRN share it), form the products, hand over
       // code_ready: this lane's earlier test of the block (issued before the
       // epilogue, so its latency overlaps that work); the warp waits only if
       // a lane saw it incomplete
       auto products = [&](int x, bool new_code, uint32_t code_ready = 0u) -> bool {
+        const int c = slot(x);
         if (new_code) {
-          if (!__all_sync(0xffffffffu, code_ready) && !warp_wait(&s_code[x], ph_code[x])) return false;
-          ph_code[x] ^= 1u;
+          if (!__all_sync(0xffffffffu, code_ready) && !warp_wait(&s_code[c], ph_code[c])) return false;
+          ph_code[c] ^= 1u;
         }
-        p1(zr, A0 + x * T::A_BYTES, CODE0 + x * T::CODE_REGION);
+        p1(zr, A0 + x * T::A_BYTES, CODE0 + c * T::CODE_REGION);
         signal(x);
         return true;
       };
@@ -1054,16 +1118,33 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       auto released = [&](int x) {
         if (lane == 0) mbar_arrive(&s_p1[x]);
       };
-      for (int x = 0; x < 2 && !failed; ++x) {
-        failed = !products(x, true);
-        if (!failed && B == 1) released(x);
+      // the first step of the unit's first round
+      if (T::BLKCH) {
+        load_z(0);
+        failed = !products(0, true);
+        if (!failed) {
+          load_z(1);
+          failed = !products(1, false);
+        }
+        if (!failed && NI == 1) {
+          released(0);
+          released(1);
+        }
+      } else {
+        load_z(0);
+        for (int x = 0; x < 2 && !failed; ++x) {
+          failed = !products(x, true);
+          if (!failed && NI == 1) released(x);
+        }
       }
       for (int r = r0; r < r1 && !failed; ++r)
-       for (int b = 0; b < B && !failed; ++b) {
-        const bool more = b + 1 < B || r + 1 < r1;  // a next block of this unit follows
-        // both chains have formed this block's products: bring the next
-        // block's Z into the registers while the transforms run
-        if (NCB && more) load_z(b + 1 < B ? b + 1 : 0);
+       for (int b = 0; b < NI && !failed; ++b) {
+        const bool more = b + 1 < NI || r + 1 < r1;  // a next step of this unit follows
+        const int bn = b + 1 < NI ? b + 1 : 0;        // its index
+        // both chains have formed this step's products: bring the next
+        // step's Z (BLKCH: that of chain a's next block) into the registers
+        // while the transforms run
+        if (NCB && more) load_z(T::BLKCH ? 2 * bn : bn);
         // P2, P3 for chain a then chain b, each after its own MMA stage
 #pragma unroll 1
         for (int st = 0; st < T::NST - 1 && !failed; ++st) {
@@ -1082,8 +1163,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
             signal(x);
           }
         }
-        // P4 of this round, then at once the products of the chain's next
-        // round, so that the tensor cores are not left idle across rounds
+        // P4 of this step, then at once the products of the chain's next
+        // step, so that the tensor cores are not left idle across rounds
 #pragma unroll 1
         for (int x = 0; x < 2 && !failed; ++x) {
           if (!warp_wait(&s_done[x], ph_done[x])) {
@@ -1092,22 +1173,33 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
           }
           ph_done[x] ^= 1u;
           tc_fence_after();
-          // test the chain's next code block now, use the answer after P4
-          const uint32_t code_ready = (more && b + 1 == B) ? mbar_try_wait(&s_code[x], ph_code[x]) : 0u;
+          // a new PRN starts with the next step (BLKCH: chain a waits for
+          // the shared slot, chain b follows it); test its code block now,
+          // use the answer after P4
+          const bool new_code = more && b + 1 == NI && (!T::BLKCH || x == 0);
+          const uint32_t code_ready = new_code ? mbar_try_wait(&s_code[slot(x)], ph_code[slot(x)]) : 0u;
           // non-negative floats order like their bit patterns
           float pmax;
-          if constexpr (NCB)
-            pmax = p4_nc(x, g, b);
-          else
+          if constexpr (NCB) {
+            // BLKCH: chain a's block 0 starts the sums, chain b's last block
+            // ends them
+            const bool first = T::BLKCH ? (b == 0 && x == 0) : b == 0;
+            const bool last = T::BLKCH ? (b + 1 == NI && x == 1) : b + 1 == NI;
+            pmax = p4_nc(x, g, first, last);
+          } else {
             pmax = p4(x, g);
+          }
           const unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(pmax));
           if (lane == 0 && bits != 0u)
             atomicMax(p.keys + (size_t)ab_h * p.n_prn + prn_of(r, x), (unsigned long long)bits << 32);
-          // the next products are those of block b + 1, or of the next
-          // round's block 0
+          // the next products are those of step b + 1, or of the next
+          // round's step 0
           if (more) {
-            failed = !products(x, b + 1 == B, code_ready);
-            if (!failed && (NCB ? (b + 1 < B ? b + 1 : 0) == B - 1 : true)) released(x);
+            failed = !products(x, new_code, code_ready);
+            // BLKCH: the Z of chain b's next block, for its products after
+            // its P4
+            if (!failed && T::BLKCH && x == 0) load_z(2 * bn + 1);
+            if (!failed && (NCB ? bn == NI - 1 : true)) released(x);
           }
         }
        }
@@ -1139,8 +1231,8 @@ cudaError_t run_tc3(const PolyClass& pc, const SearchDims& dims, int B, const vo
   p.B = NCB ? B : 1;
   p.n_items = dims.n_ant * dims.nb * (NCB ? 1 : 2) * p.groups;
   // too few items to fill the SMs (the non-coherent search on a few rows):
-  // split each item's PRN pairs over CTAs
-  const int n_rounds = (dims.n_prn + 1) / 2;
+  // split each item's rounds (PRN pairs, or PRNs with BLKCH) over CTAs
+  const int n_rounds = T::BLKCH ? dims.n_prn : (dims.n_prn + 1) / 2;
   p.split = 1;
   if (NCB && p.n_items > 0 && p.n_items < num_sms && n_rounds > 1) {
     p.split = (num_sms + p.n_items - 1) / p.n_items;
@@ -1209,6 +1301,12 @@ std::vector<unsigned char> tc_dft_matrices(int M) {
   return {};
 }
 
+double tc_key_amplitude(const PolyClass& pc) {
+  int kz = 0, kd = 0;
+  tc_scales(pc, &kz, &kd);
+  return (double)(1ull << (kz + kd));
+}
+
 float tc_z_scale(const PolyClass& pc) {
   int kz = 0, kd = 0;
   tc_scales(pc, &kz, &kd);
@@ -1242,8 +1340,13 @@ cudaError_t launch_correlate_tc(const PolyClass& pc, const SearchDims& dims, con
 cudaError_t launch_correlate_tc_nc(const PolyClass& pc, const SearchDims& dims, int B, const void* d_bmat,
                                    const void* d_z16, const void* d_d16, unsigned long long* d_keys, int* d_err,
                                    int test_flags, int num_sms, cudaStream_t st) {
-  if (pc.M != 1 || B < 1) return cudaErrorInvalidValue;
-  return run_tc3<1, true>(pc, dims, B, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
+  if (B < 1) return cudaErrorInvalidValue;
+  switch (pc.M) {
+    case 1: return run_tc3<1, true>(pc, dims, B, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
+    case 4: return run_tc3<4, true>(pc, dims, B, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
+    case 10: return run_tc3<10, true>(pc, dims, B, d_bmat, d_z16, d_d16, d_keys, d_err, test_flags, num_sms, st);
+  }
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace tga

@@ -91,6 +91,8 @@ cudaError_t launch_forward_seqs_tc(const PolyClass& pc, long long n_seq, float2*
                                    float z16_scale, int num_sms, cudaStream_t st);
 // FP16 scale of Z in the tensor-core operands
 float tc_z_scale(const PolyClass& pc);
+// |y| of a tensor-core key's row maximum is sqrt(key) x tc_key_amplitude
+double tc_key_amplitude(const PolyClass& pc);
 // forward transform of n_seq Lc-point sequences in place (any count)
 cudaError_t launch_forward_seqs(const PolyClass& pc, long long n_seq, float2* d_z, int num_sms, cudaStream_t st);
 cudaError_t launch_code_spectra(const PolyClass& pc, const int8_t* d_chips, int n_prn, float2* d_D,
@@ -98,14 +100,18 @@ cudaError_t launch_code_spectra(const PolyClass& pc, const int8_t* d_chips, int 
 cudaError_t launch_correlate(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
                              const float2* d_D, unsigned long long* d_keys, int num_sms,
                              cudaStream_t st);
-// FP32 re-evaluation of each (antenna, PRN)'s selected row: rewrites best.p / best.tau.
-// With d_rowbuf (n_ant * n_prn * P floats) it also leaves each row's |y|^2 there.
-cudaError_t launch_refine(const PolyClass& pc, const SearchDims& dims, const float2* d_Z, const float2* d_D,
-                          BestRow* d_best, float* d_rowbuf, int num_sms, cudaStream_t st);
-// Second peak (best.p2) from the rows launch_refine left in d_rowbuf; the
-// result equals launch_second_peak's.
-cudaError_t launch_second_scan(const PolyClass& pc, const SearchDims& dims, float* d_rowbuf, BestRow* d_best,
-                               int chip_width, int num_sms, cudaStream_t st);
+// launch_correlate over the rows listed in d_cand (*d_count of them, at
+// most capacity): each listed row's FP32 key is written where
+// launch_correlate would write it; other keys are left as they are.
+cudaError_t launch_correlate_listed(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
+                                    const float2* d_D, const int2* d_cand, const int* d_count, int capacity,
+                                    unsigned long long* d_keys, int num_sms, cudaStream_t st);
+// Lists, per (antenna, PRN), the rows whose reduced-precision key is at least
+// keep x the largest of its nb * n_hyp rows (appended to d_cand, counted in
+// *d_count, which must start at 0; d_cand holds up to n_ant * nb * n_hyp *
+// n_prn rows).  Keys are [ant][bin][hyp][prn].
+cudaError_t launch_tc_candidates(const SearchDims& dims, int n_hyp, const unsigned long long* d_keys, float keep,
+                                 int2* d_cand, int* d_count, cudaStream_t st);
 // Tensor-core search: FP16 operands in the (31, R2, R3) frequency layout
 // (launch_tc_pack of Z and of the code spectra), then the three-stage tcgen05
 // correlator (FP32 accumulation in TMEM).  Keys hold |y|^2 scaled by 2^-2k
@@ -183,10 +189,13 @@ cudaError_t launch_nc_correlate(const PolyClass& pc, const SearchDims& dims, int
                                 const float2* d_D, unsigned long long* d_keys, int num_sms, cudaStream_t st);
 cudaError_t launch_nc_reduce(const SearchDims& dims, const unsigned long long* d_keys, BestRow* d_best,
                              cudaStream_t st);
-// the selected row of every (antenna, PRN) re-evaluated in FP32 after a
-// reduced-precision non-coherent search (peak and lag replaced)
-cudaError_t launch_nc_refine(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
-                             const float2* d_D, BestRow* d_best, int num_sms, cudaStream_t st);
+// launch_nc_correlate over the (ab, prn) rows listed in d_cand (*d_count of
+// them, at most capacity), as the FP32 re-evaluation of a reduced-precision
+// search's candidates: each listed row's key is written where
+// launch_nc_correlate would write it
+cudaError_t launch_nc_correlate_listed(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
+                                       const float2* d_D, const int2* d_cand, const int* d_count, int capacity,
+                                       unsigned long long* d_keys, int num_sms, cudaStream_t st);
 cudaError_t launch_nc_second(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
                              const float2* d_D, BestRow* d_best, int chip_width, int num_sms, cudaStream_t st);
 

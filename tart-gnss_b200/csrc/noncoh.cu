@@ -180,16 +180,19 @@ __global__ void __launch_bounds__(256) nc_frontend_kernel(NcFrontParams p) {
   }
 }
 
-// NC_REFINE: the selected row of each (antenna, PRN) of a reduced-precision
-// search again in FP32: its peak and lag replace the row's
-enum NcMode { NC_PEAK = 0, NC_SECOND = 1, NC_REFINE = 2 };
+// NC_CAND: NC_PEAK over a device-built list of (ab, prn) rows (the
+// candidates of a reduced-precision search, re-evaluated in FP32): the list
+// holds *cand_count rows, each row's key goes where NC_PEAK would write it.
+enum NcMode { NC_PEAK = 0, NC_SECOND = 1, NC_CAND = 2 };
 
 struct NcParams {
   const float2* z;  // [n_ab][B][S][Lc], digit layout
   const float2* D;  // [n_prn][2][Lc]; the cyclic spectrum (index 0) is used
   int n_items, n_prn, S, P, B, chip_width;
-  unsigned long long* keys;  // NC_PEAK: [n_ab][n_prn]
-  BestRow* best;             // NC_SECOND, NC_REFINE: [n_ant][n_prn]
+  unsigned long long* keys;  // NC_PEAK, NC_CAND: [n_ab][n_prn]
+  BestRow* best;             // NC_SECOND: [n_ant][n_prn]
+  const int2* cand;          // NC_CAND: the rows
+  const int* cand_count;     // NC_CAND: their number (device)
 };
 
 template <int M, int BC, int NT, int MODE>
@@ -202,12 +205,17 @@ __global__ void __launch_bounds__(NT, 1) nc_correlate_kernel(NcParams p) {
   __shared__ unsigned int s_p2;
   const int tid = threadIdx.x, S = p.S;
   const int groups = (S + BC - 1) / BC;
-  for (int w = blockIdx.x; w < p.n_items; w += gridDim.x) {
-    constexpr bool ARGMAX = MODE == NC_PEAK || MODE == NC_REFINE;
+  const int n_work = MODE == NC_CAND ? min(p.n_items, *p.cand_count) : p.n_items;
+  for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
+    constexpr bool ARGMAX = MODE == NC_PEAK || MODE == NC_CAND;
     int ab, prn, tau_star = 0;
     if (MODE == NC_PEAK) {
       ab = w / p.n_prn;
       prn = w - ab * p.n_prn;
+    } else if (MODE == NC_CAND) {
+      const int2 c = p.cand[w];
+      ab = c.x;
+      prn = c.y;
     } else {
       const BestRow b = p.best[w];
       ab = b.ab;
@@ -304,14 +312,7 @@ __global__ void __launch_bounds__(NT, 1) nc_correlate_kernel(NcParams p) {
       }
       if ((tid & 31) == 0) atomicMax(&s_key, kbest);
       __syncthreads();
-      if (tid == 0) {
-        if (MODE == NC_PEAK) {
-          p.keys[w] = s_key;
-        } else {
-          p.best[w].tau = (int)(unsigned)(s_key & 0xffffffffull);
-          p.best[w].p = __uint_as_float((unsigned)(s_key >> 32));
-        }
-      }
+      if (tid == 0) p.keys[(size_t)ab * p.n_prn + prn] = s_key;
     } else {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) pbest = fmaxf(pbest, __shfl_xor_sync(0xffffffffu, pbest, o));
@@ -468,18 +469,21 @@ cudaError_t launch_nc_second(const PolyClass& pc, const SearchDims& dims, int B,
   return dispatch_nc<NC_SECOND>(pc.M, p, num_sms, st);
 }
 
-cudaError_t launch_nc_refine(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
-                             const float2* d_D, BestRow* d_best, int num_sms, cudaStream_t st) {
+cudaError_t launch_nc_correlate_listed(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
+                                       const float2* d_D, const int2* d_cand, const int* d_count, int capacity,
+                                       unsigned long long* d_keys, int num_sms, cudaStream_t st) {
   NcParams p = {};
   p.z = d_z;
   p.D = d_D;
-  p.best = d_best;
+  p.keys = d_keys;
+  p.cand = d_cand;
+  p.cand_count = d_count;
   p.n_prn = dims.n_prn;
   p.S = pc.S;
   p.P = pc.P;
   p.B = B;
-  p.n_items = dims.n_ant * dims.n_prn;
-  return dispatch_nc<NC_REFINE>(pc.M, p, num_sms, st);
+  p.n_items = capacity;
+  return dispatch_nc<NC_CAND>(pc.M, p, num_sms, st);
 }
 
 }  // namespace tga

@@ -31,10 +31,6 @@ struct Geo {
   }
   // digit-layout offset of (a, b, c): [a][c][b]
   __device__ static __forceinline__ int offset(int a, int b, int c) { return a * COLS + c * 33 + b; }
-  // position of output (a, b, c) in a row buffer of REFINE: the order in
-  // which consecutive threads emit it ([b][a] for M = 1, whose last stage
-  // runs per a; [a][c][b] otherwise)
-  __device__ static __forceinline__ int row_pos(int a, int b, int c) { return M == 1 ? b * 31 + a : offset(a, b, c); }
 };
 
 // FP16 operands of the tensor-core search in its (31, R2, R3) frequency
@@ -67,9 +63,11 @@ struct TcUnits {
   }
 };
 
-// REFINE re-evaluates the selected row of each (antenna, PRN) in FP32 and
-// rewrites its peak value and lag (used after a reduced-precision search).
-enum PfaMode { FWD_Z = 0, FWD_D = 1, CORR = 2, SECOND = 3, REFINE = 4 };
+// CAND is CORR over a device-built list of rows (the candidates of a
+// reduced-precision search, re-evaluated in FP32): row i of the list is
+// (ab * 2 + hyp, prn), the list holds *cand_count rows, and each row's key
+// goes where CORR would write it.
+enum PfaMode { FWD_Z = 0, FWD_D = 1, CORR = 2, SECOND = 3, CAND = 4 };
 
 struct PfaParams {
   float2* z;                  // FWD_Z: sequences, transformed in place; CORR/SECOND: Z
@@ -77,11 +75,12 @@ struct PfaParams {
   float2* Dout;               // FWD_D output
   const int8_t* chips;        // FWD_D input [n_prn][Lc]
   int n_seq;                  // FWD modes
-  int n_items;                // CORR: n_ab*2*n_prn rows; SECOND: n_ant*n_prn
+  int n_items;                // CORR: n_ab*2*n_prn rows; SECOND: n_ant*n_prn; CAND: list capacity
   int n_prn, S, P, chip_width;
-  unsigned long long* keys;   // CORR output, one per row
+  unsigned long long* keys;   // CORR / CAND output, one per row ([ab * 2 + hyp][prn])
   BestRow* best;              // SECOND in/out
-  float* rowbuf;              // REFINE (optional): |y|^2 of each item's row, [item][rho][row_pos]
+  const int2* cand;           // CAND: the rows to evaluate
+  const int* cand_count;      // CAND: their number (device)
   uint4* z16;                 // FWD_Z (optional): the transformed sequences also as TcUnits, x z16_scale
   const uint2* z16_map;       // per unit: the 4 src_offset values as 16-bit fields (0xffff: zero)
   float z16_scale;

@@ -99,6 +99,17 @@ struct tga_ctx {
   size_t gen = 0;
   std::map<std::string, GraphEntry> graphs;
   int last_graph = TGA_GRAPH_NONE;
+  // the fused class groups of the last --all call (tga_last_row_peaks)
+  struct LastGroup {
+    int Lc = 0, P = 0, n_ant = 0, nb = 0, n_prn = 0;
+    bool tc = false;
+    double amp = 1.0;  // |y| = sqrt(key power) x amp
+    const unsigned long long* keys = nullptr;
+    const int* count = nullptr;
+    int n_chunks = 1;             // counts in `count`
+    double nc_power_scale = 0.0;  // > 0: a non-coherent search (one hypothesis, power units)
+  };
+  std::vector<LastGroup> last_groups;
   // pinned host staging for results
   void* pinned = nullptr;
   size_t pinned_cap = 0;
@@ -347,6 +358,17 @@ void run_planned(tga_ctx* ctx, const std::string& key, F&& enqueue) {
 double fft_flops(double n) { return n > 1.0 ? 5.0 * n * std::log2(n) : 0.0; }
 double corr_row_flops(int P) { return fft_flops((double)P) + 9.0 * (double)P; }
 
+// Tensor-core search: rows whose FP16 key is at least kTcKeyKeep x the best
+// key of their (antenna, PRN) are re-evaluated in FP32.  kTcKeyKeep =
+// (1 - 2 d)^2 with d = 2^-6 a bound on the FP16 transform's error at a lag,
+// relative to the amplitude of the row's largest lag (measured errors stay
+// far below it; see the key-error report of tga_last_row_peaks).
+constexpr float kTcKeyKeep = (1.0f - 2.0f / 64.0f) * (1.0f - 2.0f / 64.0f);
+
+// Device bytes the non-coherent search's Z may take at once (FP32, plus the
+// FP16 operands in tensor-core mode); more antennas than fit run in chunks.
+constexpr double kNcZBudget = 24e9;
+
 const std::vector<int8_t>& cached_chips(tga_ctx* ctx, int c, int prn) {
   auto key = std::make_pair(c, prn);
   auto it = ctx->chip_cache.find(key);
@@ -453,7 +475,11 @@ struct GroupBufs {
   void* d16 = nullptr;
   void* bmat = nullptr;
   void* zmap = nullptr;   // tensor-core mode: FP16 unit offsets (tc_unit_map)
-  float* rows = nullptr;  // tensor-core mode: |y|^2 of each (antenna, PRN)'s selected row
+  // tensor-core mode: FP32 keys of the rows re-evaluated, the list of those
+  // rows and its length
+  unsigned long long* keys32 = nullptr;
+  int2* cand = nullptr;
+  int* count = nullptr;
 };
 
 GroupBufs prepare_group(tga_ctx* ctx, const ClassGroup& grp, int n_ant, int nb, const std::string& tag) {
@@ -489,7 +515,9 @@ GroupBufs prepare_group(tga_ctx* ctx, const ClassGroup& grp, int n_ant, int nb, 
     const long long n_zseq = (long long)n_ab * 2 * pc.S;
     b.z16 = ctx->buf(tag + ".z16", tc_operand_bytes(pc, n_zseq, false));
     b.d16 = ctx->buf(tag + ".d16", tc_operand_bytes(pc, (long long)n_prn * 2, true));
-    b.rows = (float*)ctx->buf(tag + ".rows", (size_t)n_ant * n_prn * pc.P * sizeof(float));
+    b.keys32 = (unsigned long long*)ctx->buf(tag + ".keys32", (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long));
+    b.cand = (int2*)ctx->buf(tag + ".cand", (size_t)n_ab * 2 * n_prn * sizeof(int2));
+    b.count = (int*)ctx->buf(tag + ".count", sizeof(int));
     // DFT matrices of the class (they depend on Lc only), uploaded once per context
     const std::string mat_name = "tcmat." + std::to_string(pc.M);
     if (!ctx->uploaded.count(mat_name)) {
@@ -542,24 +570,27 @@ void enqueue_group(tga_ctx* ctx, const ClassGroup& grp, const GroupBufs& b, cons
       return launch_correlate_tc(pc, dims, b.bmat, b.z16, b.d16, b.keys, b.err, ctx->test_flags, ctx->num_sms, st);
     });
     ctx->tc_err_pending = b.err;
+    // every row within the FP16 key error of its (antenna, PRN)'s best,
+    // re-evaluated in FP32; the bins are then reduced over the FP32 keys as
+    // in the FP32 search (rows not listed keep key 0)
+    CK(cudaMemsetAsync(b.count, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(b.keys32, 0, (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long), st));
+    timed(ctx, ("candidates" + cls).c_str(), 0.0,
+          [&] { return launch_tc_candidates(dims, 2, b.keys, kTcKeyKeep, b.cand, b.count, st); });
+    timed(ctx, ("refine" + cls).c_str(), 0.0, [&] {
+      return launch_correlate_listed(pc, dims, b.z, b.D, b.cand, b.count, n_ab * 2 * n_prn, b.keys32, ctx->num_sms,
+                                     st);
+    });
   } else {
     timed(ctx, ("forward_z" + cls).c_str(), (double)n_ab * 2 * fft_flops(pc.P),
           [&] { return launch_forward_z(pc, n_ab, b.z, ctx->num_sms, st); });
     timed(ctx, ("correlate" + cls).c_str(), (double)n_ab * 2 * n_prn * row,
           [&] { return launch_correlate(pc, dims, b.z, b.D, b.keys, ctx->num_sms, st); });
   }
-  timed(ctx, ("reduce_bins" + cls).c_str(), 0.0, [&] { return launch_reduce_bins(dims, b.keys, b.best, st); });
-  if (ctx->precision == TGA_PRECISION_FP16_TC) {
-    // the FP32 re-evaluation keeps the selected rows, and the second peak is
-    // read from them instead of transforming the rows again
-    timed(ctx, ("refine" + cls).c_str(), (double)n_ant * n_prn * row,
-          [&] { return launch_refine(pc, dims, b.z, b.D, b.best, b.rows, ctx->num_sms, st); });
-    timed(ctx, ("second_scan" + cls).c_str(), 0.0,
-          [&] { return launch_second_scan(pc, dims, b.rows, b.best, chip_width, ctx->num_sms, st); });
-  } else {
-    timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * row,
-          [&] { return launch_second_peak(pc, dims, b.z, b.D, b.best, chip_width, ctx->num_sms, st); });
-  }
+  const unsigned long long* keys32 = ctx->precision == TGA_PRECISION_FP16_TC ? b.keys32 : b.keys;
+  timed(ctx, ("reduce_bins" + cls).c_str(), 0.0, [&] { return launch_reduce_bins(dims, keys32, b.best, st); });
+  timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * row,
+        [&] { return launch_second_peak(pc, dims, b.z, b.D, b.best, chip_width, ctx->num_sms, st); });
   timed(ctx, ("finalize" + cls).c_str(), 0.0,
         [&] { return launch_finalize(pc, dims, b.best, center, b.tables, want_cn0, b.cells, st); });
   CK(cudaMemcpyAsync(host_out, b.cells, (size_t)n_ant * n_prn * sizeof(CellOut), cudaMemcpyDeviceToHost, st));
@@ -632,6 +663,7 @@ int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, si
   // to the generic path
   std::vector<ClassGroup> groups;
   std::vector<int> generic_consts;
+  ctx->last_groups.clear();
   for (int c : consts) {
     const size_t P = period_samples(c, fs);
     if (P == 0) throw InvalidArg("sampling frequency too low for " + std::string(info(c).json_key));
@@ -769,6 +801,19 @@ int acquire_all_impl(tga_ctx* ctx, const uint8_t* d_bits, size_t n_ant_total, si
   ctx->last_launches = kernel_launch_count();
   collect_times(ctx);
   check_tc_error(ctx);
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    tga_ctx::LastGroup lg;
+    lg.Lc = groups[gi].pc.Lc;
+    lg.P = groups[gi].pc.P;
+    lg.n_ant = (int)ants.size();
+    lg.nb = nb;
+    lg.n_prn = (int)groups[gi].prns.size();
+    lg.tc = ctx->precision == TGA_PRECISION_FP16_TC;
+    lg.amp = lg.tc ? tc_key_amplitude(groups[gi].pc) : 1.0;
+    lg.keys = gbufs[gi].keys;
+    lg.count = gbufs[gi].count;
+    ctx->last_groups.push_back(lg);
+  }
 
   // assemble in (constellation, prn order, antenna) order
   size_t k = 0;
@@ -1227,6 +1272,40 @@ int tga_autotune(tga_ctx* ctx, const uint8_t* d_packed_bits, size_t n_ant, size_
       e.variant = best;
     }
     *n_out = k;
+    return TGA_OK;
+  });
+}
+
+int tga_last_row_peaks(tga_ctx* ctx, int chips, double* out, size_t cap, size_t* n_out, int64_t* n_rows_refined) {
+  return guarded(ctx, [&] {
+    if (!n_out) throw InvalidArg("null n_out");
+    const tga_ctx::LastGroup* g = nullptr;
+    for (const auto& lg : ctx->last_groups)
+      if (lg.Lc == chips) g = &lg;
+    if (!g) throw InvalidArg("the last search had no fused group of " + std::to_string(chips) + " chips");
+    const bool nc = g->nc_power_scale > 0.0;
+    const size_t n = (size_t)g->n_ant * g->nb * (nc ? 1 : 2) * g->n_prn;
+    *n_out = n;
+    if (n_rows_refined) {
+      std::vector<int> cnt((size_t)g->n_chunks, 0);
+      if (g->tc) CK(cudaMemcpy(cnt.data(), g->count, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost));
+      int64_t sum = 0;
+      for (int c : cnt) sum += c;
+      *n_rows_refined = sum;
+    }
+    if (!out) return TGA_OK;
+    if (cap < n) return TGA_ERR_CAPACITY;
+    std::vector<unsigned long long> keys(n);
+    CK(cudaMemcpy(keys.data(), g->keys, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    // the reference's |IFFT_2P| / sqrt(2P) is |y| sqrt(2P) / Lc; the
+    // non-coherent power is |y|^2 nc_power_scale
+    const double scale = g->amp * std::sqrt(2.0 * (double)g->P) / (double)g->Lc;
+    for (size_t i = 0; i < n; ++i) {
+      const uint32_t bits = (uint32_t)(keys[i] >> 32);
+      float pw;
+      std::memcpy(&pw, &bits, sizeof pw);
+      out[i] = nc ? (double)pw * g->amp * g->amp * g->nc_power_scale : std::sqrt((double)pw) * scale;
+    }
     return TGA_OK;
   });
 }
@@ -1766,160 +1845,297 @@ int tga_rfi_scan(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant, size_t row_b
 }
 
 // ---------------------------------------------------------------------------
-// non-coherent search (tga_search_noncoherent)
+// non-coherent search (tga_search_noncoherent, tga_search_noncoherent_multi)
 // ---------------------------------------------------------------------------
-int tga_search_noncoherent(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant_total, size_t row_bytes, double fs,
-                           const tga_nc_options* opt, tga_nc_cell* out, size_t cap, size_t* n_out) {
-  return guarded(ctx, [&] {
-    if (!h_bits || !opt || !n_out || n_ant_total == 0 || row_bytes == 0 || !(fs > 0)) throw InvalidArg("bad arguments");
-    const int c = opt->constellation;
-    if (c < 0 || c >= N_CONST) throw InvalidArg("bad constellation");
-    if (opt->n_bins < 1 || opt->coherent_periods < 1 || opt->blocks < 1 || opt->start < 0 ||
-        !(opt->bin_step_hz >= 0))
-      throw InvalidArg("bad search geometry");
-    std::vector<int32_t> ants, prn_list;
-    if (opt->ant_filter) {
-      for (size_t i = 0; i < opt->n_ant_filter; ++i) {
-        if (opt->ant_filter[i] < 0 || (size_t)opt->ant_filter[i] >= n_ant_total)
-          throw InvalidArg("antenna index out of range");
-        ants.push_back(opt->ant_filter[i]);
-      }
+namespace {
+
+// One constellation's search of a multi call, validated.
+struct NcMember {
+  const tga_nc_options* opt = nullptr;
+  int c = 0;
+  std::vector<int32_t> ants, prns;
+  PolyClass pc;
+  size_t out_off = 0;  // first cell of this member in the caller's output
+};
+
+NcMember nc_member(tga_ctx* ctx, const tga_nc_options* opt, size_t n_ant_total, size_t row_bytes, double fs) {
+  NcMember m;
+  m.opt = opt;
+  const int c = opt->constellation;
+  if (c < 0 || c >= N_CONST) throw InvalidArg("bad constellation");
+  m.c = c;
+  if (opt->n_bins < 1 || opt->coherent_periods < 1 || opt->blocks < 1 || opt->start < 0 || !(opt->bin_step_hz >= 0))
+    throw InvalidArg("bad search geometry");
+  if (opt->ant_filter) {
+    for (size_t i = 0; i < opt->n_ant_filter; ++i) {
+      if (opt->ant_filter[i] < 0 || (size_t)opt->ant_filter[i] >= n_ant_total)
+        throw InvalidArg("antenna index out of range");
+      m.ants.push_back(opt->ant_filter[i]);
+    }
+  } else {
+    for (size_t i = 0; i < n_ant_total; ++i) m.ants.push_back((int32_t)i);
+  }
+  if (m.ants.empty()) throw InvalidArg("no antennas selected");
+  const ConstellationInfo& ci = info(c);
+  if (opt->prn_filter) {
+    for (size_t i = 0; i < opt->n_prn_filter; ++i) {
+      validate_prn(c, opt->prn_filter[i]);
+      m.prns.push_back(opt->prn_filter[i]);
+    }
+  } else {
+    for (int q = ci.prn_first; q <= ci.prn_last; ++q) m.prns.push_back(q);
+  }
+  const size_t P = period_samples(c, fs);
+  if (P == 0) throw InvalidArg("sampling frequency too low for " + std::string(ci.json_key));
+  const long long need = opt->start + (long long)opt->blocks * opt->coherent_periods * (long long)P;
+  if (need > (long long)row_bytes * 8) throw InvalidArg("the blocks run past the end of the recording");
+  std::vector<int> prns_i(m.prns.begin(), m.prns.end());
+  if (!poly_class_for(ctx, c, (double)P, P, 2 * P, prns_i, &m.pc)) {
+    ctx->err = "non-coherent search needs an integer number of samples per chip";
+    throw std::domain_error(ctx->err);
+  }
+  return m;
+}
+
+// Members that can share one front end: the same polyphase class and the
+// same blocks, Doppler grid and antennas.
+bool nc_same_group(const NcMember& a, const NcMember& b) {
+  const tga_nc_options *x = a.opt, *y = b.opt;
+  return same_class(a.pc, b.pc) && x->center_freq == y->center_freq && x->bin_step_hz == y->bin_step_hz &&
+         x->n_bins == y->n_bins && x->coherent_periods == y->coherent_periods && x->blocks == y->blocks &&
+         x->start == y->start && a.ants == b.ants;
+}
+
+// The search of one group on the device bits (means already computed):
+// front end and forward transform once, then every member's PRNs together.
+// Writes each member's cells at its out_off.  gi names the group's key
+// buffers, which stay alive for tga_last_row_peaks.
+void nc_run_group(tga_ctx* ctx, const uint8_t* d_bits, size_t row_bytes, const double* d_mean, double fs,
+                  const std::vector<NcMember*>& mem, int gi, tga_nc_cell* out) {
+  const NcMember& m0 = *mem[0];
+  const tga_nc_options* opt = m0.opt;
+  const PolyClass& pc = m0.pc;
+  const size_t P = pc.P;
+  cudaStream_t st = ctx->stream;
+  const std::vector<int32_t>& ants = m0.ants;
+  std::vector<std::pair<int, int>> prns;  // (constellation, prn) in member order
+  for (const NcMember* m : mem)
+    for (int q : m->prns) prns.push_back({m->c, q});
+  const int n_ant = (int)ants.size(), n_prn = (int)prns.size(), nb = opt->n_bins, B = opt->blocks;
+  const std::string tag = "nc" + std::to_string(gi);
+  int32_t* d_ant = (int32_t*)ctx->buf(tag + ".ant", ants.size() * sizeof(int32_t));
+  CK(cudaMemcpyAsync(d_ant, ants.data(), ants.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  std::vector<double> fc(nb);
+  for (int i = 0; i < nb; ++i) fc[i] = opt->center_freq + (double)(i - (nb - 1) / 2) * opt->bin_step_hz;
+  double* d_fc = (double*)ctx->buf(tag + ".fc", fc.size() * sizeof(double));
+  CK(cudaMemcpyAsync(d_fc, fc.data(), fc.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  std::vector<int8_t> chips((size_t)n_prn * pc.Lc);
+  for (int i = 0; i < n_prn; ++i) {
+    const std::vector<int8_t>& ch = cached_chips(ctx, prns[i].first, prns[i].second);
+    std::memcpy(&chips[(size_t)i * pc.Lc], ch.data(), (size_t)pc.Lc);
+  }
+  int8_t* d_chips = (int8_t*)ctx->buf(tag + ".chips", chips.size());
+  CK(cudaMemcpyAsync(d_chips, chips.data(), chips.size(), cudaMemcpyHostToDevice, st));
+  ctx->h2d += ants.size() * sizeof(int32_t) + fc.size() * sizeof(double) + chips.size();
+  SampleSource src;
+  src.bits = d_bits;
+  src.row_bytes = row_bytes;
+  src.mean = d_mean;
+  src.ant = d_ant;
+  src.n_ant = n_ant;
+  src.pc = 6.283185307179586 / fs;
+  SearchDims dims;
+  dims.n_ant = n_ant;
+  dims.nb = nb;
+  dims.n_prn = n_prn;
+  dims.fc = d_fc;
+  // Antennas run in chunks, so that Z (FP32, and in tensor-core mode its
+  // FP16 operands) stays within kNcZBudget bytes; keys and results are
+  // [antenna]-major, so each chunk owns a contiguous part of them.
+  const bool tc = ctx->precision == TGA_PRECISION_FP16_TC;
+  const long long seq_per_ant = (long long)nb * B * pc.S;
+  const double z_per_ant = (double)seq_per_ant * pc.Lc * (sizeof(float2) + (tc ? 4.0 : 0.0));
+  long long chunk = (long long)std::floor(kNcZBudget / z_per_ant);
+  chunk = std::min<long long>(std::max<long long>(chunk, 1), n_ant);
+  chunk = std::min<long long>(chunk, 65535 / ((long long)nb * B));  // front-end grid rows
+  if (chunk < 1) throw InvalidArg("too many bins x blocks for one front-end launch");
+  const int n_chunks = (int)((n_ant + chunk - 1) / chunk);
+  const long long n_seq = chunk * seq_per_ant;
+  const size_t n_rows = (size_t)n_ant * nb * n_prn;
+  float2* d_z = (float2*)ctx->buf("nc.z", (size_t)n_seq * pc.Lc * sizeof(float2));
+  float2* d_D = (float2*)ctx->buf(tag + ".D", (size_t)n_prn * 2 * pc.Lc * sizeof(float2));
+  unsigned long long* d_keys = (unsigned long long*)ctx->buf(tag + ".keys", n_rows * sizeof(unsigned long long));
+  BestRow* d_best = (BestRow*)ctx->buf(tag + ".best", (size_t)n_ant * n_prn * sizeof(BestRow));
+  const double row = corr_row_flops(pc.P);
+  timed(ctx, "nc_code_spectra", (double)n_prn * 2 * fft_flops(pc.Lc),
+        [&] { return launch_code_spectra(pc, d_chips, n_prn, d_D, ctx->num_sms, st); });
+  // tensor-core mode: FP16 operands, DFT matrices, and the FP32
+  // re-evaluation's keys, row list and per-chunk counts
+  void *d_z16 = nullptr, *d_zmap = nullptr, *d_d16 = nullptr, *d_bmat = nullptr;
+  int *d_err = nullptr, *d_count = nullptr;
+  unsigned long long* d_keys32 = nullptr;
+  int2* d_cand = nullptr;
+  if (tc) {
+    d_z16 = ctx->buf("nc.z16", tc_operand_bytes(pc, n_seq, false));
+    d_zmap = tc_unit_map_buf(ctx, pc.M);
+    d_err = (int*)ctx->buf("tc.err", sizeof(int));
+    d_d16 = ctx->buf(tag + ".d16", tc_operand_bytes(pc, (long long)n_prn * 2, true));
+    const std::string mat_name = "tcmat." + std::to_string(pc.M);
+    if (!ctx->uploaded.count(mat_name)) {
+      const std::vector<unsigned char> mats = tc_dft_matrices(pc.M);
+      d_bmat = ctx->buf(mat_name, mats.size());
+      CK(cudaMemcpy(d_bmat, mats.data(), mats.size(), cudaMemcpyHostToDevice));
+      ctx->uploaded[mat_name] = {};
     } else {
-      for (size_t i = 0; i < n_ant_total; ++i) ants.push_back((int32_t)i);
+      d_bmat = ctx->buf(mat_name, 0);
     }
-    const ConstellationInfo& ci = info(c);
-    if (opt->prn_filter) {
-      for (size_t i = 0; i < opt->n_prn_filter; ++i) {
-        validate_prn(c, opt->prn_filter[i]);
-        prn_list.push_back(opt->prn_filter[i]);
-      }
-    } else {
-      for (int q = ci.prn_first; q <= ci.prn_last; ++q) prn_list.push_back(q);
-    }
-    const size_t n_cells = ants.size() * prn_list.size();
-    *n_out = n_cells;
-    if (!out) return TGA_OK;
-    if (cap < n_cells) return TGA_ERR_CAPACITY;
-    const size_t P = period_samples(c, fs);
-    const long long need = opt->start + (long long)opt->blocks * opt->coherent_periods * (long long)P;
-    if (need > (long long)row_bytes * 8) throw InvalidArg("the blocks run past the end of the recording");
-    PolyClass pc;
-    std::vector<int> prns_i(prn_list.begin(), prn_list.end());
-    if (!poly_class_for(ctx, c, (double)P, P, 2 * P, prns_i, &pc)) {
-      ctx->err = "non-coherent search needs an integer number of samples per chip";
-      return TGA_ERR_UNSUPPORTED;
-    }
-    begin_call(ctx);
-    const int n_ant = (int)ants.size(), n_prn = (int)prn_list.size(), nb = opt->n_bins, B = opt->blocks;
-    cudaStream_t st = ctx->stream;
-    uint8_t* d_bits = (uint8_t*)ctx->buf("nc.bits", n_ant_total * row_bytes);
-    CK(cudaMemcpyAsync(d_bits, h_bits, n_ant_total * row_bytes, cudaMemcpyHostToDevice, st));
-    ctx->h2d += n_ant_total * row_bytes;
-    double* d_mean = (double*)ctx->buf("nc.mean", n_ant_total * sizeof(double));
-    CK(launch_antenna_means(d_bits, (int)n_ant_total, row_bytes, d_mean, st));
-    int32_t* d_ant = (int32_t*)ctx->buf("nc.ant", ants.size() * sizeof(int32_t));
-    CK(cudaMemcpyAsync(d_ant, ants.data(), ants.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-    std::vector<double> fc(nb);
-    for (int i = 0; i < nb; ++i) fc[i] = opt->center_freq + (double)(i - (nb - 1) / 2) * opt->bin_step_hz;
-    double* d_fc = (double*)ctx->buf("nc.fc", fc.size() * sizeof(double));
-    CK(cudaMemcpyAsync(d_fc, fc.data(), fc.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    std::vector<int8_t> chips((size_t)n_prn * pc.Lc);
-    for (int i = 0; i < n_prn; ++i) {
-      const std::vector<int8_t>& ch = cached_chips(ctx, c, prn_list[i]);
-      std::memcpy(&chips[(size_t)i * pc.Lc], ch.data(), (size_t)pc.Lc);
-    }
-    int8_t* d_chips = (int8_t*)ctx->buf("nc.chips", chips.size());
-    CK(cudaMemcpyAsync(d_chips, chips.data(), chips.size(), cudaMemcpyHostToDevice, st));
-    SampleSource src;
-    src.bits = d_bits;
-    src.row_bytes = row_bytes;
-    src.mean = d_mean;
-    src.ant = d_ant;
-    src.n_ant = n_ant;
-    src.pc = 6.283185307179586 / fs;
-    SearchDims dims;
-    dims.n_ant = n_ant;
-    dims.nb = nb;
-    dims.n_prn = n_prn;
-    dims.fc = d_fc;
-    const long long n_seq = (long long)n_ant * nb * B * pc.S;
-    float2* d_z = (float2*)ctx->buf("nc.z", (size_t)n_seq * pc.Lc * sizeof(float2));
-    float2* d_D = (float2*)ctx->buf("nc.D", (size_t)n_prn * 2 * pc.Lc * sizeof(float2));
-    unsigned long long* d_keys =
-        (unsigned long long*)ctx->buf("nc.keys", (size_t)n_ant * nb * n_prn * sizeof(unsigned long long));
-    BestRow* d_best = (BestRow*)ctx->buf("nc.best", (size_t)n_ant * n_prn * sizeof(BestRow));
-    const double row = corr_row_flops(pc.P);
-    timed(ctx, "nc_code_spectra", (double)n_prn * 2 * fft_flops(pc.Lc),
-          [&] { return launch_code_spectra(pc, d_chips, n_prn, d_D, ctx->num_sms, st); });
-    timed(ctx, "nc_frontend", (double)n_ant * nb * B * 10.0 * pc.P * opt->coherent_periods,
-          [&] { return launch_nc_frontend(src, dims, pc, opt->coherent_periods, B, opt->start, d_z, st); });
-    // the tensor-core path covers Lc = 1023 (GPS, SBAS, QZSS C/A); other code
-    // lengths run the FP32 search whatever the precision
-    const bool tc = ctx->precision == TGA_PRECISION_FP16_TC && pc.M == 1;
-    void* d_z16 = tc ? ctx->buf("nc.z16", tc_operand_bytes(pc, n_seq, false)) : nullptr;
-    void* d_zmap = tc ? tc_unit_map_buf(ctx, pc.M) : nullptr;
+    d_keys32 = (unsigned long long*)ctx->buf(tag + ".keys32", n_rows * sizeof(unsigned long long));
+    d_cand = (int2*)ctx->buf(tag + ".cand", n_rows * sizeof(int2));
+    d_count = (int*)ctx->buf(tag + ".count", (size_t)n_chunks * sizeof(int));
+    timed(ctx, "nc_tc_pack", 0.0,
+          [&] { return launch_tc_pack(pc, d_D, (long long)n_prn * 2, true, d_d16, ctx->num_sms, st); });
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(d_count, 0, (size_t)n_chunks * sizeof(int), st));
+    CK(cudaMemsetAsync(d_keys, 0, n_rows * sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(d_keys32, 0, n_rows * sizeof(unsigned long long), st));
+    ctx->tc_err_pending = d_err;
+  }
+  for (int ch = 0; ch < n_chunks; ++ch) {
+    const int a0 = (int)(ch * chunk), na = (int)std::min<long long>(chunk, n_ant - a0);
+    const size_t r0 = (size_t)a0 * nb * n_prn;
+    SampleSource cs = src;
+    cs.ant = d_ant + a0;
+    cs.n_ant = na;
+    SearchDims cd = dims;
+    cd.n_ant = na;
+    const long long cseq = (long long)na * seq_per_ant;
+    BestRow* cbest = d_best + (size_t)a0 * n_prn;
+    timed(ctx, "nc_frontend", (double)na * nb * B * 10.0 * pc.P * opt->coherent_periods,
+          [&] { return launch_nc_frontend(cs, cd, pc, opt->coherent_periods, B, opt->start, d_z, st); });
     // in tensor-core mode the forward transform also writes Z's FP16 operands
-    timed(ctx, "nc_forward_z", (double)n_ant * nb * B * fft_flops(pc.P), [&] {
-      return tc ? launch_forward_seqs_tc(pc, n_seq, d_z, d_z16, d_zmap, tc_z_scale(pc), ctx->num_sms, st)
-                : launch_forward_seqs(pc, n_seq, d_z, ctx->num_sms, st);
+    timed(ctx, "nc_forward_z", (double)na * nb * B * fft_flops(pc.P), [&] {
+      return tc ? launch_forward_seqs_tc(pc, cseq, d_z, d_z16, d_zmap, tc_z_scale(pc), ctx->num_sms, st)
+                : launch_forward_seqs(pc, cseq, d_z, ctx->num_sms, st);
     });
     if (tc) {
-      int* d_err = (int*)ctx->buf("tc.err", sizeof(int));
-      void* d_d16 = ctx->buf("nc.d16", tc_operand_bytes(pc, (long long)n_prn * 2, true));
-      const std::string mat_name = "tcmat." + std::to_string(pc.M);
-      void* d_bmat = nullptr;
-      if (!ctx->uploaded.count(mat_name)) {
-        const std::vector<unsigned char> mats = tc_dft_matrices(pc.M);
-        d_bmat = ctx->buf(mat_name, mats.size());
-        CK(cudaMemcpy(d_bmat, mats.data(), mats.size(), cudaMemcpyHostToDevice));
-        ctx->uploaded[mat_name] = {};
-      } else {
-        d_bmat = ctx->buf(mat_name, 0);
-      }
-      timed(ctx, "nc_tc_pack", 0.0,
-            [&] { return launch_tc_pack(pc, d_D, (long long)n_prn * 2, true, d_d16, ctx->num_sms, st); });
-      CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
-      CK(cudaMemsetAsync(d_keys, 0, (size_t)n_ant * nb * n_prn * sizeof(unsigned long long), st));
-      timed(ctx, "nc_correlate_tc", (double)n_ant * nb * n_prn * B * row, [&] {
-        return launch_correlate_tc_nc(pc, dims, B, d_bmat, d_z16, d_d16, d_keys, d_err, ctx->test_flags,
+      timed(ctx, "nc_correlate_tc", (double)na * nb * n_prn * B * row, [&] {
+        return launch_correlate_tc_nc(pc, cd, B, d_bmat, d_z16, d_d16, d_keys + r0, d_err, ctx->test_flags,
                                       ctx->num_sms, st);
       });
-      ctx->tc_err_pending = d_err;
+      // rows within the FP16 key error of their (antenna, PRN)'s best,
+      // re-evaluated in FP32; the bins are then reduced over the FP32 keys
+      timed(ctx, "nc_candidates", 0.0, [&] {
+        return launch_tc_candidates(cd, 1, d_keys + r0, kTcKeyKeep, d_cand + r0, d_count + ch, st);
+      });
+      timed(ctx, "nc_refine", 0.0, [&] {
+        return launch_nc_correlate_listed(pc, cd, B, d_z, d_D, d_cand + r0, d_count + ch, na * nb * n_prn,
+                                          d_keys32 + r0, ctx->num_sms, st);
+      });
     } else {
-      timed(ctx, "nc_correlate", (double)n_ant * nb * n_prn * B * row,
-            [&] { return launch_nc_correlate(pc, dims, B, d_z, d_D, d_keys, ctx->num_sms, st); });
+      timed(ctx, "nc_correlate", (double)na * nb * n_prn * B * row,
+            [&] { return launch_nc_correlate(pc, cd, B, d_z, d_D, d_keys + r0, ctx->num_sms, st); });
     }
-    timed(ctx, "nc_reduce", 0.0, [&] { return launch_nc_reduce(dims, d_keys, d_best, st); });
-    if (tc)
-      timed(ctx, "nc_refine", (double)n_ant * n_prn * B * row,
-            [&] { return launch_nc_refine(pc, dims, B, d_z, d_D, d_best, ctx->num_sms, st); });
-    timed(ctx, "nc_second", (double)n_ant * n_prn * B * row, [&] {
-      return launch_nc_second(pc, dims, B, d_z, d_D, d_best, chip_width_of(fs), ctx->num_sms, st);
-    });
-    std::vector<BestRow> best((size_t)n_ant * n_prn);
-    CK(cudaMemcpyAsync(best.data(), d_best, best.size() * sizeof(BestRow), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    collect_times(ctx);
-    check_tc_error(ctx);
-    ctx->last_cells = (double)n_ant * nb * n_prn * (double)P * B;
-    // |y| of the polyphase correlator is Lc |r|; report (|r| sqrt(N))^2 per block
-    const double scale = (double)opt->coherent_periods * (double)P / ((double)pc.Lc * (double)pc.Lc);
-    size_t k = 0;
-    for (int q = 0; q < n_prn; ++q)
+    timed(ctx, "nc_reduce", 0.0, [&] { return launch_nc_reduce(cd, (tc ? d_keys32 : d_keys) + r0, cbest, st); });
+    timed(ctx, "nc_second", (double)na * n_prn * B * row,
+          [&] { return launch_nc_second(pc, cd, B, d_z, d_D, cbest, chip_width_of(fs), ctx->num_sms, st); });
+  }
+  std::vector<BestRow> best((size_t)n_ant * n_prn);
+  CK(cudaMemcpyAsync(best.data(), d_best, best.size() * sizeof(BestRow), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  ctx->d2h += best.size() * sizeof(BestRow);
+  check_tc_error(ctx);
+  ctx->last_cells += (double)n_ant * nb * n_prn * (double)P * B;
+  // |y| of the polyphase correlator is Lc |r|; report (|r| sqrt(N))^2 per block
+  const double scale = (double)opt->coherent_periods * (double)P / ((double)pc.Lc * (double)pc.Lc);
+  tga_ctx::LastGroup lg;
+  lg.Lc = pc.Lc;
+  lg.P = pc.P;
+  lg.n_ant = n_ant;
+  lg.nb = nb;
+  lg.n_prn = n_prn;
+  lg.tc = tc;
+  lg.amp = tc ? tc_key_amplitude(pc) : 1.0;
+  lg.keys = d_keys;
+  lg.count = d_count;
+  lg.n_chunks = n_chunks;
+  lg.nc_power_scale = scale;
+  ctx->last_groups.push_back(lg);
+  // each member's cells in (PRN, antenna) order
+  int q0 = 0;
+  for (const NcMember* m : mem) {
+    size_t k = m->out_off;
+    for (size_t qi = 0; qi < m->prns.size(); ++qi)
       for (int a = 0; a < n_ant; ++a, ++k) {
-        const BestRow& r = best[(size_t)a * n_prn + q];
+        const BestRow& r = best[(size_t)a * n_prn + q0 + qi];
         tga_nc_cell& o = out[k];
         std::memset(&o, 0, sizeof o);
-        o.prn = prn_list[q];
+        o.prn = m->prns[qi];
         o.antenna = ants[a];
-        o.best_freq_idx = r.ab - a * nb;
+        o.best_freq_idx = r.ab % nb;  // r.ab counts antennas within the chunk
         o.best_codephase = r.tau;
         o.power = (double)r.p * scale;
         o.second_power = (double)r.p2 * scale;
         o.frequency = fc[o.best_freq_idx] - opt->center_freq;
       }
-    return TGA_OK;
-  });
+    q0 += (int)m->prns.size();
+  }
+}
+
+int nc_search(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant_total, size_t row_bytes, double fs,
+              const tga_nc_options* opts, size_t n_opts, tga_nc_cell* out, size_t cap, size_t* n_out) {
+  if (!h_bits || !opts || !n_out || n_opts == 0 || n_ant_total == 0 || row_bytes == 0 || !(fs > 0))
+    throw InvalidArg("bad arguments");
+  std::vector<NcMember> mem;
+  size_t n_cells = 0;
+  for (size_t i = 0; i < n_opts; ++i) {
+    try {
+      mem.push_back(nc_member(ctx, &opts[i], n_ant_total, row_bytes, fs));
+    } catch (const std::domain_error&) {
+      return TGA_ERR_UNSUPPORTED;
+    }
+    mem.back().out_off = n_cells;
+    n_cells += mem.back().ants.size() * mem.back().prns.size();
+  }
+  *n_out = n_cells;
+  if (!out) return TGA_OK;
+  if (cap < n_cells) return TGA_ERR_CAPACITY;
+  begin_call(ctx);
+  ctx->last_groups.clear();
+  cudaStream_t st = ctx->stream;
+  uint8_t* d_bits = (uint8_t*)ctx->buf("nc.bits", n_ant_total * row_bytes);
+  CK(cudaMemcpyAsync(d_bits, h_bits, n_ant_total * row_bytes, cudaMemcpyHostToDevice, st));
+  ctx->h2d += n_ant_total * row_bytes;
+  double* d_mean = (double*)ctx->buf("nc.mean", n_ant_total * sizeof(double));
+  CK(launch_antenna_means(d_bits, (int)n_ant_total, row_bytes, d_mean, st));
+  // members sharing a front end run together, in the order of their first member
+  std::vector<bool> done(mem.size(), false);
+  int gi = 0;
+  for (size_t i = 0; i < mem.size(); ++i) {
+    if (done[i]) continue;
+    std::vector<NcMember*> grp{&mem[i]};
+    done[i] = true;
+    for (size_t j = i + 1; j < mem.size(); ++j)
+      if (!done[j] && nc_same_group(mem[i], mem[j])) {
+        grp.push_back(&mem[j]);
+        done[j] = true;
+      }
+    nc_run_group(ctx, d_bits, row_bytes, d_mean, fs, grp, gi++, out);
+  }
+  collect_times(ctx);
+  return TGA_OK;
+}
+
+}  // namespace
+
+int tga_search_noncoherent(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant_total, size_t row_bytes, double fs,
+                           const tga_nc_options* opt, tga_nc_cell* out, size_t cap, size_t* n_out) {
+  return guarded(ctx, [&] { return nc_search(ctx, h_bits, n_ant_total, row_bytes, fs, opt, 1, out, cap, n_out); });
+}
+
+int tga_search_noncoherent_multi(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant_total, size_t row_bytes,
+                                 double fs, const tga_nc_options* opts, size_t n_opts, tga_nc_cell* out, size_t cap,
+                                 size_t* n_out) {
+  return guarded(ctx, [&] { return nc_search(ctx, h_bits, n_ant_total, row_bytes, fs, opts, n_opts, out, cap, n_out); });
 }
 
 // ---------------------------------------------------------------------------

@@ -28,6 +28,8 @@ LIB_PATH = os.path.join(HERE, "libtga.so")
 
 GPS, GALILEO, BEIDOU, SBAS, L1C, QZSS = range(6)
 NAMES = ["gps", "galileo", "beidou", "sbas", "l1c", "qzss"]
+# PRN range of each constellation, in constellation order
+PRN_RANGE = [(1, 38), (1, 50), (1, 63), (120, 158), (1, 63), (184, 206)]
 ALL = 0x3F
 GPS_IF = 4.092e6
 GPS_SEARCH_BAND = 6000.0
@@ -176,6 +178,7 @@ def lib():
     L.tga_set_test_flags.argtypes = [_P, i32]
     L.tga_rfi_scan.argtypes = [_P, _P, sz, sz, dbl, _P]
     L.tga_search_noncoherent.argtypes = [_P, _P, sz, sz, dbl, _P, _P, sz, _P]
+    L.tga_search_noncoherent_multi.argtypes = [_P, _P, sz, sz, dbl, _P, sz, _P, sz, _P]
     L.tga_results_json.argtypes = [_P, sz, _P, sz, ctypes.c_uint32, i32, dbl, dbl, _P, _P]
     L.tga_observation_read_hdf5.argtypes = [ctypes.c_char_p, _P]
     L.tga_observation_free.argtypes = [_P]
@@ -186,6 +189,7 @@ def lib():
     L.tga_acquire_single_static.argtypes = [i32, _P, _P, sz, dbl, dbl, dbl, i32, sz, _P, _P]
     L.tga_last_transfer_bytes.argtypes = [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.tga_kernel_times.argtypes = [_P, i32, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_int)]
+    L.tga_last_row_peaks.argtypes = [_P, i32, _P, sz, ctypes.POINTER(sz), ctypes.POINTER(ctypes.c_int64)]
     _lib = L
     return L
 
@@ -400,6 +404,18 @@ class Context:
             out[NAMES[c]] = {"antenna_numbers": ants, "results": results}
         return out
 
+    def row_peaks(self, chips):
+        """Row peaks of the last acquire_cells call for its group of `chips`-chip
+        codes as the search's arithmetic computed them (tga_last_row_peaks):
+        array [n_ant, n_bins, 2 hypotheses, n_prn] in signal_strength units,
+        and the number of rows the tensor-core search re-evaluated in FP32."""
+        n = ctypes.c_size_t()
+        refined = ctypes.c_int64()
+        self._check(lib().tga_last_row_peaks(self._h, int(chips), None, 0, ctypes.byref(n), ctypes.byref(refined)))
+        out = np.zeros(n.value, dtype=np.float64)
+        self._check(lib().tga_last_row_peaks(self._h, int(chips), _ptr(out), len(out), ctypes.byref(n), None))
+        return out, int(refined.value)
+
     def set_test_flags(self, flags):
         """Test hooks (TGA_TEST_*); 0 in normal use."""
         self._check(lib().tga_set_test_flags(self._h, int(flags)))
@@ -540,6 +556,43 @@ class Context:
                                                  float(sampling_freq), ctypes.byref(o), _ptr(out), len(out),
                                                  ctypes.byref(n)))
         return out
+
+    def search_noncoherent_multi(self, packed_bits, sampling_freq, searches):
+        """Several non-coherent searches of one recording in one call
+        (tga_search_noncoherent_multi).  searches: list of dicts with the
+        keyword arguments of search_noncoherent plus `constellation`.  Returns
+        one record array per search, in order."""
+        bits = np.ascontiguousarray(packed_bits, dtype=np.uint8)
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        keep, opts = [], (NcOptions * len(searches))()
+        for i, sd in enumerate(searches):
+            pr = sd.get("prns")
+            an = sd.get("ants")
+            pr = None if pr is None else np.ascontiguousarray(pr, dtype=np.int32)
+            an = None if an is None else np.ascontiguousarray(an, dtype=np.int32)
+            keep += [pr, an]
+            opts[i] = NcOptions(int(sd["constellation"]), None if pr is None else pr.ctypes.data_as(i32p),
+                                0 if pr is None else len(pr), None if an is None else an.ctypes.data_as(i32p),
+                                0 if an is None else len(an), float(sd.get("center_freq", GPS_IF)),
+                                float(sd.get("bin_step_hz", 500.0)), int(sd.get("n_bins", 21)),
+                                int(sd.get("coherent_periods", 1)), int(sd.get("blocks", 10)), int(sd.get("start", 0)))
+        n = ctypes.c_size_t()
+        self._check(lib().tga_search_noncoherent_multi(self._h, _ptr(bits), bits.shape[0], bits.shape[1],
+                                                       float(sampling_freq), opts, len(searches), None, 0,
+                                                       ctypes.byref(n)))
+        out = np.zeros(n.value, dtype=NC_CELL_DTYPE)
+        self._check(lib().tga_search_noncoherent_multi(self._h, _ptr(bits), bits.shape[0], bits.shape[1],
+                                                       float(sampling_freq), opts, len(searches), _ptr(out), len(out),
+                                                       ctypes.byref(n)))
+        del keep
+        res, k = [], 0
+        for sd in searches:
+            n_ant = bits.shape[0] if sd.get("ants") is None else len(sd["ants"])
+            n_prn = len(sd["prns"]) if sd.get("prns") is not None else PRN_RANGE[int(sd["constellation"])][1] - \
+                PRN_RANGE[int(sd["constellation"])][0] + 1
+            res.append(out[k:k + n_ant * n_prn])
+            k += n_ant * n_prn
+        return res
 
     def acr_table(self, constellation, prn=1, sampling_freq=16.368e6, cn0_lo=33.0, cn0_hi=62.0, cn0_step=0.5,
                   trials=100):

@@ -77,3 +77,31 @@ def test_single_two_period_block_matches_dropin(ctx):
     assert d["hypothesis"] == 0
     assert g["best_codephase"] == d["best_codephase"] % P and g["best_freq_idx"] == d["best_freq_idx"]
     assert abs(g["power"] - d["signal_strength"] ** 2) <= 2 * REL_TOL * g["power"]
+
+
+def test_multi_call_equals_single_calls(ctx):
+    """tga_search_noncoherent_multi: GPS and SBAS (one shared front end),
+    Galileo with its own blocks and grid, in one call, equal to the three
+    searches run one by one, in both arithmetics."""
+    P = 16368
+    sats = [(O.GPS, 6, 4000, 900.0, 44.0), (O.SBAS, 127, 123, -1400.0, 44.0), (O.GALILEO, 8, 30000, 375.0, 44.0)]
+    bits = synth(sats, 8 * P, seed=71, n_ant=2)
+    searches = [dict(constellation=tga.GPS, prns=[6, 9], bin_step_hz=500.0, n_bins=21, coherent_periods=1, blocks=8),
+                dict(constellation=tga.SBAS, prns=[127, 140], bin_step_hz=500.0, n_bins=21, coherent_periods=1,
+                     blocks=8),
+                dict(constellation=tga.GALILEO, prns=[8, 2], bin_step_hz=125.0, n_bins=41, coherent_periods=1,
+                     blocks=2)]
+    for prec in (tga.PRECISION_FP32, tga.PRECISION_FP16_TC):
+        ctx.set_precision(prec)
+        try:
+            multi = ctx.search_noncoherent_multi(bits, FS, searches)
+            for sd, m in zip(searches, multi):
+                kw = {k: v for k, v in sd.items() if k != "constellation"}
+                one = ctx.search_noncoherent(bits, FS, sd["constellation"], **kw)
+                for k in ("prn", "antenna", "best_freq_idx", "best_codephase", "power", "second_power", "frequency"):
+                    np.testing.assert_array_equal(m[k], one[k], err_msg=k)
+        finally:
+            ctx.set_precision(tga.PRECISION_FP32)
+    assert multi[0]["best_codephase"][0] == (P - 4000) % P
+    assert multi[1]["best_codephase"][0] == (P - 123) % P
+    assert multi[2]["best_codephase"][0] == (4 * P - 30000) % (4 * P)
