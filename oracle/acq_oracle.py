@@ -71,8 +71,33 @@ def lib():
         L.oracle_b1cp_bits.argtypes = [ctypes.c_int, ctypes.c_char_p]
         L.oracle_l1cp_bits.argtypes = [ctypes.c_int, ctypes.c_char_p]
         L.oracle_ca_from_delay.argtypes = [ctypes.c_int, dp]
+        _load_tables(L)
         _lib = L
     return _lib
+
+
+TABLES = os.path.join(os.path.dirname(HERE), "tests", "golden", "tables.json")
+
+
+def tables():
+    """The oracle's own copy of the reference's data tables (read from its
+    sources by tests/golden/make_golden.py)."""
+    import json
+    with open(TABLES) as f:
+        return json.load(f)
+
+
+def _load_tables(L):
+    t = tables()
+    ip = lambda v: (ctypes.c_int * len(v))(*v)
+    L.oracle_set_ca_delays(ip(t["gps_g2_delay"]), ip(t["sbas_g2_delay"]), ip(t["qzss_g2_delay"]))
+    L.oracle_set_weil(ip([x for p in t["b1cp_weil_wp"] for x in p]), ip([x for p in t["l1cp_weil_wp"] for x in p]))
+    for i, h in enumerate(t["galileo_e1c_hex"]):
+        L.oracle_set_e1c_hex(i + 1, h.encode())
+    for tid, key in enumerate(("acr_gps_l1_ca", "acr_galileo_e1c", "acr_beidou_b1c", "acr_gps_l1c")):
+        rows = [x for p in t[key] for x in p]
+        if not L.oracle_set_acr(tid, (ctypes.c_double * len(rows))(*rows), len(t[key])):
+            raise ValueError("ACR table %s does not fit the oracle" % key)
 
 
 def _dp(a):

@@ -12,14 +12,44 @@
  *
  * Written in the reference's own bipolar formulation (values +-1 multiplied
  * together) on purpose, so that it is independent of the product's bitwise
- * LFSR code in tart-gnss_b200/csrc/codes.cpp.
+ * LFSR code in tart-gnss_b200/csrc/codes.cpp.  Its data tables (G2 delays,
+ * Weil parameters, Galileo hex codes, ACR tables) are its own copy, read
+ * from the reference sources into tests/golden/tables.json and handed over
+ * by acq_oracle.py through the oracle_set_* calls below before any use; the
+ * product's generated header is not included.
  */
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
-#include "../tart-gnss_b200/csrc/gnss_tables.h"
+/* ---- tables (set once by the loader) -------------------------------------- */
+static int g_gps_g2[38], g_sbas_g2[39], g_qzss_g2[23];
+static int g_b1cp_wp[63][2], g_l1cp_wp[63][2];
+static char g_e1c_hex[50][1024];
+static double g_acr[4][128][2];
+static int g_acr_n[4];
+
+void oracle_set_ca_delays(const int* gps /*38*/, const int* sbas /*39*/, const int* qzss /*23*/) {
+  memcpy(g_gps_g2, gps, sizeof g_gps_g2);
+  memcpy(g_sbas_g2, sbas, sizeof g_sbas_g2);
+  memcpy(g_qzss_g2, qzss, sizeof g_qzss_g2);
+}
+void oracle_set_weil(const int* b1cp /*63 x 2*/, const int* l1cp /*63 x 2*/) {
+  memcpy(g_b1cp_wp, b1cp, sizeof g_b1cp_wp);
+  memcpy(g_l1cp_wp, l1cp, sizeof g_l1cp_wp);
+}
+void oracle_set_e1c_hex(int prn, const char* hex /*1023 digits*/) {
+  memcpy(g_e1c_hex[prn - 1], hex, 1023);
+  g_e1c_hex[prn - 1][1023] = 0;
+}
+/* Returns 0 when the table does not fit. */
+int oracle_set_acr(int id, const double* rows /*n x 2*/, int n) {
+  if (id < 0 || id > 3 || n < 1 || n > 128) return 0;
+  memcpy(g_acr[id], rows, (size_t)n * 2 * sizeof(double));
+  g_acr_n[id] = n;
+  return 1;
+}
 
 /* ---- C/A Gold codes: acquisition.rs:96-125 ------------------------------- */
 void oracle_ca_from_delay(int g2shift, double* out /*1023*/) {
@@ -57,7 +87,7 @@ static void legendre(int n, unsigned char* seq) {
 
 void oracle_b1cp_bits(int prn, unsigned char* out /*10230*/) {
   static unsigned char L[10243];
-  int n, w = TGA_B1CP_WP[prn - 1][0], p = TGA_B1CP_WP[prn - 1][1];
+  int n, w = g_b1cp_wp[prn - 1][0], p = g_b1cp_wp[prn - 1][1];
   legendre(10243, L);
   for (n = 0; n < 10230; ++n) {
     int k = (n + p - 1) % 10243;
@@ -68,7 +98,7 @@ void oracle_b1cp_bits(int prn, unsigned char* out /*10230*/) {
 void oracle_l1cp_bits(int prn, unsigned char* out /*10230*/) {
   static unsigned char L[10223], W[10223];
   static const unsigned char ex[7] = {0, 1, 1, 0, 1, 0, 0};
-  int k, o = 0, w = TGA_L1CP_WP[prn - 1][0], p = TGA_L1CP_WP[prn - 1][1];
+  int k, o = 0, w = g_l1cp_wp[prn - 1][0], p = g_l1cp_wp[prn - 1][1];
   legendre(10223, L);
   for (k = 0; k < 10223; ++k) W[k] = L[k] ^ L[(k + w) % 10223];
   for (k = 0; k < p - 1; ++k) out[o++] = W[k];
@@ -78,7 +108,7 @@ void oracle_l1cp_bits(int prn, unsigned char* out /*10230*/) {
 
 /* ---- Galileo hex decode: galileo.rs:82-94 -------------------------------- */
 void oracle_e1c_chips(int prn, double* out /*4092*/) {
-  const char* hex = TGA_GALILEO_E1C_HEX[prn - 1];
+  const char* hex = g_e1c_hex[prn - 1];
   int i, bit;
   for (i = 0; i < 1023; ++i) {
     char c = hex[i];
@@ -98,15 +128,15 @@ int oracle_base_sequence(int constellation, int prn, double* out /*>=20460*/) {
   switch (constellation) {
     case 0:
       if (prn < 1 || prn > 38) return 0;
-      oracle_ca_from_delay(TGA_GPS_G2_DELAY[prn - 1], out);
+      oracle_ca_from_delay(g_gps_g2[prn - 1], out);
       return 1023;
     case 3:
       if (prn < 120 || prn > 158) return 0;
-      oracle_ca_from_delay(TGA_SBAS_G2_DELAY[prn - 120], out);
+      oracle_ca_from_delay(g_sbas_g2[prn - 120], out);
       return 1023;
     case 5:
       if (prn < 184 || prn > 206) return 0;
-      oracle_ca_from_delay(TGA_QZSS_G2_DELAY[prn - 184], out);
+      oracle_ca_from_delay(g_qzss_g2[prn - 184], out);
       return 1023;
     case 1:
       if (prn < 1 || prn > 50) return 0;
@@ -145,14 +175,12 @@ int oracle_resampled(int constellation, int prn, double samples_per_code, size_t
 
 /* ---- ACR: acr.rs:49-84 ---------------------------------------------------- */
 static const double (*acr_table(int id, int* n))[2] {
-  switch (id) {
-    case 0: *n = 59; return TGA_GPS_L1_CA_ACR_TABLE;
-    case 1: *n = 71; return TGA_GALILEO_E1C_ACR_TABLE;
-    case 2: *n = 79; return TGA_BEIDOU_B1C_ACR_TABLE;
-    case 3: *n = 79; return TGA_GPS_L1C_ACR_TABLE;
+  if (id < 0 || id > 3 || g_acr_n[id] == 0) {
+    *n = 0;
+    return 0;
   }
-  *n = 0;
-  return 0;
+  *n = g_acr_n[id];
+  return (const double(*)[2])g_acr[id];
 }
 
 int oracle_acr_table(int id, double* out, int cap) {

@@ -17,7 +17,7 @@ data (interface-control-document tables) or calibration data, not code:
 Numbers are copied as the decimal strings written in the reference, so the
 C compiler rounds them to exactly the same IEEE doubles as rustc does.
 
-Usage:  python gen_tables.py [reference_src_dir]   (default /root/reference/src)
+Usage:  python gen_tables.py <reference_src_dir>
 The generated header is committed; this script only needs re-running if the
 reference tables change.
 """
@@ -74,6 +74,7 @@ def main(src):
     w = L.append
     w("/* Generated by gen_tables.py from the tart-gnss-acquire v0.4.0 sources. Do not edit. */")
     w("/* Signal-definition (ICD) and ACR calibration tables; see gen_tables.py for provenance. */")
+    w("/* The values come from tart-gnss (tmolteno/tart-gnss), licensed GPL-3.0 (its Cargo.toml). */")
     w("#pragma once")
     w("#include <stdint.h>")
     w("")
@@ -107,4 +108,6 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) != 2:
+        sys.exit("usage: gen_tables.py <reference_src_dir>")
+    main(sys.argv[1])

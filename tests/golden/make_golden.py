@@ -2,7 +2,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference crate.
 
 Run in the build container (where the reference checkout exists):
-    python tests/golden/make_golden.py [/path/to/tart-gnss]
+    python tests/golden/make_golden.py /path/to/tart-gnss
 
 Outputs (committed; the GPU box never reads the reference):
 * kats.json -- known-answer vectors copied from the reference's own unit
@@ -11,6 +11,17 @@ Outputs (committed; the GPU box never reads the reference):
   (src/l1c_codes.rs:256-289), SBAS first 10 chips (src/sbas.rs:436-442),
   QZSS first 10 chips (src/qzss.rs:437-441), and the ACR mid-range points
   (src/acr.rs:150-154).
+* tables.json -- the oracle's own copy of the reference's data tables,
+  read straight from its sources (the oracle does not use the product's
+  generated header): G2 delays of GPS PRN 1-38 (src/acquisition.rs:84-87),
+  SBAS 120-158 (src/sbas.rs:39-44) and QZSS 184-206 (src/qzss.rs:40-44);
+  Weil (w, p) of the BeiDou B1C (src/beidou_codes.rs:46-63) and GPS L1C
+  (src/l1c_codes.rs:45-62) pilots; the 50 Galileo E1-C hex codes
+  (src/galileo_codes.rs:20-70); the four ACR tables (src/acr_tables.rs);
+  and the IS-GPS-200 table of the first 10 C/A chips in octal for PRN 1-32
+  (the ICD's known-answer column; the reference has no such test).
+  The tables come from tart-gnss, GPL-3.0 (Cargo.toml:7), as signal
+  definitions and calibration data.
 * tart_head.npz -- the reference's real 24-antenna TART recording
   (data/data_2026-03-09_04_25_10.145497.hdf), reduced to what the
   acquisition search reads: per antenna the count of one-bits over the
@@ -59,6 +70,7 @@ def main(ref):
     assert len(kats["sbas_first10"]) == 39 and len(kats["qzss_first10"]) == 23
     with open(os.path.join(HERE, "kats.json"), "w") as f:
         json.dump(kats, f, indent=1)
+    write_tables(extract_tables(src))
 
     hdf = os.path.join(ref, "data", "data_2026-03-09_04_25_10.145497.hdf")
     raw = open(hdf, "rb").read()
@@ -77,6 +89,58 @@ def main(ref):
                         timestamp=np.bytes_(b"2026-03-09T04:25:10.145497+00:00"))
     write_hdf5_fixture(raw, block, n_ant, row_bytes, off)
     print("wrote kats.json, tart_head.npz and tart_head4096.hdf", ones[:4], off)
+
+
+# IS-GPS-200 Table 3-Ia, "First 10 Chips (Octal)" of the C/A code, PRN 1-32
+# (chip 1 first, MSB; a chip of logic 1 is a 1 bit)
+CA_FIRST10_OCTAL = [
+    "1440", "1620", "1710", "1744", "1133", "1455", "1131", "1454", "1626", "1504", "1642", "1750", "1764", "1772",
+    "1775", "1776", "1156", "1467", "1633", "1715", "1746", "1763", "1063", "1706", "1743", "1761", "1770", "1774",
+    "1127", "1453", "1625", "1712"]
+
+
+def _array_body(text, name):
+    """The text between the opening '[' of the array literal assigned to
+    `name` and its closing '];' (comments removed)."""
+    i = text.index(name)
+    i = text.index("=", i)
+    j = text.index("[", i)
+    k = text.index("];", j)
+    return re.sub(r"//[^\n]*", "", text[j + 1:k])
+
+
+def extract_tables(src):
+    rd = lambda f: open(os.path.join(src, f)).read()
+    ints = lambda body: [int(x) for x in re.findall(r"-?\d+", body)]
+    pairs = lambda body: [[int(a), int(b)] for a, b in re.findall(r"\(\s*(\d+)\s*,\s*(\d+)\s*\)", body)]
+    fpairs = lambda body: [[float(a), float(b)] for a, b in
+                           re.findall(r"\(\s*([-+0-9.eE]+)\s*,\s*([-+0-9.eE]+)\s*\)", body)]
+    t = {
+        "gps_g2_delay": ints(_array_body(rd("acquisition.rs"), "CODE_DELAY_TABLE")),
+        "sbas_g2_delay": ints(_array_body(rd("sbas.rs"), "CODE_DELAY_TABLE")),
+        "qzss_g2_delay": ints(_array_body(rd("qzss.rs"), "CODE_DELAY_TABLE")),
+        "b1cp_weil_wp": pairs(_array_body(rd("beidou_codes.rs"), "B1CP_PARAMS")),
+        "l1cp_weil_wp": pairs(_array_body(rd("l1c_codes.rs"), "L1CP_PARAMS")),
+        "galileo_e1c_hex": re.findall(r'"([0-9A-Fa-f]{1023})"', rd("galileo_codes.rs")),
+        "ca_first10_octal": CA_FIRST10_OCTAL,
+    }
+    acr = rd("acr_tables.rs")
+    for key, name in (("acr_gps_l1_ca", "GPS_L1_CA_ACR_TABLE"), ("acr_galileo_e1c", "GALILEO_E1C_ACR_TABLE"),
+                      ("acr_beidou_b1c", "BEIDOU_B1C_ACR_TABLE"), ("acr_gps_l1c", "GPS_L1C_ACR_TABLE")):
+        t[key] = fpairs(_array_body(acr, "static " + name))
+    sizes = {k: len(v) for k, v in t.items()}
+    assert sizes == {"gps_g2_delay": 38, "sbas_g2_delay": 39, "qzss_g2_delay": 23, "b1cp_weil_wp": 63,
+                     "l1cp_weil_wp": 63, "galileo_e1c_hex": 50, "ca_first10_octal": 32, "acr_gps_l1_ca": 59,
+                     "acr_galileo_e1c": 71, "acr_beidou_b1c": 79, "acr_gps_l1c": 79}, sizes
+    t["provenance"] = ("tart-gnss-acquire v0.4.0 sources (GPL-3.0): signal-definition and calibration tables; "
+                       "IS-GPS-200 Table 3-Ia first-10-chip octal column")
+    return t
+
+
+def write_tables(t):
+    """tables.json with one table per line."""
+    with open(os.path.join(HERE, "tables.json"), "w") as f:
+        f.write("{\n" + ",\n".join("%s: %s" % (json.dumps(k), json.dumps(v)) for k, v in t.items()) + "\n}\n")
 
 
 # byte offsets, inside the first 6176 bytes of the reference file, of the
@@ -102,4 +166,6 @@ def write_hdf5_fixture(raw, block, n_ant, row_bytes, off):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py /path/to/tart-gnss")
+    main(sys.argv[1])

@@ -149,3 +149,50 @@ def test_real_fixture_shape(golden_dir):
     assert float(z["sampling_frequency"]) == 16368000.0
     frac = z["ones"] / (int(z["row_bytes"]) * 8.0)
     assert np.all((frac > 0.44) & (frac < 0.56))
+
+
+def test_gps_ca_first10_octal_is_gps_200():
+    # IS-GPS-200 Table 3-Ia, first 10 chips of the C/A code in octal, PRN 1-32
+    # (tables.json; the reference has no such test).  The table counts a chip
+    # of logic 1 as a 1 bit, and the reference's bipolar C/A chip is +1 for
+    # logic 1 (acquisition.rs:96-125: registers start at -1 = logic 1, chip =
+    # -(g1 g2)), so +1 -> 1 here -- the complement of the mapping the
+    # reference's SBAS / QZSS octal tests use for their tables.
+    want = O.tables()["ca_first10_octal"]
+    for prn in range(1, 33):
+        c = O.base_sequence(O.GPS, prn)[:10]
+        assert chips10_to_octal(-c) == want[prn - 1], prn
+
+
+def _header_tables():
+    """The product's generated table header, parsed as text."""
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    h = open(os.path.join(root, "tart-gnss_b200", "csrc", "gnss_tables.h")).read()
+
+    def body(name):
+        i = h.index(name)
+        return h[h.index("{", i) + 1:h.index("};", i)]
+    ints = lambda b: [int(x) for x in re.findall(r"-?\d+", b)]
+    out = {"gps_g2_delay": ints(body("TGA_GPS_G2_DELAY")), "sbas_g2_delay": ints(body("TGA_SBAS_G2_DELAY")),
+           "qzss_g2_delay": ints(body("TGA_QZSS_G2_DELAY")),
+           "galileo_e1c_hex": re.findall(r'"([0-9A-F]{1023})"', body("TGA_GALILEO_E1C_HEX"))}
+    for key, name in (("b1cp_weil_wp", "TGA_B1CP_WP"), ("l1cp_weil_wp", "TGA_L1CP_WP")):
+        v = ints(body(name + "[63][2]"))
+        out[key] = [v[2 * i:2 * i + 2] for i in range(len(v) // 2)]
+    for key, name in (("acr_gps_l1_ca", "TGA_GPS_L1_CA_ACR_TABLE"), ("acr_galileo_e1c", "TGA_GALILEO_E1C_ACR_TABLE"),
+                      ("acr_beidou_b1c", "TGA_BEIDOU_B1C_ACR_TABLE"), ("acr_gps_l1c", "TGA_GPS_L1C_ACR_TABLE")):
+        v = [float(x) for x in re.findall(r"[-+0-9.eE]+", body(name + "["))]
+        out[key] = [v[2 * i:2 * i + 2] for i in range(len(v) // 2)]
+    return out
+
+
+def test_oracle_tables_equal_product_header():
+    """The oracle's tables (tests/golden/tables.json, read from the reference
+    sources) and the product's generated header hold the same values, so a
+    transcription error in either shows up here rather than passing every
+    parity test on both sides."""
+    mine, theirs = O.tables(), _header_tables()
+    for key, v in theirs.items():
+        want = mine[key] if key != "galileo_e1c_hex" else [x.upper() for x in mine[key]]
+        assert v == want, key
