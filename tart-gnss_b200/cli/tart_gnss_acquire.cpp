@@ -7,6 +7,20 @@
 // (main.rs:482-694) and the RFI report --rfi (main.rs:439-478, rfi.rs).
 // Modes outside these (--simulate, --test-antennas) are reported as
 // unsupported.  Errors exit with status 1 like the reference.
+//
+// Flags of this engine beyond the reference's, each off by default so the
+// default run is the reference's search:
+//   --precision fp32|fp16tc   arithmetic of the search transforms (fp32);
+//   --coherent-periods K, --noncoh B
+//                             non-coherent search: B coherent blocks of K code
+//                             periods summed in power (default: the
+//                             reference's single two-period window);
+//   --bin-hz H                Doppler bin width of the non-coherent search
+//                             (default 1 / (2 K T), T the code period);
+//   --refine                  fine acquisition of every detected satellite
+//                             (joint Newton refinement of delay, Doppler and
+//                             per-antenna phase), added as "refined".
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -32,6 +46,11 @@ struct Args {
        simulate = false;
   bool has_min_cn0 = false;
   double min_cn0 = 44.0;
+  // extensions (see the header comment)
+  int precision = TGA_PRECISION_FP32;
+  bool nc = false, refine = false;
+  long coherent_periods = 1, blocks = 1;
+  double bin_hz = NAN;
 };
 
 [[noreturn]] void die(const std::string& msg, const char* prog, bool usage) {
@@ -41,7 +60,8 @@ struct Args {
                  "usage: %s --file <observation.hdf> [--i <i> --j <j>] [--all] [--gps] [--galileo] [--beidou] "
                  "[--sbas] [--l1c] [--qzss] [--cn0] [--test-antennas] [--test-min-cn0 <x>] [--rfi] [--prn <a,b,...>] "
                  "[--ant <a,b,...>] [--filter-phase-mad <x>] [--filter-freq-mad <x>] [--output <path>] [--debug] "
-                 "[--benchmark]\n",
+                 "[--benchmark] [--precision <fp32|fp16tc>] [--coherent-periods <K>] [--noncoh <B>] [--bin-hz <H>] "
+                 "[--refine]\n",
                  prog);
   std::exit(1);
 }
@@ -110,6 +130,16 @@ Args parse_args(int argc, char** argv) {
     else if (s == "--version") a.version = true;
     else if (s == "--rfi") a.rfi = true;
     else if (s == "--simulate") a.simulate = true;
+    else if (s == "--precision") {
+      const std::string v = val(k, "--precision");
+      if (v == "fp32") a.precision = TGA_PRECISION_FP32;
+      else if (v == "fp16tc") a.precision = TGA_PRECISION_FP16_TC;
+      else die("invalid value for --precision: " + v + " (fp32 or fp16tc)", prog, true);
+    }
+    else if (s == "--coherent-periods") { std::string v = val(k, s.c_str()); if (!parse_int(v, &a.coherent_periods) || a.coherent_periods < 1) die("invalid positive integer for --coherent-periods: " + v, prog, true); a.nc = true; }
+    else if (s == "--noncoh") { std::string v = val(k, s.c_str()); if (!parse_int(v, &a.blocks) || a.blocks < 1) die("invalid positive integer for --noncoh: " + v, prog, true); a.nc = true; }
+    else if (s == "--bin-hz") { std::string v = val(k, s.c_str()); if (!parse_f64(v, &a.bin_hz) || !(a.bin_hz > 0)) die("invalid positive float for --bin-hz: " + v, prog, true); }
+    else if (s == "--refine") a.refine = true;
     else if (s == "--sources" || s == "--positions" || s == "--N" || s == "--diameter" || s == "--seed" ||
              s == "--sample-rate" || s == "--center-freq" || s == "--band" || s == "--snr") (void)val(k, s.c_str());
     else die("unknown argument: " + s, prog, true);
@@ -122,6 +152,13 @@ Args parse_args(int argc, char** argv) {
     if (!(a.gps || a.galileo || a.beidou || a.sbas || a.l1c || a.qzss))
       a.gps = a.galileo = a.beidou = a.sbas = a.l1c = a.qzss = true;
   }
+  if (!std::isnan(a.bin_hz) && !a.nc)
+    die("--bin-hz sets the non-coherent search's grid: give --noncoh or --coherent-periods (the reference's "
+        "two-period search keeps its 300 Hz grid)", prog, true);
+  if (a.nc && (a.benchmark || a.rfi || a.test_antennas))
+    die("--noncoh / --coherent-periods apply to the acquisition search only", prog, true);
+  if (a.refine && (a.benchmark || a.rfi || a.test_antennas))
+    die("--refine applies to the acquisition search only", prog, true);
   if (a.rfi) {
     if (a.benchmark) die("--rfi cannot be combined with --benchmark", prog, true);
     if (a.test_antennas) die("--rfi cannot be combined with --test-antennas", prog, true);
@@ -147,6 +184,99 @@ void write_out(const std::string& json, const std::string& path, const char* wha
 
 const char* kNames[6] = {"GPS L1 C/A", "Galileo E1-C", "BeiDou B1C", "SBAS L1 C/A", "GPS L1C", "QZSS L1 C/A"};
 const int kNumPrns[6] = {38, 50, 63, 39, 63, 23};
+const int kFirstPrn[6] = {1, 1, 1, 120, 1, 184};
+// CombinedOutput field order (lib.rs:32-45) and sv labels (acquisition.rs:351 and twins)
+const int kJsonOrder[6] = {TGA_GPS, TGA_GALILEO, TGA_BEIDOU, TGA_SBAS, TGA_L1C, TGA_QZSS};
+const char* kJsonKey[6] = {"gps", "galileo", "beidou", "sbas", "l1c", "qzss"};
+const double kPeriodS[6] = {0.001, 0.004, 0.010, 0.001, 0.010, 0.001};
+
+std::string sv_label(int c, int prn) {
+  char b[32];
+  switch (c) {
+    case TGA_GPS: std::snprintf(b, sizeof b, "GPS%02d", prn); break;
+    case TGA_GALILEO: std::snprintf(b, sizeof b, "GSAT%02d", prn); break;
+    case TGA_BEIDOU: std::snprintf(b, sizeof b, "BEIDOU%02d", prn); break;
+    case TGA_SBAS: std::snprintf(b, sizeof b, "SBAS%03d", prn); break;
+    case TGA_L1C: std::snprintf(b, sizeof b, "GPSL1C%02d", prn); break;
+    default: std::snprintf(b, sizeof b, "QZSS%03d", prn); break;
+  }
+  return b;
+}
+
+// samples per code period (the library's rule: fs / 1000 for the 1 ms codes)
+size_t period_of(int c, double fs) {
+  const double v = kPeriodS[c] == 0.001 ? fs / 1000.0 : fs * kPeriodS[c];
+  return v > 0 ? (size_t)v : 0;
+}
+
+std::string num(double v) {
+  char b[64];
+  tga_format_f64(v, b, sizeof b);
+  return b;
+}
+
+void arr(std::string& s, const std::vector<double>& v, int lvl) {
+  if (v.empty()) {
+    s += "[]";
+    return;
+  }
+  s += "[\n";
+  for (size_t i = 0; i < v.size(); ++i)
+    s += std::string(2 * (lvl + 1), ' ') + num(v[i]) + (i + 1 < v.size() ? ",\n" : "\n");
+  s += std::string(2 * lvl, ' ') + "]";
+}
+
+// One satellite to refine: the grid estimate of its strongest antenna.
+struct Detected {
+  int c, prn;
+  double code_phase, frequency;  // samples; Hz relative to the centre
+  size_t period;
+  int64_t length;
+};
+
+// The "refined" list: tga_fine_acquire on every detected satellite, in the
+// serde pretty layout of the rest of the output.
+std::string refined_json(tga_ctx* ctx, const tga_observation& obs, const std::vector<Detected>& det) {
+  std::vector<tga_fine_task> tasks;
+  for (const Detected& d : det) {
+    tga_fine_task t;
+    t.constellation = d.c;
+    t.prn = d.prn;
+    t.code_phase = d.code_phase;
+    t.frequency = 4.092e6 + d.frequency;
+    t.start = 0;
+    t.length = d.length;
+    tasks.push_back(t);
+  }
+  std::vector<tga_fine_result> res(tasks.size());
+  if (!tasks.empty() &&
+      tga_fine_acquire(ctx, obs.data, obs.num_antenna, obs.row_bytes, obs.sampling_frequency, tasks.data(),
+                       tasks.size(), nullptr, res.data(), nullptr) != TGA_OK) {
+    std::fprintf(stderr, "fine acquisition failed: %s\n", tga_last_error(ctx));
+    std::exit(1);
+  }
+  std::string s = "[";
+  for (size_t i = 0; i < det.size(); ++i) {
+    const tga_fine_result& r = res[i];
+    s += std::string(i ? ",\n" : "\n") + "    {\n      \"sv\": \"" + sv_label(det[i].c, det[i].prn) +
+         "\",\n      \"code_phase_samples\": " + num(r.code_phase) + ",\n      \"codephase_frac\": " +
+         num(r.code_phase / (double)det[i].period) + ",\n      \"frequency\": " + num(r.frequency - 4.092e6) +
+         ",\n      \"power\": " + num(r.power) + ",\n      \"power_start\": " + num(r.power_start) +
+         ",\n      \"iterations\": " + std::to_string(r.iterations) + ",\n      \"converged\": " +
+         (r.converged ? "true" : "false") + "\n    }";
+  }
+  s += det.empty() ? "]" : "\n  ]";
+  return s;
+}
+
+// Appends a top-level field to a pretty-printed JSON object.
+void append_field(std::string& json, const std::string& key, const std::string& value) {
+  const size_t end = json.rfind('}');
+  size_t body = end;
+  while (body > 0 && (json[body - 1] == '\n' || json[body - 1] == ' ')) --body;
+  const bool empty = json[body - 1] == '{';
+  json = json.substr(0, body) + (empty ? "\n" : ",\n") + "  \"" + key + "\": " + value + "\n}";
+}
 
 }  // namespace
 
@@ -259,6 +389,112 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "Running %s search (%zu PRNs)...\n", kNames[c],
                      a.has_prn ? a.prn.size() : (size_t)kNumPrns[c]);
       }
+    if (tga_set_precision(ctx, a.precision) != TGA_OK) {
+      std::fprintf(stderr, "%s\n", tga_last_error(ctx));
+      return 1;
+    }
+    std::vector<int32_t> ants;
+    if (a.has_ant) ants.assign(a.ant.begin(), a.ant.end());
+    else for (size_t k = 0; k < n_ant; ++k) ants.push_back((int32_t)k);
+    if (a.nc) {
+      // non-coherent search of every selected constellation in one call
+      std::vector<tga_nc_options> opts;
+      std::vector<int> consts;
+      std::vector<double> steps;
+      for (int c = 0; c < 6; ++c) {
+        if (!flags[c]) continue;
+        tga_nc_options q;
+        std::memset(&q, 0, sizeof q);
+        q.constellation = c;
+        q.prn_filter = a.has_prn ? a.prn.data() : nullptr;
+        q.n_prn_filter = a.prn.size();
+        q.ant_filter = ants.data();
+        q.n_ant_filter = ants.size();
+        q.center_freq = 4.092e6;
+        const double step = std::isnan(a.bin_hz) ? 1.0 / (2.0 * a.coherent_periods * kPeriodS[c]) : a.bin_hz;
+        q.bin_step_hz = step;
+        q.n_bins = 2 * (int)std::floor(6000.0 / step + 1e-9) + 1;  // the reference's +-6 kHz band
+        q.coherent_periods = (int32_t)a.coherent_periods;
+        q.blocks = (int32_t)a.blocks;
+        opts.push_back(q);
+        consts.push_back(c);
+        steps.push_back(step);
+      }
+      size_t n_cells = 0;
+      rc = tga_search_noncoherent_multi(ctx, obs.data, n_ant, obs.row_bytes, fs, opts.data(), opts.size(), nullptr,
+                                        0, &n_cells);
+      std::vector<tga_nc_cell> nc(n_cells);
+      if (rc == TGA_OK)
+        rc = tga_search_noncoherent_multi(ctx, obs.data, n_ant, obs.row_bytes, fs, opts.data(), opts.size(),
+                                          nc.data(), nc.size(), &n_cells);
+      if (rc != TGA_OK) {
+        std::fprintf(stderr, "non-coherent search failed: %s\n", tga_last_error(ctx));
+        return 1;
+      }
+      // {key: {antenna_numbers, coherent_periods, blocks, bin_hz, results: [{sv, powers,
+      // second_powers, phases, freqs}]}} in CombinedOutput order, results sorted by sv
+      std::string json = "{";
+      std::vector<Detected> det;
+      bool first = true;
+      for (int jc : kJsonOrder) {
+        size_t oi = 0, off = 0;
+        for (; oi < consts.size() && consts[oi] != jc; ++oi)
+          off += ants.size() * (a.has_prn ? a.prn.size() : (size_t)kNumPrns[consts[oi]]);
+        if (oi == consts.size()) continue;
+        const size_t n_prn = a.has_prn ? a.prn.size() : (size_t)kNumPrns[jc];
+        const size_t P = period_of(jc, fs);
+        std::vector<std::pair<std::string, size_t>> order;  // (sv, prn index)
+        for (size_t qi = 0; qi < n_prn; ++qi)
+          order.push_back({sv_label(jc, a.has_prn ? a.prn[qi] : kFirstPrn[jc] + (int)qi), qi});
+        std::sort(order.begin(), order.end());
+        json += std::string(first ? "\n" : ",\n") + "  \"" + kJsonKey[jc] + "\": {\n    \"antenna_numbers\": ";
+        first = false;
+        if (ants.empty()) {
+          json += "[]";
+        } else {
+          json += "[\n";
+          for (size_t k = 0; k < ants.size(); ++k)
+            json += "      " + std::to_string(ants[k]) + (k + 1 < ants.size() ? ",\n" : "\n");
+          json += "    ]";
+        }
+        json += ",\n    \"coherent_periods\": " + std::to_string(a.coherent_periods) + ",\n    \"blocks\": " +
+                std::to_string(a.blocks) + ",\n    \"bin_hz\": " + num(steps[oi]) + ",\n    \"results\": [";
+        for (size_t r = 0; r < order.size(); ++r) {
+          const tga_nc_cell* row = &nc[off + order[r].second * ants.size()];
+          std::vector<double> pw, sp, ph, fr;
+          size_t best = 0;
+          for (size_t k = 0; k < ants.size(); ++k) {
+            pw.push_back(row[k].power);
+            sp.push_back(row[k].second_power);
+            ph.push_back((double)row[k].best_codephase / (double)P);
+            fr.push_back(row[k].frequency);
+            if (row[k].power > row[best].power) best = k;
+          }
+          json += std::string(r ? ",\n" : "\n") + "      {\n        \"sv\": \"" + order[r].first +
+                  "\",\n        \"powers\": ";
+          arr(json, pw, 4);
+          json += ",\n        \"second_powers\": ";
+          arr(json, sp, 4);
+          json += ",\n        \"phases\": ";
+          arr(json, ph, 4);
+          json += ",\n        \"freqs\": ";
+          arr(json, fr, 4);
+          json += "\n      }";
+          // detected: summed peak power at least 4 x the second peak (2 x in amplitude)
+          if (!ants.empty() && row[best].power >= 4.0 * row[best].second_power)
+            det.push_back({jc, row[best].prn, (double)row[best].best_codephase, row[best].frequency, P,
+                           (int64_t)(a.coherent_periods * P)});
+        }
+        json += order.empty() ? "]" : "\n    ]";
+        json += "\n  }";
+      }
+      json += first ? "}" : "\n}";
+      if (a.refine) append_field(json, "refined", refined_json(ctx, obs, det));
+      write_out(json, a.output, "JSON output");
+      tga_destroy(ctx);
+      tga_observation_free(&obs);
+      return 0;
+    }
     tga_all_options o;
     std::memset(&o, 0, sizeof o);
     o.constellation_mask = mask;
@@ -285,9 +521,6 @@ int main(int argc, char** argv) {
       for (const tga_cell& t : cells)
         std::fprintf(stderr, "  %d PRN %3d ant %2d: strength=%.3f  phase=%.6f  freq=%.1f Hz\n", t.constellation,
                      t.prn, t.antenna, t.signal_strength, t.codephase_frac, t.frequency);
-    std::vector<int32_t> ants;
-    if (a.has_ant) ants.assign(a.ant.begin(), a.ant.end());
-    else for (size_t k = 0; k < n_ant; ++k) ants.push_back((int32_t)k);
     char* json = nullptr;
     size_t nf = 0;
     rc = tga_results_json(cells.data(), n_cells, ants.data(), ants.size(), mask, a.cn0, a.fpm, a.ffm, &json, &nf);
@@ -296,8 +529,28 @@ int main(int argc, char** argv) {
       return 1;
     }
     if (nf > 0) std::fprintf(stderr, "Filtered out %zu results (MAD thresholds)\n", nf);
-    write_out(json, a.output, "JSON output");
+    std::string text = json;
     tga_free(json);
+    if (a.refine) {
+      // every (constellation, PRN) detected on some antenna (strength at least
+      // twice the second peak), from its strongest antenna's grid estimate over
+      // the search window of two periods
+      std::vector<Detected> det;
+      for (size_t k = 0; k < cells.size();) {
+        size_t e = k, best = k;
+        while (e < cells.size() && cells[e].constellation == cells[k].constellation && cells[e].prn == cells[k].prn) {
+          if (cells[e].signal_strength > cells[best].signal_strength) best = e;
+          ++e;
+        }
+        const tga_cell& b = cells[best];
+        const size_t P = period_of(b.constellation, fs);
+        if (b.signal_strength >= 2.0 * b.second_peak)
+          det.push_back({b.constellation, b.prn, (double)b.best_codephase, b.frequency, P, (int64_t)(2 * P)});
+        k = e;
+      }
+      append_field(text, "refined", refined_json(ctx, obs, det));
+    }
+    write_out(text, a.output, "JSON output");
     tga_destroy(ctx);
     tga_observation_free(&obs);
     return 0;

@@ -2,11 +2,14 @@
 real TART recording: acquisition JSON (--gps --cn0) and the RFI report
 (--rfi) equal what the library produces for the same rows; --benchmark
 prints the reference's schema, and tga_benchmark's searches equal the
-single-PRN calls they time."""
+single-PRN calls they time; the engine's own flags (--precision,
+--coherent-periods / --noncoh / --bin-hz, --refine) give the library's
+results."""
 import json
 import os
 import subprocess
 
+import numpy as np
 import pytest
 
 import tga
@@ -77,3 +80,61 @@ def test_library_benchmark_equals_single_prn_calls():
                                                                          r.hypothesis)
             assert g.signal_strength == r.signal_strength and g.second_peak == r.second_peak
             assert e["search_s"] > 0
+
+
+def test_cli_precision_fp16tc_same_json():
+    """--precision fp16tc: the tensor-core search gives the same JSON as the
+    default FP32 search (every cell equal)."""
+    assert _run(["--gps", "--galileo", "--cn0", "--precision", "fp16tc"]) == _run(["--gps", "--galileo", "--cn0"])
+
+
+def test_cli_noncoherent_matches_library():
+    """--coherent-periods / --noncoh / --bin-hz: the non-coherent search of
+    the selected constellations through tga_search_noncoherent_multi, the
+    JSON fields equal to the library's cells."""
+    doc = json.loads(_run(["--gps", "--sbas", "--coherent-periods", "1", "--noncoh", "2", "--bin-hz", "250"]))
+    assert list(doc) == ["gps", "sbas"]
+    o = tga.read_hdf5(FIXTURE)
+    fs = o["sampling_frequency"]
+    with tga.Context(0) as ctx:
+        want = ctx.search_noncoherent_multi(o["data"], fs, [
+            dict(constellation=c, center_freq=4.092e6, bin_step_hz=250.0, n_bins=49, coherent_periods=1, blocks=2)
+            for c in (tga.GPS, tga.SBAS)])
+    for key, cells, first in (("gps", want[0], 1), ("sbas", want[1], 120)):
+        g = doc[key]
+        assert g["antenna_numbers"] == list(range(24)) and g["coherent_periods"] == 1 and g["blocks"] == 2
+        assert g["bin_hz"] == 250.0
+        assert [r["sv"] for r in g["results"]] == sorted(r["sv"] for r in g["results"])
+        for r in g["results"]:
+            prn = int(r["sv"].lstrip("GPSBA"))
+            rows = cells[cells["prn"] == prn]
+            assert r["powers"] == rows["power"].tolist() and r["freqs"] == rows["frequency"].tolist()
+            assert r["phases"] == (rows["best_codephase"] / 16368.0).tolist()
+            assert np.array_equal(r["second_powers"], rows["second_power"])
+
+
+def test_cli_refine_adds_refined_satellites():
+    """--refine: every satellite detected on some antenna is refined from
+    its strongest antenna's grid estimate (tga_fine_acquire over the two
+    search periods); the default output is unchanged apart from the added
+    field."""
+    base = json.loads(_run(["--gps"]))
+    doc = json.loads(_run(["--gps", "--refine"]))
+    assert list(doc) == ["gps", "refined"] and doc["gps"] == base["gps"]
+    o = tga.read_hdf5(FIXTURE)
+    fs = o["sampling_frequency"]
+    with tga.Context(0) as ctx:
+        cells = ctx.acquire_cells(o["data"], fs, mask=1 << tga.GPS)
+        tasks = []
+        for prn in sorted(set(cells["prn"].tolist())):
+            rows = cells[cells["prn"] == prn]
+            b = rows[int(np.argmax(rows["signal_strength"]))]
+            if b["signal_strength"] >= 2.0 * b["second_peak"]:
+                tasks.append((tga.GPS, prn, float(b["best_codephase"]), 4.092e6 + float(b["frequency"]), 0,
+                              2 * 16368))
+        res, _ = ctx.fine_acquire(o["data"], fs, tasks)
+    assert len(doc["refined"]) == len(tasks) > 0
+    for r, t, f in zip(doc["refined"], tasks, res):
+        assert r["sv"] == "GPS%02d" % t[1]
+        assert r["code_phase_samples"] == f["code_phase"] and r["frequency"] == f["frequency"] - 4.092e6
+        assert r["converged"] == bool(f["converged"])

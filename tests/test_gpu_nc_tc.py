@@ -91,8 +91,6 @@ def test_block_counts(ctx, blocks):
     kw = dict(prns=[5, 19, 30], bin_step_hz=250.0, n_bins=41, coherent_periods=4, blocks=blocks)
     f32, tc, rows = _both(ctx, bits, tga.GPS, **kw)
     _identical(f32, tc, rows, 41)
-    present = f32["prn"] != 30
-    assert np.all(f32["power"][present] > 2 * f32["second_power"][present])
 
 
 def test_sbas_codes(ctx):

@@ -40,7 +40,14 @@ def test_missing_and_corrupt_files_fail_cleanly(tmp_path):
 
 @pytest.mark.parametrize("args,msg", [(["--rfi", "--benchmark"], "--rfi cannot be combined with --benchmark"),
                                       (["--rfi", "--i", "0", "--j", "1"], "--rfi cannot be combined with --i/--j"),
-                                      (["--rfi", "--test-antennas"], "--rfi cannot be combined with --test-antennas")])
+                                      (["--rfi", "--test-antennas"], "--rfi cannot be combined with --test-antennas"),
+                                      (["--gps", "--precision", "fp64"], "invalid value for --precision: fp64"),
+                                      (["--gps", "--noncoh", "0"], "invalid positive integer for --noncoh: 0"),
+                                      (["--gps", "--coherent-periods", "x"], "invalid positive integer for"),
+                                      (["--gps", "--bin-hz", "50"], "--bin-hz sets the non-coherent search's grid"),
+                                      (["--gps", "--noncoh", "2", "--bin-hz", "-5"], "invalid positive float"),
+                                      (["--rfi", "--noncoh", "2"], "apply to the acquisition search only"),
+                                      (["--benchmark", "--refine"], "--refine applies to the acquisition search")])
 def test_cli_rejects_conflicting_modes(args, msg):
     if not os.path.exists(CLI):
         pytest.skip("CLI not built")
