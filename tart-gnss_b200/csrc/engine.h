@@ -173,9 +173,17 @@ cudaError_t launch_fine_sums(const uint8_t* d_bits, int n_ant, size_t row_bytes,
 // exact median bin power, local maxima above 15 dB (up to cap per antenna,
 // d_count counts all), exact autocorrelation popcounts at lags 1, 3, 16
 cudaError_t rfi_scan_device(const uint8_t* d_bits, int n_ant, size_t row_bytes, const double* d_mean, double* d_z,
-                            void* d_X, double* d_p, unsigned* d_hist, unsigned long long* d_prefix,
+                            void* d_X, void* d_work, double* d_p, unsigned* d_hist, unsigned long long* d_prefix,
                             unsigned long long* d_rank, int cap, unsigned* d_count, long long* d_bins,
-                            double* d_excess, unsigned long long* d_acf, cudaStream_t st, std::string* why);
+                            double* d_excess, unsigned long long* d_acf, int num_sms, cudaStream_t st,
+                            std::string* why);
+
+// f64 spectrum of `batch` real records of n samples (n even) held as doubles
+// in d_x (overwritten): p[a][k] = |X_a[k]|^2 for k < n / 2.  d_buf holds
+// batch * n / 2 complex doubles, d_work fft64_workspace_bytes(n, batch).
+size_t fft64_workspace_bytes(long long n, int batch);
+cudaError_t real_power_spectrum(double* d_x, void* d_buf, void* d_work, long long n, int batch, double* d_p,
+                                int num_sms, cudaStream_t st, std::string* why);
 
 // ACR Monte Carlo synthesizer (examples/gen_acr_tables.rs): n_points x
 // n_trials rows of 2 * period one-bit samples, packed MSB-first

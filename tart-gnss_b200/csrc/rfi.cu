@@ -3,7 +3,8 @@
 // For every antenna row of packed bits:
 //   * z = (+-1 samples) - mean over the whole row (rfi.rs:145-147);
 //   * its spectrum in f64 (rfi.rs:100-106: FFT of the whole record, powers of
-//     the first n/2 bins), here one batched cuFFT D2Z over all antennas;
+//     the first n/2 bins), with this library's own f64 FFT (fft64.cu) over
+//     all antennas at once;
 //   * the median bin power, exactly: a radix select over the bit patterns of
 //     the non-negative powers (8 passes of 8 bits), no sorting;
 //   * local maxima p[k] > p[k-1], p[k] >= p[k+1] with 10 log10(p / floor) >
@@ -13,7 +14,6 @@
 //     popcounts: sum z_i z_{i+L} = sum s s' - m (sum s_head + sum s_tail)
 //     + (n - L) m^2 with sum s s' = (n - L) - 2 popcount(b_i xor b_{i+L}).
 #include <cuda_runtime.h>
-#include <cufft.h>
 
 #include <cstdint>
 #include <string>
@@ -33,15 +33,6 @@ __global__ void rfi_prepare_kernel(const uint8_t* __restrict__ bits, size_t row_
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int bit = (__ldg(row + (i >> 3)) >> (7 - (int)(i & 7))) & 1;
     z[(size_t)a * n + i] = (bit ? 1.0 : -1.0) - m;
-  }
-}
-
-__global__ void rfi_power_kernel(const cufftDoubleComplex* __restrict__ X, long long nx, long long half,
-                                 double* __restrict__ p) {
-  const int a = blockIdx.y;
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < half; k += (long long)gridDim.x * blockDim.x) {
-    const cufftDoubleComplex v = X[(size_t)a * nx + k];
-    p[(size_t)a * half + k] = v.x * v.x + v.y * v.y;
   }
 }
 
@@ -153,32 +144,19 @@ __global__ void rfi_acf_kernel(const uint8_t* __restrict__ bits, size_t row_byte
 }  // namespace
 
 cudaError_t rfi_scan_device(const uint8_t* d_bits, int n_ant, size_t row_bytes, const double* d_mean, double* d_z,
-                            void* d_X, double* d_p, unsigned* d_hist, unsigned long long* d_prefix,
+                            void* d_X, void* d_work, double* d_p, unsigned* d_hist, unsigned long long* d_prefix,
                             unsigned long long* d_rank, int cap, unsigned* d_count, long long* d_bins,
-                            double* d_excess, unsigned long long* d_acf, cudaStream_t st, std::string* why) {
-  const long long n = (long long)row_bytes * 8, half = n / 2, nx = n / 2 + 1;
+                            double* d_excess, unsigned long long* d_acf, int num_sms, cudaStream_t st,
+                            std::string* why) {
+  const long long n = (long long)row_bytes * 8, half = n / 2;
   if (n_ant <= 0 || n < 8) return cudaSuccess;
   cudaError_t e;
   dim3 g1(256, n_ant);
   rfi_prepare_kernel<<<g1, 256, 0, st>>>(d_bits, row_bytes, d_mean, n, d_z);
   kernel_launch_add(1);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  cufftHandle plan;
-  int nn = (int)n;
-  if (cufftPlanMany(&plan, 1, &nn, nullptr, 1, (int)n, nullptr, 1, (int)nx, CUFFT_D2Z, n_ant) != CUFFT_SUCCESS) {
-    *why = "cuFFT plan of length " + std::to_string(n) + " failed";
-    return cudaErrorUnknown;
-  }
-  cufftResult fr = cufftSetStream(plan, st);
-  if (fr == CUFFT_SUCCESS) fr = cufftExecD2Z(plan, d_z, static_cast<cufftDoubleComplex*>(d_X));
-  cufftDestroy(plan);
-  if (fr != CUFFT_SUCCESS) {
-    *why = "cuFFT D2Z failed (" + std::to_string((int)fr) + ")";
-    return cudaErrorUnknown;
-  }
-  rfi_power_kernel<<<g1, 256, 0, st>>>(static_cast<const cufftDoubleComplex*>(d_X), nx, half, d_p);
-  kernel_launch_add(1);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  // powers of the first n/2 bins of every antenna's f64 spectrum
+  if ((e = real_power_spectrum(d_z, d_X, d_work, n, n_ant, d_p, num_sms, st, why)) != cudaSuccess) return e;
   // median bin power: rank half / 2 (rfi.rs:110-111)
   if ((e = cudaMemsetAsync(d_hist, 0, (size_t)n_ant * 256 * sizeof(unsigned), st)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(d_prefix, 0, (size_t)n_ant * sizeof(unsigned long long), st)) != cudaSuccess) return e;

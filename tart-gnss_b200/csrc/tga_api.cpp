@@ -1767,6 +1767,7 @@ int tga_rfi_scan(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant, size_t row_b
     CK(launch_antenna_means(d_bits, (int)A, row_bytes, d_mean, st));
     double* d_z = (double*)ctx->buf("rfi.z", A * (size_t)n * sizeof(double));
     void* d_X = ctx->buf("rfi.X", A * (size_t)(n / 2 + 1) * 16);
+    void* d_work = ctx->buf("rfi.work", fft64_workspace_bytes(n, (int)A));
     double* d_p = (double*)ctx->buf("rfi.p", A * (size_t)half * sizeof(double));
     unsigned* d_hist = (unsigned*)ctx->buf("rfi.hist", A * 256 * sizeof(unsigned));
     unsigned long long* d_prefix = (unsigned long long*)ctx->buf("rfi.prefix", A * 8);
@@ -1776,8 +1777,8 @@ int tga_rfi_scan(tga_ctx* ctx, const uint8_t* h_bits, size_t n_ant, size_t row_b
     double* d_excess = (double*)ctx->buf("rfi.excess", A * kCap * sizeof(double));
     unsigned long long* d_acf = (unsigned long long*)ctx->buf("rfi.acf", A * 9 * 8);
     std::string why;
-    const cudaError_t e = rfi_scan_device(d_bits, (int)A, row_bytes, d_mean, d_z, d_X, d_p, d_hist, d_prefix, d_rank,
-                                          kCap, d_count, d_bins, d_excess, d_acf, st, &why);
+    const cudaError_t e = rfi_scan_device(d_bits, (int)A, row_bytes, d_mean, d_z, d_X, d_work, d_p, d_hist, d_prefix,
+                                          d_rank, kCap, d_count, d_bins, d_excess, d_acf, ctx->num_sms, st, &why);
     if (!why.empty()) throw std::runtime_error(why);
     CK(e);
     std::vector<double> mean(A);

@@ -69,3 +69,21 @@ def test_rfi_scan_matches_oracle_real_recording():
     with tga.Context(0) as ctx:
         got = ctx.rfi_scan(bits, fs)
     _compare(got, RO.run(bits, fs))
+
+
+@pytest.mark.parametrize("row_bytes", [1000, 1031, 3069], ids=["2^5x5^3", "bluestein-1031", "3x11x31"])
+def test_rfi_spectrum_any_length(row_bytes):
+    """Record lengths whose half length L = 4 row_bytes has odd radices
+    (5^3; 3 x 11 x 31) or a prime factor above the largest pass radix (1031:
+    Bluestein's chirp-z over a power-of-two convolution): the f64 spectrum,
+    lines and floor match the oracle as at the usual lengths."""
+    n = row_bytes * 8
+    i = np.arange(n)
+    sq = np.where(np.mod(i.astype(np.float64), FS / 1.5e6) < FS / 3.0e6, 1.0, -1.0)
+    rows = [3.0 * sq + _xs("oracle_xorshift_gaussian", 21, n), _xs("oracle_xorshift_gaussian", 22, n)]
+    bits = np.packbits(np.stack(rows) >= 0.0, axis=1)
+    assert bits.shape[1] == row_bytes
+    with tga.Context(0) as ctx:
+        got = ctx.rfi_scan(bits, FS)
+    _compare(got, RO.run(bits, FS))
+    assert got[0]["lines"]
