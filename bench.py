@@ -50,13 +50,16 @@ GROUP_PRNS = {1023: 100, 4092: 50, 10230: 126}
 SAMPLES_PER_CHIP = 16
 
 
-def workload_config(n_ant):
+def workload_config(n_ant, sharded=False, world=1):
     """The `config` object of both arms: the workload only, nothing of the
     arithmetic or the implementation that runs it."""
     cells = sum(n_ant * 41 * n * SAMPLES_PER_CHIP * lc for lc, n in GROUP_PRNS.items())
-    return {"workload": WORKLOAD, "n_ant": n_ant, "cells_per_step_per_gpu": float(cells),
-            "l2": "256 MB buffer written between timed steps; 3.9 GB intermediate per step",
-            "parallelism": "replicas (weak scaling: one 24-antenna observation per GPU)"}
+    par = ("antenna shards (strong scaling: the antennas of one %d-antenna observation split over %d GPUs, cells "
+           "all-gathered)" % (n_ant, world) if sharded else
+           "replicas (weak scaling: one %d-antenna observation per GPU)" % n_ant)
+    return {"workload": WORKLOAD, "n_ant": n_ant,
+            "cells_per_step_per_gpu": float(cells) / (world if sharded else 1),
+            "l2": "256 MB buffer written between timed steps; 3.9 GB intermediate per step", "parallelism": par}
 
 
 def tga_codes(c, prn, period):
@@ -485,6 +488,9 @@ def main():
     ap.add_argument("--no-fine", action="store_true", help="skip the fine-acquisition measurement")
     ap.add_argument("--no-config2", action="store_true",
                     help="skip the non-coherent --all search (per-code-length bins over 100 ms)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="with N GPUs, split the antennas of one observation over the ranks (strong scaling, "
+                         "multi_gpu.py) instead of one observation per rank")
     ap.add_argument("--no-split", action="store_true", help="skip the --benchmark-style setup/search split")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -518,9 +524,13 @@ def main():
     import ctypes
     prec_id = {"fp32": tga.PRECISION_FP32, "fp16tc": tga.PRECISION_FP16_TC}
 
+    # --sharded: this rank's antennas of the one observation (all of them at N = 1)
+    from multi_gpu import acquire_cells_sharded, shard_antennas
+    shard = shard_antennas(range(n_ant), world, rank) if args.sharded else None
+
     def step_device():
         return ctx.acquire_cells(None, FS, mask=tga.ALL, cn0=True, device_bits=d_bits.data_ptr(), n_ant=n_ant,
-                                 row_bytes=row_bytes)
+                                 row_bytes=row_bytes, ant_filter=shard)
 
     def kernel_times():
         cap = 64
@@ -767,7 +777,14 @@ def main():
         ctx.set_precision(prec_id[args.precision])
     clocks = clk.stop()
     sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
-    value = cells * world / (ms_step / 1e3)
+    # whole-job cells per step: every rank's (one observation per rank), or
+    # the one observation split over the ranks (--sharded)
+    job_cells = cells * world
+    if args.sharded and world > 1:
+        t = torch.tensor([cells], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t)
+        job_cells = float(t.item())
+    value = job_cells / (ms_step / 1e3)
 
     # end to end through the C ABI from pinned host memory
     ctx.set_precision(prec_id[args.precision])
@@ -776,7 +793,10 @@ def main():
     for i in range(0 if args.no_e2e else args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ctx.acquire_cells(host, FS, mask=tga.ALL, cn0=True)
+        if args.sharded and world > 1:
+            acquire_cells_sharded(ctx, host, FS, mask=tga.ALL, cn0=True)
+        else:
+            ctx.acquire_cells(host, FS, mask=tga.ALL, cn0=True)
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             e2e_times.append(dt)
@@ -792,12 +812,13 @@ def main():
 
     dtype = {"fp32": "f32", "fp16tc": "f16-tc+f32"}
     line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "strong" if args.sharded else "weak",
             "vs_baseline": None, "dtype": dtype[args.precision], "data": "synthetic",
-            "config": workload_config(n_ant),
+            "config": workload_config(n_ant, args.sharded, world),
             "arithmetic": ("FP16 tensor-core (tcgen05) transform, FP32 accumulation, selected rows "
                            "re-evaluated in FP32" if args.precision == "fp16tc" else "FP32 CUDA-core transform"),
-            "e2e": {"value": cells * world / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": h2d.value,
+            "e2e": {"value": job_cells / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": h2d.value,
                     "d2h_bytes_per_step": d2h.value, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": launches,
             "roofline": roofline(agg, args.precision, sm_mhz),
