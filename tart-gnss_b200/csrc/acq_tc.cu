@@ -134,6 +134,23 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
                : "r"(taddr)
                : "memory");
 }
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+               "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+               : "memory");
+}
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, const uint32_t (&r)[4]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(r[0]), "r"(r[1]),
+               "r"(r[2]), "r"(r[3])
+               : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 // Reads 16 N16 TMEM columns of this warp's 32 lanes starting at taddr and
 // waits once.
 template <int N16>
@@ -313,7 +330,16 @@ struct T3 {
   static constexpr int ACC_OUT = NST == 2 ? 33 : 2 * R3;
   static constexpr int ACC_ROWS = LAST_TILES * 128;
   static constexpr int ACC_BYTES = NCB ? (ACC_OUT * ACC_ROWS * 4 + 1023) / 1024 * 1024 : 0;
-  static constexpr int N_ACC = NCB ? (BLKCH ? 1 : 2) : 0, N_CODE = BLKCH ? 1 : 2;
+  // BLKCH keeps its one set of sums in the TMEM columns the two chains leave
+  // free ([CHAIN_COLS, 256) of each half): stage-3 tile t, half h at column
+  // sum_col(t) + 12 h, 11 columns each (its rows are the tile's lanes), so
+  // the read-modify-write of the sums uses the TMEM path instead of the
+  // shared memory the MMAs read their operands from
+  static_assert(!BLKCH || (LAST_TILES == 4 && CHAIN_COLS <= 256 - 48 && ACC_OUT == 22), "TMEM sums");
+  static constexpr int N_ACC = NCB && !BLKCH ? 2 : 0, N_CODE = BLKCH ? 1 : 2;
+  __device__ static __forceinline__ uint32_t sum_col(int t) {
+    return (uint32_t)((t < 2 ? 0 : 256) + CHAIN_COLS + (t & 1) * 24);
+  }
   // data operand regions: rows padded to whole tiles, K chunks lbo apart
   static constexpr int LBO1 = TILES1 * 128 * 16 + 16, LBO2 = TILES2 * 128 * 16 + 16 * Tc3Cfg<M>::PAD2,
                        LBO3 = TILES3 * 128 * 16 + 16 * Tc3Cfg<M>::PAD3;
@@ -1002,7 +1028,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
     // [24 h, 24 h + 22)).  task = warp + i NW keeps the warp's quadrant.
     auto p4_nc = [&](int x, int g, bool first, bool last) -> float {
       const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
-      float* acc = ACC + (size_t)(T::BLKCH ? 0 : x) * (T::ACC_BYTES / 4);
+      float* acc = ACC + (size_t)x * (T::ACC_BYTES / 4);  // unused with BLKCH (sums in TMEM)
       float best = 0.f;
       // adds the powers of 11 complex outputs (words v[o + 2 h], v[o + 2 h + 1])
       // to the 11 sums a[h ACC_ROWS]: all loads of the sums first, then the
@@ -1055,18 +1081,47 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
         }
       } else {
         constexpr int NTN = T::LAST_TILES * 4 * 2, TPWN = (NTN + NW - 1) / NW;
-#pragma unroll
+        // one task at a time (unrolled, the tasks' registers spilled)
+#pragma unroll 1
         for (int i = 0; i < TPWN; ++i) {
           const int task = warp + i * NW;
           if (task >= NTN) break;
           const int t = task / 8, half = (task >> 2) & 1;
           uint32_t v[24];
           tmem_ld_stage3<T::PAIR3>(tb + (uint32_t)(t * T::N3), half, v);
-          tmem_wait_ld();
           const int r = t * 128 + quad * 32 + lane;
           const bool valid = r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S;
-          add11(v, acc + (size_t)(11 * half) * T::ACC_ROWS + r, valid);
+          if constexpr (T::BLKCH) {
+            // sums in TMEM: load, add, store (or take the maximum)
+            const uint32_t sa = tmem_base + lane_off + T::sum_col(t) + (uint32_t)(12 * half);
+            uint32_t su[12];
+            uint32_t(&s8)[8] = *reinterpret_cast<uint32_t(*)[8]>(&su[0]);
+            uint32_t(&s4)[4] = *reinterpret_cast<uint32_t(*)[4]>(&su[8]);
+            if (!first) {
+              tmem_ld8(sa, s8);
+              tmem_ld4(sa + 8, s4);
+            }
+            tmem_wait_ld();
+#pragma unroll
+            for (int h = 0; h < 11; ++h) {
+              const float re = __uint_as_float(v[2 * h]), im = __uint_as_float(v[2 * h + 1]);
+              su[h] = __float_as_uint(fmaf(re, re, im * im) + (first ? 0.f : __uint_as_float(su[h])));
+            }
+            if (!last) {
+              su[11] = 0u;
+              tmem_st8(sa, s8);
+              tmem_st4(sa + 8, s4);
+            } else if (valid) {
+#pragma unroll
+              for (int h = 0; h < 11; ++h) best = fmaxf(best, __uint_as_float(su[h]));
+            }
+          } else {
+            tmem_wait_ld();
+            add11(v, acc + (size_t)(11 * half) * T::ACC_ROWS + r, valid);
+          }
         }
+        // the sums' stores land before this thread reads them again
+        if constexpr (T::BLKCH) tmem_wait_st();
       }
       return best;
     };

@@ -1968,7 +1968,8 @@ void nc_run_group(tga_ctx* ctx, const uint8_t* d_bits, size_t row_bytes, const d
   unsigned long long* d_keys = (unsigned long long*)ctx->buf(tag + ".keys", n_rows * sizeof(unsigned long long));
   BestRow* d_best = (BestRow*)ctx->buf(tag + ".best", (size_t)n_ant * n_prn * sizeof(BestRow));
   const double row = corr_row_flops(pc.P);
-  timed(ctx, "nc_code_spectra", (double)n_prn * 2 * fft_flops(pc.Lc),
+  const std::string cls = "[Lc=" + std::to_string(pc.Lc) + "]";
+  timed(ctx, ("nc_code_spectra" + cls).c_str(), (double)n_prn * 2 * fft_flops(pc.Lc),
         [&] { return launch_code_spectra(pc, d_chips, n_prn, d_D, ctx->num_sms, st); });
   // tensor-core mode: FP16 operands, DFT matrices, and the FP32
   // re-evaluation's keys, row list and per-chunk counts
@@ -1993,7 +1994,7 @@ void nc_run_group(tga_ctx* ctx, const uint8_t* d_bits, size_t row_bytes, const d
     d_keys32 = (unsigned long long*)ctx->buf(tag + ".keys32", n_rows * sizeof(unsigned long long));
     d_cand = (int2*)ctx->buf(tag + ".cand", n_rows * sizeof(int2));
     d_count = (int*)ctx->buf(tag + ".count", (size_t)n_chunks * sizeof(int));
-    timed(ctx, "nc_tc_pack", 0.0,
+    timed(ctx, ("nc_tc_pack" + cls).c_str(), 0.0,
           [&] { return launch_tc_pack(pc, d_D, (long long)n_prn * 2, true, d_d16, ctx->num_sms, st); });
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
     CK(cudaMemsetAsync(d_count, 0, (size_t)n_chunks * sizeof(int), st));
@@ -2011,33 +2012,33 @@ void nc_run_group(tga_ctx* ctx, const uint8_t* d_bits, size_t row_bytes, const d
     cd.n_ant = na;
     const long long cseq = (long long)na * seq_per_ant;
     BestRow* cbest = d_best + (size_t)a0 * n_prn;
-    timed(ctx, "nc_frontend", (double)na * nb * B * 10.0 * pc.P * opt->coherent_periods,
+    timed(ctx, ("nc_frontend" + cls).c_str(), (double)na * nb * B * 10.0 * pc.P * opt->coherent_periods,
           [&] { return launch_nc_frontend(cs, cd, pc, opt->coherent_periods, B, opt->start, d_z, st); });
     // in tensor-core mode the forward transform also writes Z's FP16 operands
-    timed(ctx, "nc_forward_z", (double)na * nb * B * fft_flops(pc.P), [&] {
+    timed(ctx, ("nc_forward_z" + cls).c_str(), (double)na * nb * B * fft_flops(pc.P), [&] {
       return tc ? launch_forward_seqs_tc(pc, cseq, d_z, d_z16, d_zmap, tc_z_scale(pc), ctx->num_sms, st)
                 : launch_forward_seqs(pc, cseq, d_z, ctx->num_sms, st);
     });
     if (tc) {
-      timed(ctx, "nc_correlate_tc", (double)na * nb * n_prn * B * row, [&] {
+      timed(ctx, ("nc_correlate_tc" + cls).c_str(), (double)na * nb * n_prn * B * row, [&] {
         return launch_correlate_tc_nc(pc, cd, B, d_bmat, d_z16, d_d16, d_keys + r0, d_err, ctx->test_flags,
                                       ctx->num_sms, st);
       });
       // rows within the FP16 key error of their (antenna, PRN)'s best,
       // re-evaluated in FP32; the bins are then reduced over the FP32 keys
-      timed(ctx, "nc_candidates", 0.0, [&] {
+      timed(ctx, ("nc_candidates" + cls).c_str(), 0.0, [&] {
         return launch_tc_candidates(cd, 1, d_keys + r0, kTcKeyKeep, d_cand + r0, d_count + ch, st);
       });
-      timed(ctx, "nc_refine", 0.0, [&] {
+      timed(ctx, ("nc_refine" + cls).c_str(), 0.0, [&] {
         return launch_nc_correlate_listed(pc, cd, B, d_z, d_D, d_cand + r0, d_count + ch, na * nb * n_prn,
                                           d_keys32 + r0, ctx->num_sms, st);
       });
     } else {
-      timed(ctx, "nc_correlate", (double)na * nb * n_prn * B * row,
+      timed(ctx, ("nc_correlate" + cls).c_str(), (double)na * nb * n_prn * B * row,
             [&] { return launch_nc_correlate(pc, cd, B, d_z, d_D, d_keys + r0, ctx->num_sms, st); });
     }
-    timed(ctx, "nc_reduce", 0.0, [&] { return launch_nc_reduce(cd, (tc ? d_keys32 : d_keys) + r0, cbest, st); });
-    timed(ctx, "nc_second", (double)na * n_prn * B * row,
+    timed(ctx, ("nc_reduce" + cls).c_str(), 0.0, [&] { return launch_nc_reduce(cd, (tc ? d_keys32 : d_keys) + r0, cbest, st); });
+    timed(ctx, ("nc_second" + cls).c_str(), (double)na * n_prn * B * row,
           [&] { return launch_nc_second(pc, cd, B, d_z, d_D, cbest, chip_width_of(fs), ctx->num_sms, st); });
   }
   std::vector<BestRow> best((size_t)n_ant * n_prn);
