@@ -1132,21 +1132,35 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       // this item's Z units of block blk, in registers
       uint4 zr[U];
       auto load_z = [&](int blk) {
+        // the drop-in search reads its Z once (evict first); the
+        // non-coherent search reads each block again for every PRN (pair),
+        // so it keeps the blocks in L2.  blk >= B (BLKCH, B odd) stands for
+        // zero data, which adds nothing to the sums.
+        const uint4* seq = p.z16 + (((size_t)ab_h * B + blk) * S + (size_t)g * BC) * 8 * T::ROWS1;
+        if constexpr (BC == 1) {
+          // one residue per item: unit e's offset in its sequence is its
+          // code-unit index, the high half of uoff
+          const bool any = g < S && blk < B;
 #pragma unroll
-        for (int k = 0; k < U; ++k) {
-          const int e = tid + k * NTS;
-          zr[k] = make_uint4(0u, 0u, 0u, 0u);
-          if (e < T::UNITS) {
-            const int j = e / T::NR1, r = e - j * T::NR1;
-            const int s = r / T::ROWS1, u = r - s * T::ROWS1;
-            const int rho = g * BC + s;
-            // the drop-in search reads its Z once (evict first); the
-            // non-coherent search reads each block again for every PRN
-            // (pair), so it keeps the blocks in L2.  blk >= B (BLKCH, B
-            // odd) stands for zero data, which adds nothing to the sums.
-            if (rho < S && blk < B) {
-              const uint4* src = p.z16 + ((((size_t)ab_h * B + blk) * S + rho) * 8 + j) * T::ROWS1 + u;
+          for (int k = 0; k < U; ++k) {
+            zr[k] = make_uint4(0u, 0u, 0u, 0u);
+            if (any && (k < U - 1 || tid + k * NTS < T::UNITS)) {
+              const uint4* src = seq + (uoff[k] >> 16);
               zr[k] = NCB ? __ldcg(src) : __ldcs(src);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < U; ++k) {
+            const int e = tid + k * NTS;
+            zr[k] = make_uint4(0u, 0u, 0u, 0u);
+            if (e < T::UNITS) {
+              const int j = e / T::NR1, r = e - j * T::NR1;
+              const int s = r / T::ROWS1, u = r - s * T::ROWS1;
+              if (g * BC + s < S && blk < B) {
+                const uint4* src = seq + ((size_t)s * 8 + j) * T::ROWS1 + u;
+                zr[k] = NCB ? __ldcg(src) : __ldcs(src);
+              }
             }
           }
         }

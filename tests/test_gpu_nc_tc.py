@@ -23,7 +23,7 @@ P = 16368
 FIELDS = ("prn", "antenna", "best_freq_idx", "best_codephase", "power", "second_power", "frequency")
 # amplitude error bound of the FP16 keys relative to the (antenna, PRN)'s
 # largest, assumed by the library's candidate rule (kTcKeyKeep)
-KEY_BOUND = 2.0 ** -6
+KEY_BOUND = 2.0 ** -8
 
 
 @pytest.fixture(scope="module")

@@ -69,8 +69,8 @@ CELL_FIELDS = ("best_codephase", "best_freq_idx", "hypothesis", "signal_strength
                "frequency", "cn0_valid", "cn0_acr")
 # amplitude error bound of the FP16 row keys, relative to the largest row
 # amplitude of the (antenna, PRN), that the candidate rule of the library
-# assumes (kTcKeyKeep = (1 - 2 d)^2, d = 2^-6)
-KEY_BOUND = 2.0 ** -6
+# assumes (kTcKeyKeep = (1 - 2 d)^2, d = 2^-8)
+KEY_BOUND = 2.0 ** -8
 GROUPS = [(1 << tga.GPS | 1 << tga.SBAS | 1 << tga.QZSS, 1023), (1 << tga.GALILEO, 4092),
           (1 << tga.BEIDOU | 1 << tga.L1C, 10230)]
 
