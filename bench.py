@@ -499,6 +499,9 @@ def main():
     ap.add_argument("--no-fine", action="store_true", help="skip the fine-acquisition measurement")
     ap.add_argument("--no-config2", action="store_true",
                     help="skip the non-coherent --all search (per-code-length bins over 100 ms)")
+    ap.add_argument("--config2-only", action="store_true",
+                    help="run only the non-coherent --all search of --n-ant antennas and print its object "
+                         "(profiling runs)")
     ap.add_argument("--sharded", action="store_true",
                     help="with N GPUs, split the antennas of one observation over the ranks (strong scaling, "
                          "multi_gpu.py) instead of one observation per rank")
@@ -647,6 +650,14 @@ def main():
         return {k: {"ms_per_step": v[0] / args.steps, "share": v[0] / tot, "launches_per_step": v[1] / args.steps}
                 for k, v in agg.items()}
 
+    if args.config2_only:
+        c2 = run_config2(ctx, bits_np, sats_np, args, world, stream, flush, kernel_times, prec_id)
+        if rank == 0:
+            print(json.dumps({"config2": c2}), flush=True)
+        ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
     clk = Clocks(local)
     clk.start()
     ms_step, cells, agg, launches, out = measure(args.precision)
