@@ -36,12 +36,10 @@
 // per chain issues its MMAs.  Every wait is bounded (1 s): on expiry the kernel sets
 // *err, drains (again bounded), frees its TMEM and returns.
 //
-// The same kernel (NCB) runs the non-coherent search: every PRN pair goes
-// through B coherent blocks, the Z of each block is loaded into the registers
-// in turn, and the |y|^2 of the blocks are summed in shared memory before the
-// row maximum.  At Lc = 10230, where two chains' sums and code blocks do not
-// fit the shared memory, the two chains instead take consecutive blocks of
-// one PRN and share its code block and sums (BLKCH).
+// The same kernel (NCB) runs the non-coherent search: the two chains take
+// consecutive coherent blocks of one PRN (BLKCH), the Z of each block is
+// loaded into the registers in turn, and the |y|^2 of the blocks are summed
+// in the free TMEM columns before the row maximum.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -316,29 +314,25 @@ struct T3 {
   static constexpr int LAST_TILES = NST == 3 ? TILES3 : TILES2;
   static constexpr int LAST_ROWS = NST == 3 ? ROWS3P : ROWS2, LAST_NR = NST == 3 ? NR3 : NR2;
   static constexpr int LAST_OUT = NST == 3 ? R3 : R2;
-  // non-coherent search: |y|^2 sums over the blocks of the ACC_OUT outputs
-  // of every last-stage row (33 stage-2 outputs, or the 2 x 11 outputs of a
-  // paired stage-3 row), as [ACC_OUT][LAST_TILES * 128] floats (rows
-  // fastest: a warp's 32 lanes touch 32 banks).  The two chains run two
-  // PRNs, each with its own code block and sums, except with BLKCH (Lc =
-  // 10230, where two sets of sums and code blocks do not fit the shared
-  // memory): there the chains run consecutive blocks of one PRN and share
-  // its code block and one set of sums.
-  static constexpr bool BLKCH = NCB && M == 10;
+  // Non-coherent search (NCB): the two chains run consecutive blocks of ONE
+  // PRN (chain x takes block 2 i + x; "block chains", BLKCH), so one code
+  // block and one set of |y|^2 sums serve both.  The sums live in the TMEM
+  // columns the two chains' accumulators leave free, [CHAIN_COLS, 256) of
+  // each half: every last-stage row (a lane) has SLOTS slots of 11 outputs
+  // (the 33 stage-2 outputs, or the 2 x 11 outputs of a paired stage-3
+  // row), 12 columns per slot; tile t, slot c at sum_col(t, c).  Their
+  // read-modify-write then uses the TMEM path instead of the shared memory
+  // the MMAs read their operands from, and two sets of sums (66 to 96
+  // columns each) would not fit the 128 free columns.
+  static constexpr bool BLKCH = NCB;
   static_assert(!NCB || (NST == 2 && LAST_OUT == 33) || (NST == 3 && PAIR3 && LAST_OUT == 11),
                 "non-coherent epilogue layouts");
-  static constexpr int ACC_OUT = NST == 2 ? 33 : 2 * R3;
-  static constexpr int ACC_ROWS = LAST_TILES * 128;
-  static constexpr int ACC_BYTES = NCB ? (ACC_OUT * ACC_ROWS * 4 + 1023) / 1024 * 1024 : 0;
-  // BLKCH keeps its one set of sums in the TMEM columns the two chains leave
-  // free ([CHAIN_COLS, 256) of each half): stage-3 tile t, half h at column
-  // sum_col(t) + 12 h, 11 columns each (its rows are the tile's lanes), so
-  // the read-modify-write of the sums uses the TMEM path instead of the
-  // shared memory the MMAs read their operands from
-  static_assert(!BLKCH || (LAST_TILES == 4 && CHAIN_COLS <= 256 - 48 && ACC_OUT == 22), "TMEM sums");
-  static constexpr int N_ACC = NCB && !BLKCH ? 2 : 0, N_CODE = BLKCH ? 1 : 2;
-  __device__ static __forceinline__ uint32_t sum_col(int t) {
-    return (uint32_t)((t < 2 ? 0 : 256) + CHAIN_COLS + (t & 1) * 24);
+  static constexpr int SLOTS = NST == 2 ? 3 : 2, TILE_COLS = 12 * SLOTS;
+  static constexpr int PER_RANGE = (kTcTmemCols / 2 - CHAIN_COLS) / TILE_COLS;
+  static_assert(!NCB || LAST_TILES <= 2 * PER_RANGE, "the sums fit the free TMEM columns");
+  static constexpr int N_CODE = BLKCH ? 1 : 2;
+  __device__ static __forceinline__ uint32_t sum_col(int t, int c) {
+    return (uint32_t)((t / PER_RANGE) * (kTcTmemCols / 2) + CHAIN_COLS + (t % PER_RANGE) * TILE_COLS + 12 * c);
   }
   // data operand regions: rows padded to whole tiles, K chunks lbo apart
   static constexpr int LBO1 = TILES1 * 128 * 16 + 16, LBO2 = TILES2 * 128 * 16 + 16 * Tc3Cfg<M>::PAD2,
@@ -355,7 +349,7 @@ struct T3 {
   static constexpr int U = (UNITS + kSimtThreads - 1) / kSimtThreads;
   static_assert(8 * ROWS1 < 65536 && 8 * LBO1 < 65536, "packed unit offsets");
   static constexpr int SMEM_RAW =
-      2 * A_BYTES + B1_BYTES + B2_BYTES + B3_BYTES + N_CODE * CODE_REGION + N_ACC * ACC_BYTES + 1024;
+      2 * A_BYTES + B1_BYTES + B2_BYTES + B3_BYTES + N_CODE * CODE_REGION + 1024;
   // more than half of the SM's shared memory: one CTA, and so one 512-column
   // TMEM allocation, per SM
   static constexpr int SMEM = SMEM_RAW > 120 * 1024 ? SMEM_RAW : 120 * 1024;
@@ -519,14 +513,12 @@ __device__ __forceinline__ void tmem_ld_stage3(uint32_t taddr, int half, uint32_
 // thread until the tensor cores take it, so issuing has warps of its own,
 // one per chain.  Every wait is bounded.
 //
-// NCB (non-coherent search): the row is an (antenna, bin) and every PRN pair
-// runs through B coherent blocks; each thread keeps the |y|^2 sums of its
-// epilogue outputs in shared memory and takes the row maximum after the last
-// block.  The Z of the next block is loaded into the registers while the
-// current block's transform runs.  BLKCH (Lc = 10230): a round is one PRN,
-// whose blocks 2 i and 2 i + 1 run on chains a and b; one code block and one
-// set of sums serve both chains, and chain b's Z is loaded after chain a has
-// formed its products.
+// NCB (non-coherent search, block chains): the row is an (antenna, bin), a
+// round is one PRN, whose blocks 2 i and 2 i + 1 run on chains a and b; one
+// code block and one set of |y|^2 sums (in TMEM) serve both chains, and each
+// thread takes the row maximum of its sums after the last block.  The Z of
+// chain a's next block is loaded into the registers while the current
+// transforms run, chain b's after chain a has formed its products.
 // The code warp's thread: after the 12 SIMT warps have formed chain x's
 // products of a PRN's last block (s_p1[x]), bulk-copy the chain's next code
 // block into its slot (s_code[x]).  Its own function, so that its registers
@@ -620,8 +612,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
   unsigned char* B2 = B1 + T::B1_BYTES;
   unsigned char* B3 = B2 + T::B2_BYTES;
   unsigned char* CODE0 = B3 + T::B3_BYTES;
-  // NCB: the sums, [N_ACC][ACC_OUT][ACC_ROWS]
-  float* ACC = reinterpret_cast<float*>(CODE0 + T::N_CODE * T::CODE_REGION);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quad = warp & 3;
   // rounds: PRN pairs, or with BLKCH single PRNs; steps of a round: one per
   // coherent block, or with BLKCH one per pair of blocks (chain x takes
@@ -1019,42 +1009,49 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       }
     };
 
-    // ---- P4 of the non-coherent search: add the block's |y|^2 to the
-    // chain's sums in shared memory (first: the sums start at it); after the
-    // last block (last), the row maximum of the sums ----
+    // ---- P4 of the non-coherent search: add the block's |y|^2 to the sums
+    // in TMEM (first: the sums start at it); after the last block (last),
+    // the row maximum of the sums ----
     // Two-stage split: tasks are (stage-2 tile, lane quadrant, outputs
     // [11 c, 11 c + 11)).  Three-stage paired split: tasks are (stage-3
-    // tile, lane quadrant, half h: the 11 outputs of accumulator columns
-    // [24 h, 24 h + 22)).  task = warp + i NW keeps the warp's quadrant.
+    // tile, lane quadrant, half c: the 11 outputs of accumulator columns
+    // [24 c, 24 c + 22)).  task = warp + i NW keeps the warp's quadrant,
+    // whose lanes hold the task's rows in the accumulator and in the sums.
+    // One task at a time (unrolled, the tasks' registers spilled).
     auto p4_nc = [&](int x, int g, bool first, bool last) -> float {
       const uint32_t tb = tmem_base + lane_off + (uint32_t)(x * (kTcTmemCols / 2));
-      float* acc = ACC + (size_t)x * (T::ACC_BYTES / 4);  // unused with BLKCH (sums in TMEM)
       float best = 0.f;
-      // adds the powers of 11 complex outputs (words v[o + 2 h], v[o + 2 h + 1])
-      // to the 11 sums a[h ACC_ROWS]: all loads of the sums first, then the
-      // arithmetic, then the stores -- one shared-memory latency per task
-      // instead of one per output (the compiler kept each load behind the
-      // previous store)
-      auto add11 = [&](const uint32_t* v, float* a, bool valid) {
-        float sum[11];
-#pragma unroll
-        for (int h = 0; h < 11; ++h) sum[h] = first ? 0.f : a[h * T::ACC_ROWS];
+      // the 12 sum columns of slot c of tile t (11 used), issued before the
+      // task's one wait on the TMEM loads
+      auto load_sums = [&](int t, int c, uint32_t(&su)[12]) -> uint32_t {
+        const uint32_t sa = tmem_base + lane_off + T::sum_col(t, c);
+        if (!first) {
+          tmem_ld8(sa, *reinterpret_cast<uint32_t(*)[8]>(&su[0]));
+          tmem_ld4(sa + 8, *reinterpret_cast<uint32_t(*)[4]>(&su[8]));
+        }
+        return sa;
+      };
+      // adds the powers of 11 complex outputs (words v[2 h], v[2 h + 1]) to
+      // the sums and stores them back, or after the last block takes their
+      // maximum over the valid rows
+      auto acc11 = [&](const uint32_t* v, uint32_t(&su)[12], uint32_t sa, bool valid) {
 #pragma unroll
         for (int h = 0; h < 11; ++h) {
           const float re = __uint_as_float(v[2 * h]), im = __uint_as_float(v[2 * h + 1]);
-          sum[h] = fmaf(re, re, im * im) + sum[h];
+          su[h] = __float_as_uint(fmaf(re, re, im * im) + (first ? 0.f : __uint_as_float(su[h])));
         }
         if (!last) {
-#pragma unroll
-          for (int h = 0; h < 11; ++h) a[h * T::ACC_ROWS] = sum[h];
+          su[11] = 0u;
+          tmem_st8(sa, *reinterpret_cast<const uint32_t(*)[8]>(&su[0]));
+          tmem_st4(sa + 8, *reinterpret_cast<const uint32_t(*)[4]>(&su[8]));
         } else if (valid) {
 #pragma unroll
-          for (int h = 0; h < 11; ++h) best = fmaxf(best, sum[h]);
+          for (int h = 0; h < 11; ++h) best = fmaxf(best, __uint_as_float(su[h]));
         }
       };
       if constexpr (T::NST == 2) {
         constexpr int NTN = T::LAST_TILES * 4 * 3, TPWN = (NTN + NW - 1) / NW;
-#pragma unroll
+#pragma unroll 1
         for (int i = 0; i < TPWN; ++i) {
           const int task = warp + i * NW;
           if (task >= NTN) break;
@@ -1066,22 +1063,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
             uint32_t(&q)[8] = *reinterpret_cast<uint32_t(*)[8]>(&v[8 * k]);
             tmem_ld8(tb + (uint32_t)(t * T::N2 + s0 + 8 * k), q);
           }
+          uint32_t su[12];
+          const uint32_t sa = load_sums(t, c, su);
           tmem_wait_ld();
           const int r = t * 128 + quad * 32 + lane;
           const bool valid = r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S;
-          float* a = acc + (size_t)(11 * c) * T::ACC_ROWS + r;
           // the chunk starts 22 c - s0 = 0, 6 or 4 words into v (c is
           // uniform over the warp; constant offsets keep v in registers)
           if (c == 0)
-            add11(v, a, valid);
+            acc11(v, su, sa, valid);
           else if (c == 1)
-            add11(v + 6, a, valid);
+            acc11(v + 6, su, sa, valid);
           else
-            add11(v + 4, a, valid);
+            acc11(v + 4, su, sa, valid);
         }
       } else {
         constexpr int NTN = T::LAST_TILES * 4 * 2, TPWN = (NTN + NW - 1) / NW;
-        // one task at a time (unrolled, the tasks' registers spilled)
 #pragma unroll 1
         for (int i = 0; i < TPWN; ++i) {
           const int task = warp + i * NW;
@@ -1089,40 +1086,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
           const int t = task / 8, half = (task >> 2) & 1;
           uint32_t v[24];
           tmem_ld_stage3<T::PAIR3>(tb + (uint32_t)(t * T::N3), half, v);
+          uint32_t su[12];
+          const uint32_t sa = load_sums(t, half, su);
+          tmem_wait_ld();
           const int r = t * 128 + quad * 32 + lane;
           const bool valid = r < T::LAST_NR && g * BC + r / T::LAST_ROWS < S;
-          if constexpr (T::BLKCH) {
-            // sums in TMEM: load, add, store (or take the maximum)
-            const uint32_t sa = tmem_base + lane_off + T::sum_col(t) + (uint32_t)(12 * half);
-            uint32_t su[12];
-            uint32_t(&s8)[8] = *reinterpret_cast<uint32_t(*)[8]>(&su[0]);
-            uint32_t(&s4)[4] = *reinterpret_cast<uint32_t(*)[4]>(&su[8]);
-            if (!first) {
-              tmem_ld8(sa, s8);
-              tmem_ld4(sa + 8, s4);
-            }
-            tmem_wait_ld();
-#pragma unroll
-            for (int h = 0; h < 11; ++h) {
-              const float re = __uint_as_float(v[2 * h]), im = __uint_as_float(v[2 * h + 1]);
-              su[h] = __float_as_uint(fmaf(re, re, im * im) + (first ? 0.f : __uint_as_float(su[h])));
-            }
-            if (!last) {
-              su[11] = 0u;
-              tmem_st8(sa, s8);
-              tmem_st4(sa + 8, s4);
-            } else if (valid) {
-#pragma unroll
-              for (int h = 0; h < 11; ++h) best = fmaxf(best, __uint_as_float(su[h]));
-            }
-          } else {
-            tmem_wait_ld();
-            add11(v, acc + (size_t)(11 * half) * T::ACC_ROWS + r, valid);
-          }
+          acc11(v, su, sa, valid);
         }
-        // the sums' stores land before this thread reads them again
-        if constexpr (T::BLKCH) tmem_wait_st();
       }
+      // the sums' stores land before this thread reads them again
+      tmem_wait_st();
       return best;
     };
 
