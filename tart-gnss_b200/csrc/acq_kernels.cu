@@ -295,6 +295,8 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
       ab_h = c.x;
       prn = c.y;
     }
+    // where the item's key goes: CORR's item w is the row ab_h * n_prn + prn
+    const int key_at = MODE == CAND ? ab_h * p.n_prn + prn : w;
     const int hyp = ab_h & 1;
     // CORR: running maximum of |y|^2 and a compact code of its position
     // ((rho*31 + a)*33 + b)*16 + c; the lag is decoded only on ties and once
@@ -462,8 +464,7 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
       }
       if ((tid & 31) == 0) atomicMax(&s_key, kbest);
       __syncthreads();
-      // CORR's item w is the row ab_h * n_prn + prn
-      if (tid == 0) p.keys[(size_t)ab_h * p.n_prn + prn] = s_key;
+      if (tid == 0) p.keys[key_at] = s_key;
     } else if (MODE == SECOND) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) pbest = fmaxf(pbest, __shfl_xor_sync(0xffffffffu, pbest, o));

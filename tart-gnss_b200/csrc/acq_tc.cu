@@ -736,13 +736,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
     // product units of this thread: unit e = tid + k NTS is (row r, chunk j);
     // packed (code unit index << 16) | operand byte offset
     uint32_t uoff[U];
+    // and, with BC > 1, the residue slot s < BC of each unit, 4 bits per
+    // unit (the unit's Z offset in its item is s * 8 ROWS1 + its code-unit
+    // index)
+    uint32_t uslot = 0u;
+    static_assert(U <= 8 && BC <= 16, "packed unit slots");
 #pragma unroll
     for (int k = 0; k < U; ++k) {
       const int e = tid + k * NTS;
       const int j = e / T::NR1, r = e - j * T::NR1;
-      const int u = r - (r / T::ROWS1) * T::ROWS1;
+      const int sl = r / T::ROWS1, u = r - sl * T::ROWS1;
       uoff[k] = e < T::UNITS ? ((uint32_t)(j * T::ROWS1 + u) << 16) | (uint32_t)(T::arow1(r) * 16 + j * T::LBO1)
                              : 0u;
+      if (BC > 1 && e < T::UNITS) uslot |= (uint32_t)sl << (4 * k);
     }
     uint32_t ph_done[2] = {0u, 0u}, ph_code[2] = {0u, 0u};
     bool failed = false;
@@ -1106,35 +1112,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       uint4 zr[U];
       auto load_z = [&](int blk) {
         // the drop-in search reads its Z once (evict first); the
-        // non-coherent search reads each block again for every PRN (pair),
+        // non-coherent search reads each block again for every PRN,
         // so it keeps the blocks in L2.  blk >= B (BLKCH, B odd) stands for
         // zero data, which adds nothing to the sums.
         const uint4* seq = p.z16 + (((size_t)ab_h * B + blk) * S + (size_t)g * BC) * 8 * T::ROWS1;
-        if constexpr (BC == 1) {
-          // one residue per item: unit e's offset in its sequence is its
-          // code-unit index, the high half of uoff
-          const bool any = g < S && blk < B;
+        const int live = blk < B ? S - g * BC : 0;  // residue slots with data
 #pragma unroll
-          for (int k = 0; k < U; ++k) {
-            zr[k] = make_uint4(0u, 0u, 0u, 0u);
-            if (any && (k < U - 1 || tid + k * NTS < T::UNITS)) {
-              const uint4* src = seq + (uoff[k] >> 16);
-              zr[k] = NCB ? __ldcg(src) : __ldcs(src);
-            }
-          }
-        } else {
-#pragma unroll
-          for (int k = 0; k < U; ++k) {
-            const int e = tid + k * NTS;
-            zr[k] = make_uint4(0u, 0u, 0u, 0u);
-            if (e < T::UNITS) {
-              const int j = e / T::NR1, r = e - j * T::NR1;
-              const int s = r / T::ROWS1, u = r - s * T::ROWS1;
-              if (g * BC + s < S && blk < B) {
-                const uint4* src = seq + ((size_t)s * 8 + j) * T::ROWS1 + u;
-                zr[k] = NCB ? __ldcg(src) : __ldcs(src);
-              }
-            }
+        for (int k = 0; k < U; ++k) {
+          zr[k] = make_uint4(0u, 0u, 0u, 0u);
+          const int sl = BC == 1 ? 0 : (int)((uslot >> (4 * k)) & 15u);
+          if (sl < live && (k < U - 1 || tid + k * NTS < T::UNITS)) {
+            const uint4* src = seq + (uint32_t)sl * (8u * T::ROWS1) + (uoff[k] >> 16);
+            zr[k] = NCB ? __ldcg(src) : __ldcs(src);
           }
         }
       };
