@@ -88,6 +88,21 @@ __device__ __forceinline__ uint32_t mbar_try_wait(uint64_t* bar, uint32_t parity
       : "memory");
   return done;
 }
+// The same test with a suspend-time hint: a thread whose phase has not
+// completed sleeps until it completes or `ns` nanoseconds pass, instead of
+// returning at once to poll again, so waiting warps leave their
+// sub-partition's issue slots to the warps that work.
+__device__ __forceinline__ uint32_t mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return done;
+}
 // D[tmem] (+)= A[smem desc] * B[smem desc]^T, kind::f16, no lanes masked.
 __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
   const uint32_t z = 0;
@@ -205,6 +220,7 @@ constexpr int kTcThreads = kSimtThreads + 96;
 constexpr int kTcTmemCols = 512;
 constexpr long long kWaitPolls = 1LL << 22;
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per wait on the tensor cores
+constexpr uint32_t kSuspendNs = 20000;                  // longest sleep of one test (20 us)
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
   unsigned long long t;
@@ -212,14 +228,15 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   return t;
 }
 // polls the mbarrier phase until it completes, at most kWaitPolls times and
-// kWaitNs nanoseconds (a suspended try_wait has no fixed duration)
+// kWaitNs nanoseconds; after the first test each one may sleep up to
+// kSuspendNs (woken when the phase completes), so the bound is on the timer
 __device__ __forceinline__ uint32_t bounded_wait(uint64_t* bar, uint32_t phase) {
   uint32_t done = mbar_try_wait(bar, phase);
   if (done) return done;  // the common case reads no timer
   const unsigned long long t0 = globaltimer_ns();
   for (long long k = 0; k < kWaitPolls && !done; ++k) {
-    done = mbar_try_wait(bar, phase);
-    if (!done && (k & 63) == 63 && globaltimer_ns() - t0 > kWaitNs) break;
+    done = mbar_try_wait_sleep(bar, phase, kSuspendNs);
+    if (!done && (k & 7) == 7 && globaltimer_ns() - t0 > kWaitNs) break;
   }
   return done;
 }
