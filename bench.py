@@ -826,6 +826,16 @@ def main():
     lib.tga_last_transfer_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
                                             ctypes.POINTER(ctypes.c_uint64)]
     lib.tga_last_transfer_bytes(ctx._h, ctypes.byref(h2d), ctypes.byref(d2h))
+    # the same searches as a stream of observations (tga_acquire_all_stream):
+    # the copy of observation i + 1 overlaps the search of observation i
+    stream_s = None
+    if not args.no_e2e and not (args.sharded and world > 1):
+        seq = [host] * max(args.steps, 2)
+        ctx.acquire_cells_stream(seq, FS, mask=tga.ALL, cn0=True)  # warm-up: both buffers' plans
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.acquire_cells_stream(seq, FS, mask=tga.ALL, cn0=True)
+        stream_s = (time.perf_counter() - t0) / len(seq)
     e2e_s = statistics.mean(e2e_times) if e2e_times else float("nan")
     if world > 1:
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
@@ -843,6 +853,11 @@ def main():
             "e2e": {"value": job_cells / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": h2d.value,
                     "d2h_bytes_per_step": d2h.value, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": launches,
+            "e2e_stream": None if stream_s is None else {
+                "value": job_cells / stream_s, "unit": "cells/s", "ms_per_observation": stream_s * 1e3,
+                "observations": max(args.steps, 2),
+                "how": "tga_acquire_all_stream over the steps' observations from pinned host memory: each copy "
+                       "overlaps the previous search"},
             "roofline": roofline(agg, args.precision, sm_mhz),
             "kernels": kernels(agg),
             "clocks": clocks}

@@ -205,6 +205,17 @@ int tga_acquire_single_static(int constellation, const float* d_signal_f32,
 int tga_acquire_all(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, size_t row_bytes,
                     double sampling_freq, const tga_all_options* opt, tga_cell* out,
                     size_t out_capacity, size_t* n_out);
+/* A stream of observations: n_obs recordings of the same shape searched one
+ * after the other with the same options, each exactly as tga_acquire_all
+ * would search it (the cells of observation i at out + i * C, C the count
+ * of tga_all_cell_count; *n_out = n_obs * C), while the host-to-device copy
+ * of observation i + 1 runs on a second stream during the search of
+ * observation i (two device buffers, alternated).  The host rows should be
+ * pinned for the copies to overlap.  No counterpart in the reference: it
+ * serves a receiver that acquires on a stream of recordings. */
+int tga_acquire_all_stream(tga_ctx* ctx, const uint8_t* const* h_packed_bits, size_t n_obs, size_t n_ant,
+                           size_t row_bytes, double sampling_freq, const tga_all_options* opt, tga_cell* out,
+                           size_t out_capacity, size_t* n_out);
 int tga_acquire_all_device(tga_ctx* ctx, const uint8_t* d_packed_bits, size_t n_ant,
                            size_t row_bytes, double sampling_freq, const tga_all_options* opt,
                            tga_cell* out, size_t out_capacity, size_t* n_out);

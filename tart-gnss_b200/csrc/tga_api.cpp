@@ -44,6 +44,10 @@ struct tga_ctx {
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
+  // tga_acquire_all_stream: the stream of the host-to-device copies and the
+  // event of each of its two bits buffers (created on first use)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copied[2] = {nullptr, nullptr};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::string err;
   std::map<std::string, DevBuf> bufs;
@@ -1063,6 +1067,9 @@ int tga_destroy(tga_ctx* ctx) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   for (auto& kv : ctx->bufs)
     if (kv.second.p) cudaFree(kv.second.p);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  for (cudaEvent_t& e : ctx->copied)
+    if (e) cudaEventDestroy(e);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
@@ -1117,6 +1124,52 @@ int tga_acquire_all(tga_ctx* ctx, const uint8_t* h_packed_bits, size_t n_ant, si
     CK(cudaMemcpyAsync(d_bits, h_packed_bits, bytes, cudaMemcpyHostToDevice, ctx->stream));
     ctx->h2d += bytes;
     return acquire_all_impl(ctx, d_bits, n_ant, row_bytes, sampling_freq, opt, out, out_capacity, n_out);
+  });
+}
+
+int tga_acquire_all_stream(tga_ctx* ctx, const uint8_t* const* h_packed_bits, size_t n_obs, size_t n_ant,
+                           size_t row_bytes, double sampling_freq, const tga_all_options* opt, tga_cell* out,
+                           size_t out_capacity, size_t* n_out) {
+  return guarded(ctx, [&] {
+    if (!h_packed_bits || !opt || !n_out) throw InvalidArg("null argument");
+    for (size_t i = 0; i < n_obs; ++i)
+      if (!h_packed_bits[i]) throw InvalidArg("null bits of observation " + std::to_string(i));
+    size_t per = 0;
+    int rc = tga_all_cell_count(n_ant, opt, &per);
+    if (rc != TGA_OK) return rc;
+    *n_out = per * n_obs;
+    if (!out) return TGA_OK;
+    if (out_capacity < per * n_obs) return TGA_ERR_CAPACITY;
+    if (n_obs == 0) return TGA_OK;
+    if (!ctx->copy_stream) {
+      CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+      for (cudaEvent_t& e : ctx->copied) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    const size_t bytes = n_ant * row_bytes;
+    begin_call(ctx);
+    // both buffers before the first search, so that neither is reallocated
+    // (and the searches' cached graphs stay valid) in the middle of the run
+    uint8_t* buf[2] = {(uint8_t*)ctx->buf("bits", bytes), (uint8_t*)ctx->buf("bits.2", bytes)};
+    auto copy = [&](size_t i) {
+      CK(cudaMemcpyAsync(buf[i & 1], h_packed_bits[i], bytes, cudaMemcpyHostToDevice, ctx->copy_stream));
+      CK(cudaEventRecord(ctx->copied[i & 1], ctx->copy_stream));
+      ctx->h2d += bytes;
+    };
+    // the copy of observation i + 1 is queued before the search of i, which
+    // returns only when it has finished (so buffer (i + 1) & 1, read by
+    // search i - 1, is free)
+    copy(0);
+    double total_ms = 0.0;
+    size_t n_i = 0;
+    for (size_t i = 0; i < n_obs; ++i) {
+      CK(cudaStreamWaitEvent(ctx->stream, ctx->copied[i & 1], 0));
+      if (i + 1 < n_obs) copy(i + 1);
+      rc = acquire_all_impl(ctx, buf[i & 1], n_ant, row_bytes, sampling_freq, opt, out + i * per, per, &n_i);
+      if (rc != TGA_OK) return rc;
+      total_ms += ctx->last_ms;
+    }
+    ctx->last_ms = total_ms;
+    return TGA_OK;
   });
 }
 

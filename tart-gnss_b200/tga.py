@@ -159,6 +159,8 @@ def lib():
         getattr(L, nm).argtypes = [_P, _P, _P, sz, dbl, dbl, dbl, i32, sz, ctypes.POINTER(Result)]
     L.tga_acquire_all.argtypes = [_P, _P, sz, sz, dbl, ctypes.POINTER(AllOptions), _P, sz, ctypes.POINTER(sz)]
     L.tga_acquire_all_device.argtypes = L.tga_acquire_all.argtypes
+    L.tga_acquire_all_stream.argtypes = [_P, _P, sz, sz, sz, dbl, ctypes.POINTER(AllOptions), _P, sz,
+                                         ctypes.POINTER(sz)]
     L.tga_all_cell_count.argtypes = [sz, ctypes.POINTER(AllOptions), ctypes.POINTER(sz)]
     L.tga_last_search_stats.argtypes = [_P, ctypes.POINTER(dbl), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(dbl)]
     L.tga_acr_cn0.argtypes = [_P, _P, sz, i32, _P, _P]
@@ -370,6 +372,28 @@ class Context:
                        len(out), ctypes.byref(n)))
         del keep
         return out
+
+    def acquire_cells_stream(self, observations, sampling_freq, mask=ALL, ant_filter=None, prn_filter=None,
+                             center_freq=GPS_IF, search_band=GPS_SEARCH_BAND, cn0=False):
+        """tga_acquire_all_stream: a list of host observations of one shape
+        [n_ant, row_bytes] searched in turn, the copy of the next one
+        overlapping the search of the current one.  Returns one cell array
+        per observation."""
+        obs = [np.ascontiguousarray(o, dtype=np.uint8) for o in observations]
+        n_ant, row_bytes = obs[0].shape
+        if any(o.shape != (n_ant, row_bytes) for o in obs):
+            raise ValueError("observations of different shapes")
+        o, keep = self._options(mask, ant_filter, prn_filter, center_freq, search_band, cn0, False)
+        ptrs = (ctypes.c_void_p * len(obs))(*[x.ctypes.data for x in obs])
+        n = ctypes.c_size_t()
+        self._check(lib().tga_acquire_all_stream(self._h, ptrs, len(obs), n_ant, row_bytes, float(sampling_freq),
+                                                 ctypes.byref(o), None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, dtype=CELL_DTYPE)
+        self._check(lib().tga_acquire_all_stream(self._h, ptrs, len(obs), n_ant, row_bytes, float(sampling_freq),
+                                                 ctypes.byref(o), _ptr(out), len(out), ctypes.byref(n)))
+        del keep
+        per = len(out) // len(obs)
+        return [out[i * per:(i + 1) * per] for i in range(len(obs))]
 
     def acquire_all(self, packed_bits, sampling_freq, mask=ALL, ant_filter=None, prn_filter=None,
                     center_freq=GPS_IF, search_band=GPS_SEARCH_BAND, cn0=False, debug=False):

@@ -135,3 +135,26 @@ def test_timeout_reported_through_captured_and_replayed_graphs():
         ref.set_graphs(False)
         ref.set_precision(tga.PRECISION_FP16_TC)
         _same(got, ref.acquire_cells(bits, FS, mask=mask, prn_filter=[5]))
+
+
+def test_stream_of_observations_equals_single_calls():
+    """tga_acquire_all_stream: four observations (two distinct recordings,
+    each twice, so both alternated buffers serve a cached graph plan) in
+    one call, the copy of each overlapping the previous search; every
+    observation's cells equal a separate tga_acquire_all call, in both
+    arithmetics."""
+    import torch
+    rng = np.random.default_rng(404)
+    obs = []
+    for _ in range(2):
+        host = torch.from_numpy(rng.integers(0, 256, size=(4, 40920), dtype=np.uint8)).pin_memory().numpy()
+        obs.append(host)
+    seq = [obs[0], obs[1], obs[0], obs[1]]
+    with tga.Context(0) as ctx:
+        for prec in (tga.PRECISION_FP32, tga.PRECISION_FP16_TC):
+            ctx.set_precision(prec)
+            want = [ctx.acquire_cells(o, 16.368e6, mask=tga.ALL, cn0=True) for o in obs]
+            got = ctx.acquire_cells_stream(seq, 16.368e6, mask=tga.ALL, cn0=True)
+            assert len(got) == 4
+            for i, g in enumerate(got):
+                assert np.array_equal(g, want[i % 2]), (prec, i)
