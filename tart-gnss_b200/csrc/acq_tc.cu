@@ -539,28 +539,33 @@ __device__ __forceinline__ void tmem_ld_stage3(uint32_t taddr, int half, uint32_
 // The code warp's thread: after the 12 SIMT warps have formed chain x's
 // products of a PRN's last block (s_p1[x]), bulk-copy the chain's next code
 // block into its slot (s_code[x]).  Its own function, so that its registers
-// are allocated apart from the SIMT warps'.
+// are allocated apart from the SIMT warps'.  The parameters it needs come
+// as scalars: a reference to the kernel's parameter block would make the
+// kernel copy the block to local memory and read every field from there.
 template <class T, bool NCB>
-__device__ __noinline__ void code_warp(const Tc3Params& p, uint64_t* s_p1, uint64_t* s_code, unsigned char* CODE0,
-                                       int n_rounds) {
+__device__ __noinline__ void code_warp(const uint4* d16, int groups, int split_nc, int n_items, int n_prn, int* err,
+                                       uint64_t* s_p1, uint64_t* s_code, unsigned char* CODE0, int n_rounds) {
   // the PRN of chain x in round r: PRN pairs, or with BLKCH one PRN per round
   auto prn_of = [&](int r, int x) -> int {
     if (T::BLKCH) return r;
-    return 2 * r + x < p.n_prn ? 2 * r + x : p.n_prn - 1;
+    return 2 * r + x < n_prn ? 2 * r + x : n_prn - 1;
   };
-  uint32_t ph_p1[2] = {0u, 0u};
-  int fetches[2] = {0, 0};
+  // bit x for barrier / slot x, in registers (the loops over x are not
+  // unrolled; arrays indexed by x would live in local memory): the phase of
+  // s_p1[x], the parity of the copies issued into slot x and whether any was
+  uint32_t ph_p1 = 0u, fetch_par = 0u, fetch_any = 0u;
   bool ok = true;
   // code block of chain x for round r of work item w, into slot `slot`
   auto fetch = [&](int slot, int x, int w, int r) {
-    const int hyp = NCB ? 0 : (w / p.groups) & 1;
-    const uint4* src = p.d16 + ((size_t)prn_of(r, x) * 2 + hyp) * 8 * T::ROWS1;
+    const int hyp = NCB ? 0 : (w / groups) & 1;
+    const uint4* src = d16 + ((size_t)prn_of(r, x) * 2 + hyp) * 8 * T::ROWS1;
     mbar_arrive_expect_tx(&s_code[slot], (uint32_t)T::CODE_BYTES);
     bulk_g2s(smem_addr(CODE0 + slot * T::CODE_REGION), src, (uint32_t)T::CODE_BYTES, &s_code[slot]);
-    ++fetches[slot];
+    fetch_par ^= 1u << slot;
+    fetch_any |= 1u << slot;
   };
-  const int split = NCB ? p.split : 1;  // the drop-in search always has enough items
-  const int n_units = p.n_items * split;
+  const int split = NCB ? split_nc : 1;  // the drop-in search always has enough items
+  const int n_units = n_items * split;
   constexpr int NSLOT = T::BLKCH ? 1 : 2;
   if ((int)blockIdx.x < n_units && n_rounds > 0)
     for (int x = 0; x < NSLOT; ++x) fetch(x, x, blockIdx.x / split, unit_round0(split, blockIdx.x, n_rounds));
@@ -573,8 +578,8 @@ __device__ __noinline__ void code_warp(const Tc3Params& p, uint64_t* s_p1, uint6
       // products of the PRN's last blocks
       if constexpr (T::BLKCH) {
         for (int x = 0; x < 2 && ok; ++x) {
-          ok = bounded_wait(&s_p1[x], ph_p1[x]) != 0;
-          ph_p1[x] ^= 1u;
+          ok = bounded_wait(&s_p1[x], (ph_p1 >> x) & 1u) != 0;
+          ph_p1 ^= 1u << x;
         }
         if (!ok) break;
         if (r + 1 < r1)
@@ -584,11 +589,11 @@ __device__ __noinline__ void code_warp(const Tc3Params& p, uint64_t* s_p1, uint6
       } else {
 #pragma unroll 1
         for (int x = 0; x < 2 && ok; ++x) {
-          if (!bounded_wait(&s_p1[x], ph_p1[x])) {
+          if (!bounded_wait(&s_p1[x], (ph_p1 >> x) & 1u)) {
             ok = false;
             break;
           }
-          ph_p1[x] ^= 1u;
+          ph_p1 ^= 1u << x;
           if (r + 1 < r1)
             fetch(x, x, w, r + 1);
           else if (un < n_units)
@@ -599,8 +604,8 @@ __device__ __noinline__ void code_warp(const Tc3Params& p, uint64_t* s_p1, uint6
   }
   // drain: the last bulk copy of each slot
   for (int x = 0; x < NSLOT; ++x)
-    if (fetches[x] > 0) bounded_wait(&s_code[x], (uint32_t)((fetches[x] - 1) & 1));
-  if (!ok) atomicExch(p.err, 1);
+    if ((fetch_any >> x) & 1u) bounded_wait(&s_code[x], ((fetch_par >> x) & 1u) ^ 1u);
+  if (!ok) atomicExch(err, 1);
 }
 
 template <int M, bool NCB>
@@ -745,7 +750,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
     __syncwarp();
   } else if (warp == NW + 2) {
     // ---------------- code warp: one thread fetches the code blocks ----------------
-    if (lane == 0) code_warp<T, NCB>(p, s_p1, s_code, CODE0, n_rounds);
+    if (lane == 0) code_warp<T, NCB>(p.d16, p.groups, p.split, p.n_items, p.n_prn, p.err, s_p1, s_code, CODE0, n_rounds);
     __syncwarp();
   } else {
     // ---------------- SIMT warps ----------------
@@ -767,7 +772,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
                              : 0u;
       if (BC > 1 && e < T::UNITS) uslot |= (uint32_t)sl << (4 * k);
     }
-    uint32_t ph_done[2] = {0u, 0u}, ph_code[2] = {0u, 0u};
+    // mbarrier phases, bit x for chain (or code slot) x: in registers (the
+    // chain loops are not unrolled; arrays indexed by x would live in local
+    // memory, and every wait would first load its phase from there)
+    uint32_t ph_done = 0u, ph_code = 0u;
     bool failed = false;
 
     // bounded wait of the whole warp: every lane tests the phase (one
@@ -1154,8 +1162,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
       auto products = [&](int x, bool new_code, uint32_t code_ready = 0u) -> bool {
         const int c = slot(x);
         if (new_code) {
-          if (!__all_sync(0xffffffffu, code_ready) && !warp_wait(&s_code[c], ph_code[c])) return false;
-          ph_code[c] ^= 1u;
+          if (!__all_sync(0xffffffffu, code_ready) && !warp_wait(&s_code[c], (ph_code >> c) & 1u)) return false;
+          ph_code ^= 1u << c;
         }
         p1(zr, A0 + x * T::A_BYTES, CODE0 + c * T::CODE_REGION);
         signal(x);
@@ -1198,11 +1206,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
         for (int st = 0; st < T::NST - 1 && !failed; ++st) {
 #pragma unroll 1
           for (int x = 0; x < 2; ++x) {
-            if (!warp_wait(&s_done[x], ph_done[x])) {
+            if (!warp_wait(&s_done[x], (ph_done >> x) & 1u)) {
               failed = true;
               break;
             }
-            ph_done[x] ^= 1u;
+            ph_done ^= 1u << x;
             tc_fence_after();
             if (st == 0)
               p2(x);
@@ -1215,17 +1223,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
         // step, so that the tensor cores are not left idle across rounds
 #pragma unroll 1
         for (int x = 0; x < 2 && !failed; ++x) {
-          if (!warp_wait(&s_done[x], ph_done[x])) {
+          if (!warp_wait(&s_done[x], (ph_done >> x) & 1u)) {
             failed = true;
             break;
           }
-          ph_done[x] ^= 1u;
+          ph_done ^= 1u << x;
           tc_fence_after();
           // a new PRN starts with the next step (BLKCH: chain a waits for
           // the shared slot, chain b follows it); test its code block now,
           // use the answer after P4
           const bool new_code = more && b + 1 == NI && (!T::BLKCH || x == 0);
-          const uint32_t code_ready = new_code ? mbar_try_wait(&s_code[slot(x)], ph_code[slot(x)]) : 0u;
+          const uint32_t code_ready = new_code ? mbar_try_wait(&s_code[slot(x)], (ph_code >> slot(x)) & 1u) : 0u;
           // non-negative floats order like their bit patterns
           float pmax;
           if constexpr (NCB) {
