@@ -265,6 +265,32 @@ cudaError_t launch_frontend(const SampleSource& src, const SearchDims& dims, con
 // ---------------------------------------------------------------------------
 // prime-factor transform engine
 // ---------------------------------------------------------------------------
+// The four largest (value, index) pairs seen by a thread, largest first;
+// values are non-negative |y|^2 (as bits they order like unsigned
+// integers), an empty place holds 0.
+struct Top4 {
+  float v[4] = {0.f, 0.f, 0.f, 0.f};
+  int i[4] = {0, 0, 0, 0};
+  __device__ __forceinline__ void add(float x, int k) {
+    if (!(x > v[3])) return;
+    const bool g0 = x > v[0], g1 = x > v[1], g2 = x > v[2];
+    v[3] = g2 ? v[2] : x;
+    i[3] = g2 ? i[2] : k;
+    v[2] = g1 ? v[1] : (g2 ? x : v[2]);
+    i[2] = g1 ? i[1] : (g2 ? k : i[2]);
+    v[1] = g0 ? v[0] : (g1 ? x : v[1]);
+    i[1] = g0 ? i[0] : (g1 ? k : i[1]);
+    v[0] = g0 ? x : v[0];
+    i[0] = g0 ? k : i[0];
+  }
+  __device__ __forceinline__ void pop() {
+    v[0] = v[1], i[0] = i[1];
+    v[1] = v[2], i[1] = i[2];
+    v[2] = v[3], i[2] = i[3];
+    v[3] = 0.f;
+  }
+};
+
 template <int M, int BC, int NT, int MINB, int MODE>
 __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
   using G = Geo<M>;
@@ -274,6 +300,13 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
   extern __shared__ float2 buf[];
   __shared__ unsigned long long s_key;
   __shared__ unsigned int s_p2;
+  // CAND with p2rows: for every residue of the row and every warp that
+  // scanned it, its four largest |y|^2 as (value bits << 32) | lag, after
+  // the transform buffer (TOP_WPS warps per residue)
+  constexpr bool TOP = MODE == CAND;
+  constexpr int TOP_WPS = NT / 32 / BC >= 1 ? NT / 32 / BC : 1;
+  unsigned long long* s_res = reinterpret_cast<unsigned long long*>(buf + BC * LC);
+  const bool keep_top = TOP && p.p2rows != nullptr;
   const int tid = threadIdx.x;
   const int S = p.S;
   const int groups = INV ? (S + BC - 1) / BC : 1;
@@ -344,6 +377,9 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
             }
             cmax = pw > pmax ? code : cmax;
             pmax = fmaxf(pw, pmax);
+            // kept in place for the second peak: the stage read its inputs
+            // from these positions into registers before any output
+            if (keep_top) reinterpret_cast<float*>(buf)[2 * (s * LC + G::offset(a, b, c))] = pw;
           } else {
             const int tau = seq_of(s) + S * G::natural(a, b, c);
             int d = tau - tau_star;
@@ -425,6 +461,53 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
         }
       }
       __syncthreads();
+      // CAND with p2rows: the four largest |y|^2 of every residue of the
+      // group (kept in place in buf) with their lags.  TOP_WPS warps scan a
+      // residue; each takes the fourth largest of its lanes' maxima as a
+      // lower bound on its four largest values, keeps per lane the four
+      // largest values at or above it, and stores the warp's four largest.
+      if (TOP && keep_top) {
+        const int warp = tid >> 5, lane = tid & 31;
+        const int sl = warp / TOP_WPS, sub = warp - sl * TOP_WPS;
+        if (sl < BC && seq_of(sl) >= 0) {  // uniform over the warp
+          const float* pws = reinterpret_cast<const float*>(buf + sl * LC);
+          unsigned mb = 0u;
+          for (int i = sub * 32 + lane; i < LC; i += TOP_WPS * 32) mb = max(mb, __float_as_uint(pws[2 * i]));
+          unsigned thr = 0u;
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            thr = __reduce_max_sync(0xffffffffu, mb);
+            const unsigned h = __ballot_sync(0xffffffffu, mb == thr);
+            if (lane == __ffs(h) - 1) mb = 0u;
+          }
+          Top4 t;
+          for (int i = sub * 32 + lane; i < LC; i += TOP_WPS * 32) {
+            const float x = pws[2 * i];
+            if (__float_as_uint(x) >= thr) t.add(x, i);
+          }
+          const int rho = seq_of(sl);
+          unsigned long long* dst = s_res + ((size_t)rho * TOP_WPS + sub) * 4;
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const unsigned vb = __float_as_uint(t.v[0]);
+            const unsigned x = __reduce_max_sync(0xffffffffu, vb);
+            const unsigned h = __ballot_sync(0xffffffffu, vb == x);
+            const int src = __ffs(h) - 1;
+            const int i = __shfl_sync(0xffffffffu, t.i[0], src);
+            if (lane == src) t.pop();
+            if (lane == r) {
+              unsigned long long k = 0ull;
+              if (x != 0u) {
+                const int a = i / COLS, rem = i - a * COLS, c = rem / 33, b = rem - c * 33;
+                k = ((unsigned long long)x << 32) | (unsigned)(rho + S * G::natural(a, b, c));
+              }
+              dst[r] = k;
+            }
+          }
+        }
+        // the next group's stage 1 overwrites the values scanned here
+        __syncthreads();
+      }
       // tensor-core operands: FP16 units straight from the transformed
       // sequences in shared memory (the work of tc_pack_kernel, without
       // reading the FP32 spectra back from memory)
@@ -465,6 +548,26 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
       if ((tid & 31) == 0) atomicMax(&s_key, kbest);
       __syncthreads();
       if (tid == 0) p.keys[key_at] = s_key;
+      // CAND with p2rows: the row's second peak against its own maximum,
+      // the largest |y|^2 more than chip_width lags (circularly) from it.
+      // At most ceil((2 chip_width + 1) / S) <= 3 lags of a residue lie that
+      // close, so the four largest of each residue (among the lists of the
+      // warps that scanned it) hold it.
+      if (TOP && keep_top && tid < 32) {
+        const unsigned long long kb = s_key;
+        const int tau_star = (int)(unsigned)kb;
+        float p2 = 0.f;
+        if (kb != 0ull)
+          for (int e = tid; e < S * TOP_WPS * 4; e += 32) {
+            const unsigned long long k = s_res[e];
+            int d = (int)(unsigned)k - tau_star;
+            d = d < 0 ? -d : d;
+            if (k != 0ull && min(d, p.P - d) > p.chip_width) p2 = fmaxf(p2, __uint_as_float((unsigned)(k >> 32)));
+          }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) p2 = fmaxf(p2, __shfl_xor_sync(0xffffffffu, p2, o));
+        if (tid == 0) p.p2rows[key_at] = p2;
+      }
     } else if (MODE == SECOND) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) pbest = fmaxf(pbest, __shfl_xor_sync(0xffffffffu, pbest, o));
@@ -513,7 +616,12 @@ template <int M, int V, int MODE>
 static cudaError_t run_pfa(const PfaParams& p, int n_work_slots, int num_sms, cudaStream_t st) {
   using C = PfaCfg<M, V>;
   constexpr int LC = Geo<M>::LC;
-  const size_t smem = (size_t)C::BC * LC * sizeof(float2);
+  size_t smem = (size_t)C::BC * LC * sizeof(float2);
+  // CAND with p2rows: the four largest |y|^2 per residue and scanning warp
+  if (MODE == CAND && p.p2rows) {
+    constexpr int WPS = C::NT / 32 / C::BC >= 1 ? C::NT / 32 / C::BC : 1;
+    smem += (size_t)p.S * WPS * 4 * sizeof(unsigned long long);
+  }
   auto kern = pfa_kernel<M, C::BC, C::NT, C::MINB, MODE>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -659,8 +767,11 @@ cudaError_t launch_second_peak(const PolyClass& pc, const SearchDims& dims, cons
 
 cudaError_t launch_correlate_listed(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
                                     const float2* d_D, const int2* d_cand, const int* d_count, int capacity,
-                                    unsigned long long* d_keys, int num_sms, cudaStream_t st) {
+                                    unsigned long long* d_keys, int num_sms, cudaStream_t st, float* d_p2rows,
+                                    int chip_width) {
   PfaParams p = {};
+  p.p2rows = d_p2rows;
+  p.chip_width = chip_width;
   p.z = const_cast<float2*>(d_Z);
   p.D = d_D;
   p.keys = d_keys;
@@ -671,6 +782,25 @@ cudaError_t launch_correlate_listed(const PolyClass& pc, const SearchDims& dims,
   p.P = pc.P;
   p.n_items = capacity;
   return dispatch_pfa<CAND>(pc, p, p.n_items, num_sms, st);
+}
+
+// The second peak of each cell from the re-evaluated rows: the cell's
+// chosen row is always one of them (its FP32 key is the cell's maximum; when
+// every key is 0, every row was listed).
+__global__ void second_from_rows_kernel(int n_cells, int n_prn, const float* __restrict__ p2rows,
+                                        BestRow* __restrict__ best) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= n_cells) return;
+  const BestRow b = best[w];
+  best[w].p2 = p2rows[(size_t)(b.ab * 2 + b.hyp) * n_prn + (w % n_prn)];
+}
+
+cudaError_t launch_second_from_rows(const SearchDims& dims, const float* d_p2rows, BestRow* d_best,
+                                    cudaStream_t st) {
+  const int n = dims.n_ant * dims.n_prn;
+  if (n <= 0) return cudaSuccess;
+  second_from_rows_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, dims.n_prn, d_p2rows, d_best);
+  return TGA_LAUNCHED();
 }
 
 // Rows of a reduced-precision search to re-evaluate in FP32.  Per (antenna,

@@ -102,10 +102,16 @@ cudaError_t launch_correlate(const PolyClass& pc, const SearchDims& dims, const 
                              cudaStream_t st);
 // launch_correlate over the rows listed in d_cand (*d_count of them, at
 // most capacity): each listed row's FP32 key is written where
-// launch_correlate would write it; other keys are left as they are.
+// launch_correlate would write it; other keys are left as they are.  With
+// d_p2rows, each listed row's second peak against its own maximum (what
+// launch_second_peak computes for a chosen row) is written there as well.
 cudaError_t launch_correlate_listed(const PolyClass& pc, const SearchDims& dims, const float2* d_Z,
                                     const float2* d_D, const int2* d_cand, const int* d_count, int capacity,
-                                    unsigned long long* d_keys, int num_sms, cudaStream_t st);
+                                    unsigned long long* d_keys, int num_sms, cudaStream_t st,
+                                    float* d_p2rows = nullptr, int chip_width = 0);
+// d_best[w].p2 = d_p2rows at the row d_best[w] chose (the keys' layout).
+cudaError_t launch_second_from_rows(const SearchDims& dims, const float* d_p2rows, BestRow* d_best,
+                                    cudaStream_t st);
 // Lists, per (antenna, PRN), the rows whose reduced-precision key is at least
 // keep x the largest of its nb * n_hyp rows (appended to d_cand, counted in
 // *d_count, which must start at 0; d_cand holds up to n_ant * nb * n_hyp *

@@ -81,6 +81,8 @@ struct PfaParams {
   BestRow* best;              // SECOND in/out
   const int2* cand;           // CAND: the rows to evaluate
   const int* cand_count;      // CAND: their number (device)
+  float* p2rows;              // CAND (optional): each listed row's second peak
+                              // against its own maximum, where its key goes
   uint4* z16;                 // FWD_Z (optional): the transformed sequences also as TcUnits, x z16_scale
   const uint2* z16_map;       // per unit: the 4 src_offset values as 16-bit fields (0xffff: zero)
   float z16_scale;

@@ -487,6 +487,8 @@ struct GroupBufs {
   unsigned long long* keys32 = nullptr;
   int2* cand = nullptr;
   int* count = nullptr;
+  // and each re-evaluated row's second peak against its own maximum
+  float* p2rows = nullptr;
 };
 
 GroupBufs prepare_group(tga_ctx* ctx, const ClassGroup& grp, int n_ant, int nb, const std::string& tag) {
@@ -523,6 +525,7 @@ GroupBufs prepare_group(tga_ctx* ctx, const ClassGroup& grp, int n_ant, int nb, 
     b.z16 = ctx->buf(tag + ".z16", tc_operand_bytes(pc, n_zseq, false));
     b.d16 = ctx->buf(tag + ".d16", tc_operand_bytes(pc, (long long)n_prn * 2, true));
     b.keys32 = (unsigned long long*)ctx->buf(tag + ".keys32", (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long));
+    b.p2rows = (float*)ctx->buf(tag + ".p2rows", (size_t)n_ab * 2 * n_prn * sizeof(float));
     b.cand = (int2*)ctx->buf(tag + ".cand", (size_t)n_ab * 2 * n_prn * sizeof(int2));
     b.count = (int*)ctx->buf(tag + ".count", sizeof(int));
     // DFT matrices of the class (they depend on Lc only), uploaded once per context
@@ -559,6 +562,11 @@ void enqueue_group(tga_ctx* ctx, const ClassGroup& grp, const GroupBufs& b, cons
 
   const double row = corr_row_flops(pc.P);
   const std::string cls = "[Lc=" + std::to_string(pc.Lc) + "]";
+  // tensor-core mode takes the second peaks from the FP32 re-evaluation,
+  // which keeps the four largest |y|^2 of every residue of a row: enough
+  // while at most three lags of a residue lie within chip_width of the peak
+  // (chip_width = S samples at every fused rate)
+  const bool rows_p2 = ctx->precision == TGA_PRECISION_FP16_TC && (2 * chip_width + pc.S) / pc.S <= 3;
   timed(ctx, ("code_spectra" + cls).c_str(), (double)n_prn * 2 * fft_flops(pc.Lc),
         [&] { return launch_code_spectra(pc, b.chips, n_prn, b.D, ctx->num_sms, st); });
   timed(ctx, ("frontend" + cls).c_str(), (double)n_ab * 10.0 * pc.P,
@@ -582,11 +590,14 @@ void enqueue_group(tga_ctx* ctx, const ClassGroup& grp, const GroupBufs& b, cons
     // in the FP32 search (rows not listed keep key 0)
     CK(cudaMemsetAsync(b.count, 0, sizeof(int), st));
     CK(cudaMemsetAsync(b.keys32, 0, (size_t)n_ab * 2 * n_prn * sizeof(unsigned long long), st));
+    if (rows_p2) CK(cudaMemsetAsync(b.p2rows, 0, (size_t)n_ab * 2 * n_prn * sizeof(float), st));
     timed(ctx, ("candidates" + cls).c_str(), 0.0,
           [&] { return launch_tc_candidates(dims, 2, b.keys, kTcKeyKeep, b.cand, b.count, st); });
+    // the re-evaluation also keeps each row's second peak, so the chosen
+    // rows need no second transform
     timed(ctx, ("refine" + cls).c_str(), 0.0, [&] {
       return launch_correlate_listed(pc, dims, b.z, b.D, b.cand, b.count, n_ab * 2 * n_prn, b.keys32, ctx->num_sms,
-                                     st);
+                                     st, rows_p2 ? b.p2rows : nullptr, chip_width);
     });
   } else {
     timed(ctx, ("forward_z" + cls).c_str(), (double)n_ab * 2 * fft_flops(pc.P),
@@ -596,8 +607,12 @@ void enqueue_group(tga_ctx* ctx, const ClassGroup& grp, const GroupBufs& b, cons
   }
   const unsigned long long* keys32 = ctx->precision == TGA_PRECISION_FP16_TC ? b.keys32 : b.keys;
   timed(ctx, ("reduce_bins" + cls).c_str(), 0.0, [&] { return launch_reduce_bins(dims, keys32, b.best, st); });
-  timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * row,
-        [&] { return launch_second_peak(pc, dims, b.z, b.D, b.best, chip_width, ctx->num_sms, st); });
+  if (rows_p2)
+    timed(ctx, ("second_peak" + cls).c_str(), 0.0,
+          [&] { return launch_second_from_rows(dims, b.p2rows, b.best, st); });
+  else
+    timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * row,
+          [&] { return launch_second_peak(pc, dims, b.z, b.D, b.best, chip_width, ctx->num_sms, st); });
   timed(ctx, ("finalize" + cls).c_str(), 0.0,
         [&] { return launch_finalize(pc, dims, b.best, center, b.tables, want_cn0, b.cells, st); });
   CK(cudaMemcpyAsync(host_out, b.cells, (size_t)n_ant * n_prn * sizeof(CellOut), cudaMemcpyDeviceToHost, st));
