@@ -519,19 +519,17 @@ __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
           if (q < 0) continue;
           const uint2 m = __ldg(p.z16_map + r);
           const unsigned off[4] = {m.x & 0xffffu, m.x >> 16, m.y & 0xffffu, m.y >> 16};
-          uint32_t h[4];
+          float2 v[4];
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            float2 v = make_float2(0.f, 0.f);
+            v[i] = make_float2(0.f, 0.f);
             if (off[i] != 0xffffu) {
-              v = buf[s * LC + (int)off[i]];
-              v.x *= p.z16_scale;
-              v.y *= p.z16_scale;
+              v[i] = buf[s * LC + (int)off[i]];
+              v[i].x *= p.z16_scale;
+              v[i].y *= p.z16_scale;
             }
-            const __half2 hv = __floats2half2_rn(v.x, v.y);
-            h[i] = *reinterpret_cast<const uint32_t*>(&hv);
           }
-          p.z16[(size_t)q * U::PER_SEQ + r] = make_uint4(h[0], h[1], h[2], h[3]);
+          p.z16[(size_t)q * U::PER_SEQ + r] = pack_unit(v);
         }
         __syncthreads();
       }

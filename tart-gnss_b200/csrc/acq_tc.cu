@@ -388,21 +388,21 @@ struct T3 {
 
 __device__ __forceinline__ uint32_t h2_bits(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
 __device__ __forceinline__ __half2 bits_h2(uint32_t u) { return *reinterpret_cast<__half2*>(&u); }
-__device__ __forceinline__ uint32_t pack_h2(float lo, float hi) { return h2_bits(__floats2half2_rn(lo, hi)); }
 // round two FP32 values to FP16, clamping to +-65504 instead of overflowing
 __device__ __forceinline__ uint32_t pack_h2_sat(float lo, float hi) {
   uint32_t d;
   asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
   return d;
 }
-// c * z for FP16 complex c = (cr, ci), z = (zr, zi):
-// cr (zr, zi) + ci (-zi, zr), with (-zi, zr) from swapping the halves of z
-// and flipping the sign bit of the low one
-__device__ __forceinline__ uint32_t cmul_h2(uint32_t z, uint32_t c) {
-  const __half2 cc = bits_h2(c);
-  const uint32_t zs = __byte_perm(z, 0u, 0x1032u) ^ 0x00008000u;
-  const __half2 t = __hmul2(__low2half2(cc), bits_h2(z));
-  return h2_bits(__hfma2(__high2half2(cc), bits_h2(zs), t));
+// The products of two split units (pack_unit): c z for each of the four
+// values, as a split unit, per pair (re, im) = (cr zr - ci zi, cr zi + ci zr)
+// with the products cr zr and cr zi rounded first.
+__device__ __forceinline__ uint4 cmul_unit(uint4 z, uint4 c) {
+  const __half2 zr0 = bits_h2(z.x), zr1 = bits_h2(z.y), zi0 = bits_h2(z.z), zi1 = bits_h2(z.w);
+  const __half2 cr0 = bits_h2(c.x), cr1 = bits_h2(c.y), ci0 = bits_h2(c.z), ci1 = bits_h2(c.w);
+  return make_uint4(h2_bits(__hfma2(ci0, __hneg2(zi0), __hmul2(cr0, zr0))),
+                    h2_bits(__hfma2(ci1, __hneg2(zi1), __hmul2(cr1, zr1))),
+                    h2_bits(__hfma2(ci0, zr0, __hmul2(cr0, zi0))), h2_bits(__hfma2(ci1, zr1, __hmul2(cr1, zi1))));
 }
 __device__ __forceinline__ void st_shared_u32(unsigned char* p, uint32_t v) { *reinterpret_cast<uint32_t*>(p) = v; }
 
@@ -411,12 +411,15 @@ __device__ __forceinline__ void st_shared_u32(unsigned char* p, uint32_t v) { *r
 // column k = 2 d + (0 re | 1 im), entries of exp(+2 pi i t d / R); zero
 // outside 2R x 2R.  PAIR repeats the block at row and column offset `off`.
 // `atom` selects the K entries [atom KB / 2, (atom + 1) KB / 2) written here.
-template <int R, int N, int KB, bool PAIR>
+// SPLIT: the K entries in the order of split units (pack_unit), column
+// k = 8 (d / 4) + 4 (0 re | 1 im) + d % 4.
+template <int R, int N, int KB, bool PAIR, bool SPLIT = false>
 void host_idft_matrix(unsigned char* dst, int off, int atom = 0) {
   const double kPi = 3.14159265358979323846;
   for (int n = 0; n < N; ++n)
     for (int k = 0; k < KB / 2; ++k) {
       int nn = n, kk = k + atom * (KB / 2);
+      if (SPLIT) kk = 2 * (4 * (kk >> 3) + (kk & 3)) + ((kk >> 2) & 1);  // to the interleaved order
       bool in = nn < 2 * R && kk < 2 * R;
       if (!in && PAIR && nn >= off && nn < off + 2 * R && kk >= off && kk < off + 2 * R) {
         nn -= off;
@@ -453,22 +456,21 @@ __global__ void __launch_bounds__(256) tc_pack_kernel(const float2* __restrict__
     const int d3 = u / T::R2, d2 = u - d3 * T::R2;
     const int kpart = T::freq_part(d2, T::R2, T::E2) + T::freq_part(d3, T::R3, T::E3);
     const float2* s = src + seq * T::LC;
-    uint32_t h[4];
+    float2 v[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int d1 = 4 * j + i;
-      float2 v = make_float2(0.f, 0.f);
+      v[i] = make_float2(0.f, 0.f);
       if (d1 < 31) {
         // the 31-digit is the same in both layouts: (31, 33, M) digit a = d1
         const int k = (T::freq_part(d1, 31, T::E1) + kpart) % T::LC;
         const int kb = (T::UB * k) % 33, kc = M == 1 ? 0 : (T::UC * k) % M;
-        v = __ldg(s + d1 * T::OCOLS + kc * 33 + kb);
-        v.x *= scale;
-        v.y *= scale;
+        v[i] = __ldg(s + d1 * T::OCOLS + kc * 33 + kb);
+        v[i].x *= scale;
+        v[i].y *= scale;
       }
-      h[i] = pack_h2(v.x, v.y);
     }
-    dst[e] = make_uint4(h[0], h[1], h[2], h[3]);
+    dst[e] = pack_unit(v);
   }
 }
 
@@ -808,8 +810,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
           const int k = k0 + i;
           if (k < U && (k < U - 1 || tid + k * NTS < T::UNITS)) {
             const uint4 cc = c[i], z = zr[k];
-            *reinterpret_cast<uint4*>(A + (uoff[k] & 0xFFFFu)) =
-                make_uint4(cmul_h2(z.x, cc.x), cmul_h2(z.y, cc.y), cmul_h2(z.z, cc.z), cmul_h2(z.w, cc.w));
+            *reinterpret_cast<uint4*>(A + (uoff[k] & 0xFFFFu)) = cmul_unit(z, cc);
           }
         }
       }
@@ -1332,7 +1333,7 @@ template <int M>
 std::vector<unsigned char> build_matrices() {
   using T = T3<M>;
   std::vector<unsigned char> b((size_t)(T::B1_BYTES + T::B2_BYTES + T::B3_BYTES), 0);
-  host_idft_matrix<31, T::N1, T::KB1, false>(b.data(), 0);
+  host_idft_matrix<31, T::N1, T::KB1, false, true>(b.data(), 0);
   for (int a = 0; a < T::B2_ATOMS; ++a)
     host_idft_matrix<T::R2, T::N2, T::KB2, false>(b.data() + T::B1_BYTES + a * T::N2 * T::KB2, 0, a);
   if (T::NST == 3)

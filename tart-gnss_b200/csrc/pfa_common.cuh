@@ -1,6 +1,7 @@
 // Shared definitions of the prime-factor transform kernels (FP32 SIMT and
 // tensor-core variants).
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -37,9 +38,20 @@ struct Geo {
 // layout (Lc = 31 R2 R3; (R2, R3) = (33, 1), (12, 11), (30, 11) for M = 1,
 // 4, 10).  Unit (seq, j, u), u = d3 R2 + d2, holds the spectrum at digits
 // (d1, d2, d3), d1 = 4j .. 4j + 3 (zero for d1 >= 31), as 4 half2 (16
-// bytes).  A frequency digit d of radix R stands for the natural
+// bytes) split into real and imaginary parts: (re0, re1), (re2, re3),
+// (im0, im1), (im2, im3) (pack_unit), so that the products of two units
+// take four packed FP16 operations per pair of values and need no
+// repacking; the stage-1 operand rows keep this order of their K entries
+// and the stage-1 DFT matrix is built for it.  A frequency digit d of radix R stands for the natural
 // frequencies k = d (LC / R) (mod R); src_offset is where the FP32 engine's
 // digit layout [a][c][b] of the (31, 33, M) map holds the same frequency.
+__device__ __forceinline__ uint4 pack_unit(const float2 (&v)[4]) {
+  const __half2 a = __floats2half2_rn(v[0].x, v[1].x), b = __floats2half2_rn(v[2].x, v[3].x);
+  const __half2 c = __floats2half2_rn(v[0].y, v[1].y), d = __floats2half2_rn(v[2].y, v[3].y);
+  return make_uint4(*reinterpret_cast<const uint32_t*>(&a), *reinterpret_cast<const uint32_t*>(&b),
+                    *reinterpret_cast<const uint32_t*>(&c), *reinterpret_cast<const uint32_t*>(&d));
+}
+
 template <int M>
 struct TcUnits {
   static constexpr int R2 = M == 1 ? 33 : M == 4 ? 12 : 30, R3 = M == 1 ? 1 : 11;
