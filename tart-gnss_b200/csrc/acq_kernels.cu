@@ -265,32 +265,6 @@ cudaError_t launch_frontend(const SampleSource& src, const SearchDims& dims, con
 // ---------------------------------------------------------------------------
 // prime-factor transform engine
 // ---------------------------------------------------------------------------
-// The four largest (value, index) pairs seen by a thread, largest first;
-// values are non-negative |y|^2 (as bits they order like unsigned
-// integers), an empty place holds 0.
-struct Top4 {
-  float v[4] = {0.f, 0.f, 0.f, 0.f};
-  int i[4] = {0, 0, 0, 0};
-  __device__ __forceinline__ void add(float x, int k) {
-    if (!(x > v[3])) return;
-    const bool g0 = x > v[0], g1 = x > v[1], g2 = x > v[2];
-    v[3] = g2 ? v[2] : x;
-    i[3] = g2 ? i[2] : k;
-    v[2] = g1 ? v[1] : (g2 ? x : v[2]);
-    i[2] = g1 ? i[1] : (g2 ? k : i[2]);
-    v[1] = g0 ? v[0] : (g1 ? x : v[1]);
-    i[1] = g0 ? i[0] : (g1 ? k : i[1]);
-    v[0] = g0 ? x : v[0];
-    i[0] = g0 ? k : i[0];
-  }
-  __device__ __forceinline__ void pop() {
-    v[0] = v[1], i[0] = i[1];
-    v[1] = v[2], i[1] = i[2];
-    v[2] = v[3], i[2] = i[3];
-    v[3] = 0.f;
-  }
-};
-
 template <int M, int BC, int NT, int MINB, int MODE>
 __global__ void __launch_bounds__(NT, MINB) pfa_kernel(PfaParams p) {
   using G = Geo<M>;
@@ -785,19 +759,19 @@ cudaError_t launch_correlate_listed(const PolyClass& pc, const SearchDims& dims,
 // The second peak of each cell from the re-evaluated rows: the cell's
 // chosen row is always one of them (its FP32 key is the cell's maximum; when
 // every key is 0, every row was listed).
-__global__ void second_from_rows_kernel(int n_cells, int n_prn, const float* __restrict__ p2rows,
+__global__ void second_from_rows_kernel(int n_cells, int n_hyp, int n_prn, const float* __restrict__ p2rows,
                                         BestRow* __restrict__ best) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= n_cells) return;
   const BestRow b = best[w];
-  best[w].p2 = p2rows[(size_t)(b.ab * 2 + b.hyp) * n_prn + (w % n_prn)];
+  best[w].p2 = p2rows[(size_t)(b.ab * n_hyp + b.hyp) * n_prn + (w % n_prn)];
 }
 
-cudaError_t launch_second_from_rows(const SearchDims& dims, const float* d_p2rows, BestRow* d_best,
+cudaError_t launch_second_from_rows(const SearchDims& dims, int n_hyp, const float* d_p2rows, BestRow* d_best,
                                     cudaStream_t st) {
   const int n = dims.n_ant * dims.n_prn;
   if (n <= 0) return cudaSuccess;
-  second_from_rows_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, dims.n_prn, d_p2rows, d_best);
+  second_from_rows_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, n_hyp, dims.n_prn, d_p2rows, d_best);
   return TGA_LAUNCHED();
 }
 

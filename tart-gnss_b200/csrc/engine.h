@@ -109,8 +109,10 @@ cudaError_t launch_correlate_listed(const PolyClass& pc, const SearchDims& dims,
                                     const float2* d_D, const int2* d_cand, const int* d_count, int capacity,
                                     unsigned long long* d_keys, int num_sms, cudaStream_t st,
                                     float* d_p2rows = nullptr, int chip_width = 0);
-// d_best[w].p2 = d_p2rows at the row d_best[w] chose (the keys' layout).
-cudaError_t launch_second_from_rows(const SearchDims& dims, const float* d_p2rows, BestRow* d_best,
+// d_best[w].p2 = d_p2rows at the row d_best[w] chose (the keys' layout:
+// [ab][hyp][prn] with n_hyp hypotheses, 2 for the drop-in search, 1 for the
+// non-coherent one).
+cudaError_t launch_second_from_rows(const SearchDims& dims, int n_hyp, const float* d_p2rows, BestRow* d_best,
                                     cudaStream_t st);
 // Lists, per (antenna, PRN), the rows whose reduced-precision key is at least
 // keep x the largest of its nb * n_hyp rows (appended to d_cand, counted in
@@ -206,10 +208,13 @@ cudaError_t launch_nc_reduce(const SearchDims& dims, const unsigned long long* d
 // launch_nc_correlate over the (ab, prn) rows listed in d_cand (*d_count of
 // them, at most capacity), as the FP32 re-evaluation of a reduced-precision
 // search's candidates: each listed row's key is written where
-// launch_nc_correlate would write it
+// launch_nc_correlate would write it; with d_p2rows, also each listed row's
+// second peak against its own maximum (what launch_nc_second computes for a
+// chosen row)
 cudaError_t launch_nc_correlate_listed(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
                                        const float2* d_D, const int2* d_cand, const int* d_count, int capacity,
-                                       unsigned long long* d_keys, int num_sms, cudaStream_t st);
+                                       unsigned long long* d_keys, int num_sms, cudaStream_t st,
+                                       float* d_p2rows = nullptr, int chip_width = 0);
 cudaError_t launch_nc_second(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
                              const float2* d_D, BestRow* d_best, int chip_width, int num_sms, cudaStream_t st);
 

@@ -193,6 +193,8 @@ struct NcParams {
   BestRow* best;             // NC_SECOND: [n_ant][n_prn]
   const int2* cand;          // NC_CAND: the rows
   const int* cand_count;     // NC_CAND: their number (device)
+  float* p2rows;             // NC_CAND (optional): each row's second peak
+                             // against its own maximum, where its key goes
 };
 
 template <int M, int BC, int NT, int MODE>
@@ -203,6 +205,11 @@ __global__ void __launch_bounds__(NT, 1) nc_correlate_kernel(NcParams p) {
   float* acc = reinterpret_cast<float*>(buf + BC * LC);
   __shared__ unsigned long long s_key;
   __shared__ unsigned int s_p2;
+  // NC_CAND with p2rows: for every residue and every warp that scanned it,
+  // its four largest summed |y|^2 as (value bits << 32) | lag, after acc
+  constexpr int TOP_WPS = NT / 32 / BC >= 1 ? NT / 32 / BC : 1;
+  const bool keep_top = MODE == NC_CAND && p.p2rows != nullptr;
+  unsigned long long* s_res = reinterpret_cast<unsigned long long*>(acc + BC * LC);
   const int tid = threadIdx.x, S = p.S;
   const int groups = (S + BC - 1) / BC;
   const int n_work = MODE == NC_CAND ? min(p.n_items, *p.cand_count) : p.n_items;
@@ -302,6 +309,50 @@ __global__ void __launch_bounds__(NT, 1) nc_correlate_kernel(NcParams p) {
           if (min(d, p.P - d) > p.chip_width) pbest = fmaxf(pbest, pw);
         }
       }
+      // NC_CAND with p2rows: the four largest sums of every residue of the
+      // group with their lags (as the drop-in search's re-evaluation does:
+      // a warp's fourth largest lane maximum bounds its four largest from
+      // below)
+      if (keep_top) {
+        const int warp = tid >> 5, lane = tid & 31;
+        const int sl = warp / TOP_WPS, sub = warp - sl * TOP_WPS;
+        if (sl < BC && seq_of(sl) >= 0) {  // uniform over the warp
+          const float* pws = acc + sl * LC;
+          unsigned mb = 0u;
+          for (int i = sub * 32 + lane; i < LC; i += TOP_WPS * 32) mb = max(mb, __float_as_uint(pws[i]));
+          unsigned thr = 0u;
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            thr = __reduce_max_sync(0xffffffffu, mb);
+            const unsigned h = __ballot_sync(0xffffffffu, mb == thr);
+            if (lane == __ffs(h) - 1) mb = 0u;
+          }
+          Top4 t;
+          for (int i = sub * 32 + lane; i < LC; i += TOP_WPS * 32) {
+            const float x = pws[i];
+            if (__float_as_uint(x) >= thr) t.add(x, i);
+          }
+          const int rho = seq_of(sl);
+          unsigned long long* dst = s_res + ((size_t)rho * TOP_WPS + sub) * 4;
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const unsigned vb = __float_as_uint(t.v[0]);
+            const unsigned x = __reduce_max_sync(0xffffffffu, vb);
+            const unsigned h = __ballot_sync(0xffffffffu, vb == x);
+            const int src = __ffs(h) - 1;
+            const int i = __shfl_sync(0xffffffffu, t.i[0], src);
+            if (lane == src) t.pop();
+            if (lane == r) {
+              unsigned long long k = 0ull;
+              if (x != 0u) {
+                const int a = i / COLS, rem = i - a * COLS, c = rem / 33, b = rem - c * 33;
+                k = ((unsigned long long)x << 32) | (unsigned)(rho + S * G::natural(a, b, c));
+              }
+              dst[r] = k;
+            }
+          }
+        }
+      }
       __syncthreads();
     }
     if (ARGMAX) {
@@ -313,6 +364,23 @@ __global__ void __launch_bounds__(NT, 1) nc_correlate_kernel(NcParams p) {
       if ((tid & 31) == 0) atomicMax(&s_key, kbest);
       __syncthreads();
       if (tid == 0) p.keys[(size_t)ab * p.n_prn + prn] = s_key;
+      // NC_CAND with p2rows: the row's second peak against its own maximum
+      // (at most three lags of a residue lie within chip_width of it)
+      if (keep_top && tid < 32) {
+        const unsigned long long kb = s_key;
+        const int tau = (int)(unsigned)kb;
+        float p2 = 0.f;
+        if (kb != 0ull)
+          for (int e = tid; e < S * TOP_WPS * 4; e += 32) {
+            const unsigned long long k = s_res[e];
+            int d = (int)(unsigned)k - tau;
+            d = d < 0 ? -d : d;
+            if (k != 0ull && min(d, p.P - d) > p.chip_width) p2 = fmaxf(p2, __uint_as_float((unsigned)(k >> 32)));
+          }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) p2 = fmaxf(p2, __shfl_xor_sync(0xffffffffu, p2, o));
+        if (tid == 0) p.p2rows[(size_t)ab * p.n_prn + prn] = p2;
+      }
     } else {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) pbest = fmaxf(pbest, __shfl_xor_sync(0xffffffffu, pbest, o));
@@ -343,7 +411,11 @@ template <int M, int MODE>
 cudaError_t run_nc(const NcParams& p, int num_sms, cudaStream_t st) {
   using C = NcCfg<M>;
   constexpr int LC = Geo<M>::LC;
-  const size_t smem = (size_t)C::BC * LC * (sizeof(float2) + sizeof(float));
+  size_t smem = (size_t)C::BC * LC * (sizeof(float2) + sizeof(float));
+  if (MODE == NC_CAND && p.p2rows) {
+    constexpr int WPS = C::NT / 32 / C::BC >= 1 ? C::NT / 32 / C::BC : 1;
+    smem += (size_t)p.S * WPS * 4 * sizeof(unsigned long long);
+  }
   auto kern = nc_correlate_kernel<M, C::BC, C::NT, MODE>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -471,8 +543,11 @@ cudaError_t launch_nc_second(const PolyClass& pc, const SearchDims& dims, int B,
 
 cudaError_t launch_nc_correlate_listed(const PolyClass& pc, const SearchDims& dims, int B, const float2* d_z,
                                        const float2* d_D, const int2* d_cand, const int* d_count, int capacity,
-                                       unsigned long long* d_keys, int num_sms, cudaStream_t st) {
+                                       unsigned long long* d_keys, int num_sms, cudaStream_t st, float* d_p2rows,
+                                       int chip_width) {
   NcParams p = {};
+  p.p2rows = d_p2rows;
+  p.chip_width = chip_width;
   p.z = d_z;
   p.D = d_D;
   p.keys = d_keys;

@@ -75,6 +75,32 @@ struct TcUnits {
   }
 };
 
+// The four largest (value, index) pairs seen by a thread, largest first;
+// values are non-negative |y|^2 (as bits they order like unsigned
+// integers), an empty place holds 0.
+struct Top4 {
+  float v[4] = {0.f, 0.f, 0.f, 0.f};
+  int i[4] = {0, 0, 0, 0};
+  __device__ __forceinline__ void add(float x, int k) {
+    if (!(x > v[3])) return;
+    const bool g0 = x > v[0], g1 = x > v[1], g2 = x > v[2];
+    v[3] = g2 ? v[2] : x;
+    i[3] = g2 ? i[2] : k;
+    v[2] = g1 ? v[1] : (g2 ? x : v[2]);
+    i[2] = g1 ? i[1] : (g2 ? k : i[2]);
+    v[1] = g0 ? v[0] : (g1 ? x : v[1]);
+    i[1] = g0 ? i[0] : (g1 ? k : i[1]);
+    v[0] = g0 ? x : v[0];
+    i[0] = g0 ? k : i[0];
+  }
+  __device__ __forceinline__ void pop() {
+    v[0] = v[1], i[0] = i[1];
+    v[1] = v[2], i[1] = i[2];
+    v[2] = v[3], i[2] = i[3];
+    v[3] = 0.f;
+  }
+};
+
 // CAND is CORR over a device-built list of rows (the candidates of a
 // reduced-precision search, re-evaluated in FP32): row i of the list is
 // (ab * 2 + hyp, prn), the list holds *cand_count rows, and each row's key

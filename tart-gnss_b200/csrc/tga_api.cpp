@@ -609,7 +609,7 @@ void enqueue_group(tga_ctx* ctx, const ClassGroup& grp, const GroupBufs& b, cons
   timed(ctx, ("reduce_bins" + cls).c_str(), 0.0, [&] { return launch_reduce_bins(dims, keys32, b.best, st); });
   if (rows_p2)
     timed(ctx, ("second_peak" + cls).c_str(), 0.0,
-          [&] { return launch_second_from_rows(dims, b.p2rows, b.best, st); });
+          [&] { return launch_second_from_rows(dims, 2, b.p2rows, b.best, st); });
   else
     timed(ctx, ("second_peak" + cls).c_str(), (double)n_ant * n_prn * row,
           [&] { return launch_second_peak(pc, dims, b.z, b.D, b.best, chip_width, ctx->num_sms, st); });
@@ -2048,6 +2048,12 @@ void nc_run_group(tga_ctx* ctx, const uint8_t* d_bits, size_t row_bytes, const d
   int *d_err = nullptr, *d_count = nullptr;
   unsigned long long* d_keys32 = nullptr;
   int2* d_cand = nullptr;
+  // tensor-core mode takes the second peaks from the FP32 re-evaluation
+  // (the four largest sums per residue; exact while at most three lags of a
+  // residue lie within chip_width of the peak)
+  float* d_p2rows = nullptr;
+  const int cw = chip_width_of(fs);
+  const bool rows_p2 = tc && (2 * cw + pc.S) / pc.S <= 3;
   if (tc) {
     d_z16 = ctx->buf("nc.z16", tc_operand_bytes(pc, n_seq, false));
     d_zmap = tc_unit_map_buf(ctx, pc.M);
@@ -2063,6 +2069,7 @@ void nc_run_group(tga_ctx* ctx, const uint8_t* d_bits, size_t row_bytes, const d
       d_bmat = ctx->buf(mat_name, 0);
     }
     d_keys32 = (unsigned long long*)ctx->buf(tag + ".keys32", n_rows * sizeof(unsigned long long));
+    if (rows_p2) d_p2rows = (float*)ctx->buf(tag + ".p2rows", n_rows * sizeof(float));
     d_cand = (int2*)ctx->buf(tag + ".cand", n_rows * sizeof(int2));
     d_count = (int*)ctx->buf(tag + ".count", (size_t)n_chunks * sizeof(int));
     timed(ctx, ("nc_tc_pack" + cls).c_str(), 0.0,
@@ -2071,6 +2078,7 @@ void nc_run_group(tga_ctx* ctx, const uint8_t* d_bits, size_t row_bytes, const d
     CK(cudaMemsetAsync(d_count, 0, (size_t)n_chunks * sizeof(int), st));
     CK(cudaMemsetAsync(d_keys, 0, n_rows * sizeof(unsigned long long), st));
     CK(cudaMemsetAsync(d_keys32, 0, n_rows * sizeof(unsigned long long), st));
+    if (rows_p2) CK(cudaMemsetAsync(d_p2rows, 0, n_rows * sizeof(float), st));
     ctx->tc_err_pending = d_err;
   }
   for (int ch = 0; ch < n_chunks; ++ch) {
@@ -2102,15 +2110,19 @@ void nc_run_group(tga_ctx* ctx, const uint8_t* d_bits, size_t row_bytes, const d
       });
       timed(ctx, ("nc_refine" + cls).c_str(), 0.0, [&] {
         return launch_nc_correlate_listed(pc, cd, B, d_z, d_D, d_cand + r0, d_count + ch, na * nb * n_prn,
-                                          d_keys32 + r0, ctx->num_sms, st);
+                                          d_keys32 + r0, ctx->num_sms, st, rows_p2 ? d_p2rows + r0 : nullptr, cw);
       });
     } else {
       timed(ctx, ("nc_correlate" + cls).c_str(), (double)na * nb * n_prn * B * row,
             [&] { return launch_nc_correlate(pc, cd, B, d_z, d_D, d_keys + r0, ctx->num_sms, st); });
     }
     timed(ctx, ("nc_reduce" + cls).c_str(), 0.0, [&] { return launch_nc_reduce(cd, (tc ? d_keys32 : d_keys) + r0, cbest, st); });
-    timed(ctx, ("nc_second" + cls).c_str(), (double)na * n_prn * B * row,
-          [&] { return launch_nc_second(pc, cd, B, d_z, d_D, cbest, chip_width_of(fs), ctx->num_sms, st); });
+    if (rows_p2)
+      timed(ctx, ("nc_second" + cls).c_str(), 0.0,
+            [&] { return launch_second_from_rows(cd, 1, d_p2rows + r0, cbest, st); });
+    else
+      timed(ctx, ("nc_second" + cls).c_str(), (double)na * n_prn * B * row,
+            [&] { return launch_nc_second(pc, cd, B, d_z, d_D, cbest, cw, ctx->num_sms, st); });
   }
   std::vector<BestRow> best((size_t)n_ant * n_prn);
   CK(cudaMemcpyAsync(best.data(), d_best, best.size() * sizeof(BestRow), cudaMemcpyDeviceToHost, st));
