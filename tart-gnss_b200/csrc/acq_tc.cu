@@ -1070,7 +1070,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) pfa_tc3_kernel(Tc3Params p) {
 #pragma unroll
         for (int h = 0; h < 11; ++h) {
           const float re = __uint_as_float(v[2 * h]), im = __uint_as_float(v[2 * h + 1]);
-          su[h] = __float_as_uint(fmaf(re, re, im * im) + (first ? 0.f : __uint_as_float(su[h])));
+          // two FMAs per output (these sums only rank rows for the FP32
+          // re-evaluation, which recomputes the chosen values)
+          su[h] = __float_as_uint(fmaf(re, re, fmaf(im, im, first ? 0.f : __uint_as_float(su[h]))));
         }
         if (!last) {
           su[11] = 0u;
