@@ -64,7 +64,7 @@ struct BestRow {
   int32_t hyp;     // 0 [c,c], 1 [c,-c]
   int32_t tau;     // lag in samples, [0, P)
   float p;         // |y|^2 at the peak
-  float p2;        // second peak |y|^2 (set by the second-peak pass); 0 when none
+  float p2;        // second peak |y|^2 (second-peak pass, or the re-evaluated rows); 0 when none
 };
 
 // Finalised cell (device side); host converts to tga_cell.
